@@ -1,0 +1,174 @@
+/*
+ * fvr_b200.h -- C ABI of the B200 (sm_100a) Diff-FVR hot-path library
+ * (libfvr_b200.so).
+ *
+ * Conventions shared by every entry point:
+ *   - All array arguments are DEVICE pointers owned by the caller; the library
+ *     never allocates per call.  Temporary space comes from a caller-provided
+ *     `workspace` whose minimum size is returned by the matching
+ *     fvr_*_workspace() query.
+ *   - `stream` is a cudaStream_t passed as void*; work is stream-ordered and
+ *     no call synchronises the device.
+ *   - Every entry point returns an fvr_status; nothing throws across the ABI.
+ *   - Complex arrays are interleaved (re, im) pairs.
+ *   - Sizes are int64_t element counts.
+ *
+ * The comment above each function names the reference interface it replaces
+ * (paths inside the pareelamre/diff-fvr project).
+ */
+#ifndef FVR_B200_H
+#define FVR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FVR_OK = 0,
+  FVR_ERR_ARG = 1,         /* null pointer, bad size, stride or alignment   */
+  FVR_ERR_DTYPE = 2,       /* unsupported storage dtype for this entry      */
+  FVR_ERR_UNSUPPORTED = 3, /* e.g. FFT length with a prime factor above 13  */
+  FVR_ERR_WORKSPACE = 4,   /* caller workspace smaller than the query says  */
+  FVR_ERR_CUDA = 5,        /* launch or driver error (cudaGetLastError)     */
+  FVR_ERR_TIMEOUT = 6      /* a bounded device-side wait gave up            */
+} fvr_status;
+
+typedef enum { FVR_F32 = 0, FVR_BF16 = 1, FVR_F16 = 2, FVR_F64 = 3 } fvr_dtype;
+
+const char* fvr_status_string(int status);
+int fvr_version(void);
+/* 1 if the device (ordinal) is sm_100 (B200 family), 0 otherwise. */
+int fvr_device_supported(int device);
+
+/* ---------------------------------------------------------------- FFT ---- */
+/* Replaces torch.fft.fftn/ifft2/fft2 + fftshift/ifftshift at
+ * src/fvr/torch_engine.py:80-81, 238-239, 263, 322-323,
+ * src/fvr/cone_beam_fvr.py:291-294, 502-505 and scipy.fft at
+ * src/fvr/diff_fvr.py:54, 168.  Lengths: 2^a 3^b 5^c 7^d 11^e 13^f <= 16384. */
+int fvr_fft_supported(int64_t n);
+/* tw_out: n complex (prec FVR_F32: float2, FVR_F64: double2) = exp(-2 pi i m/n) */
+int fvr_fft_twiddles(int64_t n, int prec, void* tw_out, void* stream);
+/* Batch of zero-padded real volumes [batch][d][h][w] -> centred spectra
+ * [batch][Dp][Hp][Wp] complex.  convention 0: torch engine (pad, fftn,
+ * fftshift; torch_engine.py:56-86); 1: NumPy renderer (optional sinc^2
+ * premultiplication tables wz/wy/wx, pad, ifftshift, fftn, fftshift;
+ * diff_fvr.py:34-54); 2: PoU blocks (already padded; ifftshift, fftn,
+ * fftshift; cone_beam_fvr.py:291-294). */
+int fvr_spectrum3d(const void* vol, int vol_dtype, int64_t batch, int64_t d, int64_t h, int64_t w, int64_t Dp,
+                   int64_t Hp, int64_t Wp, int convention, const double* wz, const double* wy, const double* wx,
+                   int prec, void* out, const void* tw_x, const void* tw_y, const void* tw_z, void* stream);
+/* Batched 2D FFT of [batch][n0][n1] (complex, or real if in_real).
+ * in_shift / out_shift: 0 none, 1 ifftshift, 2 fftshift (applied before /
+ * after the transform).  out_mode 0: complex (scaled); 1: real part; 2: real
+ * part + ReLU, written into the crop window [r0, r0+nr) x [c0, c0+nc).
+ * `work` holds batch*n0*n1 complex and may alias `in` for complex input. */
+int fvr_fft2d(const void* in, int in_real, int64_t batch, int64_t n0, int64_t n1, int prec, int inverse,
+              int in_shift, int out_shift, double scale, int out_mode, void* out, int64_t crop_r0, int64_t crop_nr,
+              int64_t crop_c0, int64_t crop_nc, const void* tw0, const void* tw1, void* work, void* stream);
+
+/* ------------------------------------------------- stencil spectrum ---- */
+/* Stencil layout of a D x H x W centred complex spectrum: (D+1)(H+1)(W+1)
+ * entries, each the 8 complex corners of one trilinear cell (corners outside
+ * the volume are zero).  f32: 64 B per entry; bf16 / f16: 32 B per entry, f16
+ * with a power-of-two scale per 16^3-entry brick.  Built from a "master"
+ * spectrum in f32 or bf16, planar [2][D][H][W] (master_planar = 1, the
+ * reference's f_vol_5d[0]) or interleaved [D][H][W][2] (master_planar = 0).  Storage for the
+ * spectrum buffer f_vol_5d of src/fvr/torch_engine.py:83-88 and its
+ * to_precision cast (:90-95). */
+int64_t fvr_stencil_bytes(int64_t D, int64_t H, int64_t W, int dtype);
+int64_t fvr_stencil_scale_count(int64_t D, int64_t H, int64_t W);
+/* scratch_max: fvr_stencil_scale_count() uint32 (f16 only, else NULL) */
+int fvr_stencil_build(const void* master, int master_dtype, int master_planar, int64_t D, int64_t H, int64_t W,
+                      int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream);
+
+/* --------------------------------------- drop-in trilinear slice gather -- */
+/* fourier_slice_3d on the reference layout vol[B][2][D][H][W] (dtype f32 /
+ * bf16 / f16), p = c + fx[q] u[n] + fy[q] v[n], zero-padding partial
+ * interpolation; out[B][N][2][K] in the volume dtype.
+ * Replaces _TritonFourierSlice3DFn.forward, src/fvr/triton_slice.py:274-303. */
+int fvr_slice3d_fwd(const void* vol, int dtype, int64_t B, int64_t D, int64_t H, int64_t W, const float* u,
+                    const float* v, int64_t N, const float* fx, const float* fy, int64_t K, float cx, float cy,
+                    float cz, void* out, void* stream);
+int64_t fvr_slice3d_bwd_workspace(int64_t N, int64_t K);
+/* dL/du, dL/dv [N][3] (fp64 accumulation, deterministic).
+ * Replaces _TritonFourierSlice3DFn.backward, src/fvr/triton_slice.py:305-339. */
+int fvr_slice3d_bwd(const void* vol, int dtype, int64_t B, int64_t D, int64_t H, int64_t W, const void* grad_out,
+                    const float* u, const float* v, int64_t N, const float* fx, const float* fy, int64_t K, float cx,
+                    float cy, float cz, float* gu, float* gv, void* workspace, int64_t ws_bytes, void* stream);
+
+/* -------------------------------------- parallel-beam (torch engine) ---- */
+/* Slice axes for poses[C][6] (yaw, pitch, roll deg; tx, ty, tz): axes[C][8] =
+ * (u_xyz, v_xyz, tx, ty), u = R[0,:]*((W-1)/2,(H-1)/2,(D-1)/2), v = R[1,:]*(..),
+ * R = Rz(yaw) Ry(pitch) Rx(roll) in fp64, lateral view R . Rz(90 deg).
+ * view 0 = 'ap', 1 = 'lateral'.  src/fvr/torch_engine.py:139-211. */
+int fvr_tc_axes(const float* poses, int64_t C, int view, int64_t D, int64_t H, int64_t W, float* axes,
+                void* stream);
+int64_t fvr_tc_sncc_workspace(int64_t C, int64_t R);
+/* Fused zero-IFFT spectral NCC, pass 1: per candidate one pass gathering the
+ * slice, applying the phase ramp kappa*(ku tx + kv ty) and the high-pass
+ * table hp (NULL = none), and reducing the NCC moments against ftarg[R][R]
+ * (complex); with_grad also reduces the 14 pose-gradient moments.  Per-tile
+ * partial sums go to `workspace`.  lin = torch.linspace(-1, 1, R).
+ * Replaces TorchDiffFVREngine._spectral_ncc_core / forward_spectral_ncc,
+ * src/fvr/torch_engine.py:269-307 (the gather of :176-234 included). */
+int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
+                        const float* axes, int64_t C, const void* ftarg, const float* hp, const float* lin,
+                        int64_t R, double kappa, int with_grad, void* workspace, int64_t ws_bytes, void* stream);
+/* Pass 2: tile sums in fp64 -> mom[C][17 or 3] (kept for the backward);
+ * loss = 1 - mean_c ncc_c (f32 scalar); ncc_out[C] optional. */
+int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int with_grad, double* mom, float* loss,
+                         float* ncc_out, void* stream);
+/* dL/dposes[C][6] from the saved moments and the device scalar g = dL/dloss
+ * (tz column is zero: the reference never reads poses[:, 5]).  accumulate != 0
+ * adds into grad_poses.  Autograd backward of torch_engine.py:269-307. */
+int fvr_tc_sncc_backward(const double* mom, const float* g, const float* poses, int64_t C, int view, int64_t D,
+                         int64_t H, int64_t W, double kappa, float* grad_poses, int accumulate, void* stream);
+/* Modulated slice S*exp(i phase) -> out[C][R][R] complex; shift != 0 writes it
+ * in ifftshift order (input of the image IFFT).
+ * Replaces TorchDiffFVREngine._extract_slice_spectrum, torch_engine.py:176-234. */
+int fvr_tc_slice(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
+                 const float* axes, int64_t C, const float* lin, int64_t R, double kappa, int shift, void* out,
+                 void* stream);
+int64_t fvr_tc_slice_adjoint_workspace(int64_t C, int64_t R);
+/* Pose gradient for an upstream gradient G[C][R][R] (complex) with respect to
+ * the modulated slice (same order as fvr_tc_slice with the same shift).
+ * Autograd backward of torch_engine.py:176-241. */
+int fvr_tc_slice_adjoint(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
+                         const float* axes, const float* poses, int64_t C, int view, const float* lin, int64_t R,
+                         double kappa, int shift, const void* G, void* workspace, int64_t ws_bytes,
+                         float* grad_poses, int accumulate, void* stream);
+/* out = (img > 0) ? g : 0  (ReLU adjoint of torch_engine.py:240) */
+int fvr_relu_mask(const float* img, const float* g, float* out, int64_t n, void* stream);
+/* x[i] *= table[i % per] for complex x (high-pass of prepare_spectral_target,
+ * torch_engine.py:264-266) */
+int fvr_cmul_table(void* x, const float* table, int64_t per, int64_t n, void* stream);
+/* 1 - exp(-r^2 / (2 sigma^2)), torch_engine.py:123-136 */
+int fvr_hp_filter(float* out, int64_t H, int64_t W, double sigma, void* stream);
+/* torch.linspace(start, end, n) in float32 */
+int fvr_linspace(float* out, float start, float end, int64_t n, void* stream);
+
+/* ----------------------------------------------------------- timing ---- */
+/* cudaEventRecordWithFlags(event, stream, external ? cudaEventRecordExternal
+ * : 0): lets a caller time one kernel inside a captured CUDA graph (no
+ * reference counterpart; measurement utility). */
+int fvr_event_record(void* event, void* stream, int external);
+
+/* ------------------------------------------- image-domain spectral NCC -- */
+/* Between centred spectra Fp[B][n] and Ft[Bt][n] (Bt = 1 or B, complex), both
+ * multiplied by hp[n] (NULL = none): mom[B][3] = (cross, Ep, Et) in fp64,
+ * loss = 1 - mean_b ncc_b.  Replaces TorchDiffFVREngine.spectral_ncc_loss,
+ * src/fvr/torch_engine.py:309-337 (after the fft2 + fftshift of both images). */
+int64_t fvr_cncc_workspace(int64_t B, int64_t n);
+int fvr_cncc_forward(const void* Fp, const void* Ft, int64_t B, int64_t Bt, int64_t n, const float* hp,
+                     void* workspace, int64_t ws_bytes, double* mom, float* loss, void* stream);
+/* X[B][n] = dL/dFp (complex) for the device scalar g = dL/dloss. */
+int fvr_cncc_backward(const void* Fp, const void* Ft, int64_t B, int64_t Bt, int64_t n, const float* hp,
+                      const double* mom, const float* g, void* X, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FVR_B200_H */

@@ -1,0 +1,282 @@
+"""Generate golden vectors by running the reference implementation on CPU.
+
+Usage (needs the reference checkout; run from the repository root):
+
+    python tests/golden/make_golden.py /root/reference
+
+It imports the reference's ``fvr`` package (``src/fvr``) with empty stand-ins
+for ``pydicom`` / ``SimpleITK`` (only ``dicom_loader`` needs them, and nothing
+on the rendering path calls it), runs seeded small cases through the
+reference's public entry points and its autograd, and writes the inputs and
+outputs to ``tests/golden/*.npz``.  The fixtures are committed; the tests never
+read the reference checkout.
+"""
+from __future__ import annotations
+
+import math
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+
+
+def _import_reference(ref_root: Path):
+    for name in ("pydicom", "SimpleITK"):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.path.insert(0, str(ref_root / "src"))
+    import fvr  # noqa: F401
+    from fvr import cone_beam_fvr, diff_fvr, gradients, torch_engine, triton_slice
+
+    return torch_engine, triton_slice, cone_beam_fvr, diff_fvr, gradients
+
+
+def _ellipsoids(n, seed, shape=None):
+    sys.path.insert(0, str(REPO))
+    from oracle.torch_convention import make_ellipsoid_volume
+
+    return make_ellipsoid_volume(n, seed, shape=shape)
+
+
+def gen_slice_and_warp(ts):
+    import torch
+
+    out = {}
+    # trilinear gather + adjoint (mirrors tests/test_cone_beam_fvr.py:152-177 set-up)
+    torch.manual_seed(11)
+    B_vol, D, H, W, N_pose, P = 3, 24, 20, 22, 4, 20
+    vol = torch.randn(B_vol, 2, D, H, W, dtype=torch.float32)
+    coords = torch.linspace(-0.45, 0.45, P)
+    fy, fx = torch.meshgrid(coords, coords, indexing="ij")
+    fx_flat, fy_flat = fx.reshape(-1).contiguous(), fy.reshape(-1).contiguous()
+    u0 = torch.randn(N_pose, 3) * 8.0
+    v0 = torch.randn(N_pose, 3) * 8.0
+    c = (11.0, 9.5, 10.5)
+    u = u0.clone().requires_grad_(True)
+    v = v0.clone().requires_grad_(True)
+    s = ts.fourier_slice_3d_torch(vol, u, v, fx_flat, fy_flat, c)
+    w_out = torch.randn_like(s)
+    (s * w_out).sum().backward()
+    out.update(
+        slice_vol=vol.numpy(), slice_u=u0.numpy(), slice_v=v0.numpy(), slice_fx=fx_flat.numpy(),
+        slice_fy=fy_flat.numpy(), slice_center=np.array(c), slice_out=s.detach().numpy(),
+        slice_wout=w_out.numpy(), slice_gu=u.grad.numpy(), slice_gv=v.grad.numpy(),
+    )
+    # pinhole warp-sum + adjoint (mirrors tests/test_cone_beam_fvr.py:179-205 set-up)
+    torch.manual_seed(17)
+    B_blk, N_pose, P, H, W = 4, 3, 24, 18, 20
+    imgs0 = torch.randn(B_blk, N_pose, P, P, dtype=torch.float32)
+    d_b0 = torch.full((B_blk, N_pose), 300.0) + torch.randn(B_blk, N_pose) * 15.0
+    cu0 = torch.randn(B_blk, N_pose) * 4.0
+    cv0 = torch.randn(B_blk, N_pose) * 4.0
+    rx_hw = torch.linspace(-0.08, 0.08, W).view(1, W).expand(H, W).contiguous()
+    ry_hw = torch.linspace(-0.07, 0.07, H).view(H, 1).expand(H, W).contiguous()
+    ic_hw = 1.0 / torch.sqrt((1.0 + rx_hw ** 2 + ry_hw ** 2)).clamp(min=0.1)
+    inv_ds, c_idx = 0.25, 12.0
+    t = [x.clone().requires_grad_(True) for x in (imgs0, d_b0, cu0, cv0)]
+    o = ts.pou_pinhole_warp_sum_torch(t[0], t[1], t[2], t[3], rx_hw, ry_hw, ic_hw, inv_ds, c_idx)
+    w2 = torch.randn_like(o)
+    (o * w2).sum().backward()
+    out.update(
+        warp_imgs=imgs0.numpy(), warp_db=d_b0.numpy(), warp_cu=cu0.numpy(), warp_cv=cv0.numpy(),
+        warp_rx=rx_hw.numpy(), warp_ry=ry_hw.numpy(), warp_ic=ic_hw.numpy(), warp_inv_ds=np.array(inv_ds),
+        warp_c_idx=np.array(c_idx), warp_out=o.detach().numpy(), warp_wout=w2.numpy(),
+        warp_g_imgs=t[0].grad.numpy(), warp_g_db=t[1].grad.numpy(), warp_g_cu=t[2].grad.numpy(),
+        warp_g_cv=t[3].grad.numpy(),
+    )
+    np.savez_compressed(HERE / "slice_warp.npz", **out)
+
+
+def gen_torch_engine(te):
+    import torch
+
+    out = {}
+    vol = _ellipsoids(20, 5, shape=(20, 18, 22))
+    spacing = (1.5, 1.5, 1.5)
+    eng = te.TorchDiffFVREngine(torch.from_numpy(vol), spacing=spacing, pad_factor=2.0, use_triton=False)
+    out["vol"] = vol
+    out["spacing0"] = np.array(spacing[0])
+    out["spectrum"] = eng.f_vol_5d[0].numpy()
+    poses = torch.tensor(
+        [[0.0, 0.0, 0.0, 0.0, 0.0, 0.0], [5.0, -3.0, 2.0, 4.0, -2.0, 1.0], [-7.5, 6.0, -4.0, -3.0, 2.5, -5.0]],
+        dtype=torch.float32,
+    )
+    out["poses"] = poses.numpy()
+    for view in ("ap", "lateral"):
+        for R in (20, 16):
+            with torch.no_grad():
+                out[f"slice_{view}_{R}"] = eng._extract_slice_spectrum(poses, view=view, out_res=R).numpy()
+                out[f"image_{view}_{R}"] = eng(poses, view=view, out_res=R).numpy()
+        # image-path autograd
+        p = poses.clone().requires_grad_(True)
+        img = eng(p, view=view, out_res=20)
+        w = torch.from_numpy(np.random.default_rng(3).standard_normal(img.shape).astype(np.float32))
+        (img * w).sum().backward()
+        out[f"image_w_{view}"] = w.numpy()
+        out[f"image_grad_{view}"] = p.grad.numpy()
+        # target + spectral NCC with autograd
+        tpose = torch.tensor([[2.0, -1.0, 1.5, 1.0, -0.5, 0.0]], dtype=torch.float32)
+        with torch.no_grad():
+            target = eng(tpose, view=view, out_res=20)
+            f_targ = eng.prepare_spectral_target(target, high_pass=True)
+            f_targ_nohp = eng.prepare_spectral_target(target, high_pass=False)
+        out[f"target_{view}"] = target.numpy()
+        out[f"ftarg_{view}"] = f_targ.numpy()
+        out[f"ftarg_nohp_{view}"] = f_targ_nohp.numpy()
+        p = poses.clone().requires_grad_(True)
+        loss = eng.forward_spectral_ncc(p, f_targ, view=view, high_pass=True)
+        loss.backward()
+        out[f"sncc_loss_{view}"] = loss.detach().numpy()
+        out[f"sncc_grad_{view}"] = p.grad.numpy()
+        p = poses.clone().requires_grad_(True)
+        loss = eng.forward_spectral_ncc(p, f_targ_nohp, view=view, high_pass=False)
+        loss.backward()
+        out[f"sncc_nohp_loss_{view}"] = loss.detach().numpy()
+        out[f"sncc_nohp_grad_{view}"] = p.grad.numpy()
+        # image-domain spectral NCC
+        pred = eng(poses, view=view, out_res=20).detach().requires_grad_(True)
+        l2 = eng.spectral_ncc_loss(pred, target, high_pass=True)
+        l2.backward()
+        out[f"incc_loss_{view}"] = l2.detach().numpy()
+        out[f"incc_grad_{view}"] = pred.grad.numpy()
+    # bf16 storage (CPU semantics: the stored spectrum is rounded, the slice is not)
+    eb = te.TorchDiffFVREngine(torch.from_numpy(vol), spacing=spacing, pad_factor=2.0, use_triton=False).to_precision(
+        torch.bfloat16
+    )
+    with torch.no_grad():
+        out["bf16_image_ap"] = eb(poses, view="ap", out_res=20).numpy()
+        out["bf16_spectrum"] = eb.f_vol_5d[0].float().numpy()
+    np.savez_compressed(HERE / "torch_engine.npz", **out)
+
+
+def gen_pou(cb):
+    import torch
+
+    out = {}
+    # PoU windows (cone_beam_fvr.py:42-61)
+    for length, k, ov in [(64, 2, 0.25), (96, 3, 0.25), (128, 4, 0.25), (192, 4, 0.5), (50, 3, 0.4)]:
+        ws, step = cb._make_pou_1d(length, k, ov)
+        out[f"pou1d_{length}_{k}_{ov}"] = torch.stack(ws).numpy()
+        out[f"pou1d_step_{length}_{k}_{ov}"] = np.array(step)
+    out["sinc2_12_24"] = cb._sinc2_precomp_1d(12, 24).numpy()
+
+    vol = _ellipsoids(28, 9, shape=(28, 26, 30))
+    out["vol"] = vol
+    fvr = cb.PerspectiveSlabFVR.from_volume(vol, vox_mm=2.0, grid_blocks=(2, 2, 2), block_res=12, overlap=0.25,
+                                            use_triton=False)
+    out["B"] = np.array(fvr.B)
+    out["P"] = np.array(fvr.P)
+    out["ds_block"] = np.array(fvr.ds_block)
+    out["centers"] = fvr.centers.numpy()
+    out["F_blk_ri"] = fvr.F_blk_ri.numpy()
+    out["FX_flat"] = fvr.FX_flat.numpy()
+    # a grid_center / 3-axis-different block grid build (centres only)
+    fvr2 = cb.PerspectiveSlabFVR.from_volume(vol, vox_mm=1.5, grid_blocks=(3, 2, 1), block_res=10, overlap=0.5,
+                                             center_mode="grid_center", use_triton=False)
+    out["g2_B"] = np.array(fvr2.B)
+    out["g2_centers"] = fvr2.centers.numpy()
+    out["g2_ds_block"] = np.array(fvr2.ds_block)
+    out["g2_F_blk_ri_sum"] = fvr2.F_blk_ri.double().sum(dim=(2, 3, 4)).numpy()
+
+    H, W = 24, 20
+    k_inv = torch.tensor(
+        [[1.0 / 300.0, 0.0, -W / 600.0], [0.0, 1.0 / 300.0, -H / 600.0], [0.0, 0.0, 1.0]], dtype=torch.float32
+    )
+    out["k_inv"] = k_inv.numpy()
+    lattice = fvr.make_pinhole_lattice(k_inv, sdd_mm=600.0, height=H, width=W)
+    for i, name in enumerate(["src0", "trg0", "u0", "v0", "n0", "rx", "ry", "ic"]):
+        out[f"lat_{name}"] = lattice[i].numpy()
+
+    def se3(rot_vec, trans):
+        skew = torch.zeros((rot_vec.shape[0], 3, 3), dtype=rot_vec.dtype)
+        skew[:, 0, 1], skew[:, 1, 0] = -rot_vec[:, 2], rot_vec[:, 2]
+        skew[:, 0, 2], skew[:, 2, 0] = rot_vec[:, 1], -rot_vec[:, 1]
+        skew[:, 1, 2], skew[:, 2, 1] = -rot_vec[:, 0], rot_vec[:, 0]
+        m = torch.eye(4, dtype=rot_vec.dtype).unsqueeze(0).repeat(rot_vec.shape[0], 1, 1)
+        m[:, :3, :3] = torch.matrix_exp(skew)
+        m[:, :3, 3] = trans
+        return m
+
+    rot0 = torch.tensor([[0.12, -0.08, 0.05], [-0.15, 0.10, -0.04], [0.0, 0.0, 0.0]], dtype=torch.float32)
+    xyz0 = torch.tensor([[4.0, -3.0, -300.0], [-2.0, 5.0, -310.0], [0.0, 0.0, -300.0]], dtype=torch.float32)
+    mats = se3(rot0, xyz0).detach()
+    out["mats"] = mats.numpy()
+    for tag, lat in (("inv", lattice), ("exp", lattice[:5])):
+        m = mats.clone().requires_grad_(True)
+        img = fvr.forward_pinhole(m, lat)
+        w = torch.from_numpy(np.random.default_rng(4).standard_normal(img.shape).astype(np.float32))
+        (img * w).sum().backward()
+        out[f"pin_{tag}_out"] = img.detach().numpy()
+        out[f"pin_{tag}_w"] = w.numpy()
+        out[f"pin_{tag}_gmats"] = m.grad.numpy()
+    # C-arm front-end (explicit rays) with autograd on the 6 scalars
+    for view in ("ap", "lateral"):
+        params = [torch.tensor(v, requires_grad=True) for v in (3.0, -2.0, 1.5, 1.0, -1.0, 0.5)]
+        img = fvr.forward_carm_view(*params, sad_mm=300.0, sdd_mm=600.0, det_px=20, det_fov_mm=70.0, view=view)
+        w = torch.from_numpy(np.random.default_rng(5).standard_normal(img.shape).astype(np.float32))
+        (img * w).sum().backward()
+        out[f"carm_{view}_out"] = img.detach().numpy()
+        out[f"carm_{view}_w"] = w.numpy()
+        out[f"carm_{view}_grad"] = np.array([float(p.grad) for p in params])
+    # edge-dominant NCC (fine only at H=48, multiscale at H=96)
+    rng = np.random.default_rng(6)
+    for Hs in (48, 96):
+        a = torch.from_numpy(rng.standard_normal((3, 1, Hs, Hs)).astype(np.float32)).cumsum(-1).requires_grad_(True)
+        a_leaf = a.detach().clone().requires_grad_(True)
+        b = torch.from_numpy(rng.standard_normal((3, 1, Hs, Hs)).astype(np.float32)).cumsum(-2)
+        val = cb.edge_dominant_ncc(a_leaf, b, reduction="none")
+        val.sum().backward()
+        out[f"edge_{Hs}_a"] = a_leaf.detach().numpy()
+        out[f"edge_{Hs}_b"] = b.numpy()
+        out[f"edge_{Hs}_val"] = val.detach().numpy()
+        out[f"edge_{Hs}_grad"] = a_leaf.grad.numpy()
+    np.savez_compressed(HERE / "pou.npz", **out)
+
+
+def gen_numpy(df, gr):
+    out = {}
+    vol = _ellipsoids(16, 7, shape=(16, 14, 18)).astype(np.float64)
+    out["vol"] = vol
+    ren = df.DifferentiableFourierVolumeRenderer(vol, pad_factor=2.0)
+    out["f_3d"] = ren.f_3d
+    ren_np = df.DifferentiableFourierVolumeRenderer(vol, pad_factor=2.0, apply_premultiplication=False)
+    out["f_3d_nopremult"] = ren_np.f_3d
+    pose = (3.0, -2.0, 1.5, 1.25, -0.75)
+    out["pose5"] = np.array(pose)
+    for view in ("ap", "lateral", "axial"):
+        out[f"slice_{view}"] = ren.extract_frequency_slice(*pose, view=view)
+        out[f"drr_{view}"] = ren.render_drr(*pose, view=view)
+        out[f"drr_nocrop_{view}"] = ren.render_drr(*pose, view=view, crop_to_roi=False)
+    t_ap = ren.extract_frequency_slice(0, 0, 0, view="ap")
+    t_lat = ren.extract_frequency_slice(0, 0, 0, view="lateral")
+    out["ncc_ap"] = np.array(ren.compute_spectral_ncc(out["slice_ap"], t_ap))
+    eng = gr.SpectralGradientEngine(ren)
+    test_pose = np.array([1.0, -1.0, 0.5, 1.5, -1.0, 2.0])
+    loss, grad = eng.compute_biplanar_loss_and_gradients(test_pose, t_ap, t_lat)
+    out["bip_pose"] = test_pose
+    out["bip_loss"] = np.array(loss)
+    out["bip_grad"] = grad
+    ncc, du, dv = eng.compute_spectral_ncc_and_grad_translation(out["slice_lateral"], t_lat, view="lateral")
+    out["tgrad"] = np.array([ncc, du, dv])
+    np.savez_compressed(HERE / "numpy_renderer.npz", **out)
+
+
+def main():
+    ref_root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import torch
+
+    torch.set_num_threads(4)
+    te, ts, cb, df, gr = _import_reference(ref_root)
+    gen_slice_and_warp(ts)
+    gen_torch_engine(te)
+    gen_pou(cb)
+    gen_numpy(df, gr)
+    for f in sorted(HERE.glob("*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

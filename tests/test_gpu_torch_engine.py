@@ -1,0 +1,305 @@
+"""GPU parity of the parallel-beam path (TorchDiffFVREngine drop-in), the FFT
+kernels and the drop-in slice gather, against the float64 oracle and the
+reference's golden vectors.
+
+Tolerances: FP32 path <= 1e-5 relative L2 against the float64 oracle; against
+the reference's own float32 outputs 2e-5 (the reference carries ~1e-5 of
+float32 interpolation noise, see test_oracle_golden.py); gradients 1e-4.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from oracle import torch_convention as tc
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda"
+
+
+def _t(a, dtype=torch.float32):
+    return torch.as_tensor(np.asarray(a), dtype=dtype, device=DEV)
+
+
+# ----------------------------------------------------------------------- FFT
+
+
+@pytest.mark.parametrize("shape", [(8, 12, 10), (20, 18, 22), (24, 16, 30), (13, 7, 11), (30, 35, 26)])
+def test_spectrum3d_torch_and_numpy_conventions(shape):
+    from fvr import _runtime as RT
+    from fvr import _lib as L
+
+    rng = np.random.default_rng(1)
+    vol = rng.standard_normal(shape).astype(np.float32)
+    pad = tc.padded_shape(shape, 2.0)
+    got = RT.spectrum3d(_t(vol), pad, 0).cpu().numpy()
+    ref = tc.spectrum(vol, 2.0)
+    assert rel_l2(got, ref[0] + 1j * ref[1]) < 2e-6
+    # numpy convention in fp64: pad, ifftshift, fftn, fftshift
+    padded = np.zeros(pad)
+    lo = [(p - n) // 2 for p, n in zip(pad, shape)]
+    padded[lo[0]:lo[0] + shape[0], lo[1]:lo[1] + shape[1], lo[2]:lo[2] + shape[2]] = vol
+    ref2 = np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(padded)))
+    got2 = RT.spectrum3d(_t(vol, torch.float64), pad, 1, prec=L.F64_).cpu().numpy()
+    assert rel_l2(got2, ref2) < 1e-13
+
+
+@pytest.mark.parametrize("n0,n1", [(16, 16), (20, 24), (48, 45), (96, 192), (128, 128), (26, 14)])
+def test_fft2d_shifts_scales_and_real_outputs(n0, n1):
+    from fvr import _runtime as RT
+
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((3, n0, n1)) + 1j * rng.standard_normal((3, n0, n1))
+    xt = torch.as_tensor(x.astype(np.complex64), device=DEV)
+    got = RT.fft2d(xt.clone(), inverse=False, out_shift=RT.SHIFT_FFT).cpu().numpy()
+    assert rel_l2(got, np.fft.fftshift(np.fft.fft2(x), axes=(-2, -1))) < 2e-6
+    got = RT.fft2d(xt.clone(), inverse=True, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT,
+                   scale=1.0 / (n0 * n1)).cpu().numpy()
+    ref = np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(x, axes=(-2, -1))), axes=(-2, -1))
+    assert rel_l2(got, ref) < 2e-6
+    got = RT.fft2d(xt.clone(), inverse=True, in_shift=RT.SHIFT_IFFT, scale=1.0 / (n0 * n1),
+                   out_mode=RT.OUT_RELU).cpu().numpy()
+    ref = np.maximum(np.fft.ifft2(np.fft.ifftshift(x, axes=(-2, -1))).real, 0)
+    assert rel_l2(got, ref) < 2e-6
+    # real input, crop window
+    r = rng.standard_normal((2, n0, n1))
+    got = RT.fft2d(torch.as_tensor(r, device=DEV), inverse=True, out_mode=RT.OUT_REAL, scale=0.5,
+                   crop=(1, n0 - 2, 2, n1 - 3)).cpu().numpy()
+    ref = (np.fft.ifft2(r) * n0 * n1 * 0.5).real[:, 1:n0 - 1, 2:n1 - 1]
+    assert rel_l2(got, ref) < 1e-12
+
+
+# ------------------------------------------------------------- slice gather
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+def test_fourier_slice_3d_dropin_vs_golden(golden, dtype):
+    from fvr.triton_slice import fourier_slice_3d
+
+    g = golden("slice_warp")
+    vol = _t(g["slice_vol"]).to(dtype)
+    u = _t(g["slice_u"]).requires_grad_(True)
+    v = _t(g["slice_v"]).requires_grad_(True)
+    out = fourier_slice_3d(vol, u, v, _t(g["slice_fx"]), _t(g["slice_fy"]), tuple(g["slice_center"]))
+    assert out.dtype == dtype and out.shape == g["slice_out"].shape
+    (out.float() * _t(g["slice_wout"])).sum().backward()
+    if dtype == torch.float32:
+        assert rel_l2(out.detach().cpu().numpy(), g["slice_out"]) < 2e-5
+        ref = tc.fourier_slice_3d(g["slice_vol"], g["slice_u"], g["slice_v"], g["slice_fx"], g["slice_fy"],
+                                  g["slice_center"])
+        assert rel_l2(out.detach().cpu().numpy(), ref) < 1e-5
+        assert rel_l2(u.grad.cpu().numpy(), g["slice_gu"]) < 1e-4
+        assert rel_l2(v.grad.cpu().numpy(), g["slice_gv"]) < 1e-4
+    else:
+        vb = vol.float().cpu().numpy()
+        ref = tc.fourier_slice_3d(vb, g["slice_u"], g["slice_v"], g["slice_fx"], g["slice_fy"], g["slice_center"])
+        # output rounded to bf16 like the reference's fused path (triton_slice.py:142-143)
+        assert rel_l2(out.detach().float().cpu().numpy(), ref) < 4e-3
+
+
+# ---------------------------------------------------------- torch engine
+
+
+@pytest.fixture(scope="module")
+def engine(golden):
+    from fvr.torch_engine import TorchDiffFVREngine
+
+    g = golden("torch_engine")
+    return TorchDiffFVREngine(torch.from_numpy(g["vol"]), spacing=(1.5, 1.5, 1.5), pad_factor=2.0)
+
+
+def test_engine_spectrum_matches_reference(engine, golden):
+    g = golden("torch_engine")
+    assert tuple(engine.f_vol_5d.shape) == (1,) + g["spectrum"].shape
+    assert rel_l2(engine.f_vol_5d[0].cpu().numpy(), g["spectrum"]) < 2e-6
+
+
+@pytest.mark.parametrize("view", ["ap", "lateral"])
+@pytest.mark.parametrize("R", [20, 16])
+def test_engine_slice_and_image(engine, golden, view, R):
+    g = golden("torch_engine")
+    poses = _t(g["poses"])
+    s = engine._extract_slice_spectrum(poses, view=view, out_res=R).cpu().numpy()
+    spec = tc.spectrum(g["vol"], 2.0)
+    assert rel_l2(s, tc.extract_slice_spectrum(spec, g["poses"], view, R, 1.5)) < 1e-5
+    assert rel_l2(s, g[f"slice_{view}_{R}"]) < 2e-5
+    img = engine(poses, view=view, out_res=R)
+    assert tuple(img.shape) == (3, 1, R, R) and img.dtype == torch.float32
+    img = img.cpu().numpy()
+    assert rel_l2(img, tc.forward_image(spec, g["poses"], view, R, 1.5)) < 1e-5
+    assert rel_l2(img, g[f"image_{view}_{R}"]) < 2e-5
+
+
+def _mask(grad):
+    m = np.ones(grad.shape, bool)
+    m[0, 0] = False  # identity pose: lattice-point kink, see test_oracle_golden._grad_mask
+    return m
+
+
+@pytest.mark.parametrize("view", ["ap", "lateral"])
+@pytest.mark.parametrize("high_pass", [True, False])
+def test_engine_spectral_ncc_loss_and_grad(engine, golden, view, high_pass):
+    g = golden("torch_engine")
+    tgt = _t(g[f"target_{view}"])
+    f_targ = engine.prepare_spectral_target(tgt, high_pass=high_pass)
+    key = "ftarg" if high_pass else "ftarg_nohp"
+    assert rel_l2(f_targ.cpu().numpy(), g[f"{key}_{view}"]) < 2e-6
+    poses = _t(g["poses"]).requires_grad_(True)
+    loss = engine.forward_spectral_ncc(poses, f_targ, view=view, high_pass=high_pass)
+    loss.backward()
+    lk = "sncc_loss" if high_pass else "sncc_nohp_loss"
+    gk = "sncc_grad" if high_pass else "sncc_nohp_grad"
+    assert abs(float(loss) - float(g[f"{lk}_{view}"])) < 3e-6
+    spec = tc.spectrum(g["vol"], 2.0)
+    ft = tc.prepare_spectral_target(g[f"target_{view}"], high_pass)
+    ref_loss, _ = tc.spectral_ncc(spec, g["poses"], ft, view, high_pass, 4.0, 1.5)
+    assert abs(float(loss) - ref_loss) < 2e-6
+    grad = poses.grad.cpu().numpy()
+    m = _mask(grad)
+    ref_grad = tc.spectral_ncc_grad(spec, g["poses"], ft, view, high_pass, 4.0, 1.5)
+    assert rel_l2(grad[m], ref_grad[m]) < 1e-4
+    assert rel_l2(grad[m], g[f"{gk}_{view}"][m]) < 1e-4
+    assert np.all(grad[:, 5] == 0)
+
+
+@pytest.mark.parametrize("view", ["ap", "lateral"])
+def test_engine_image_grad(engine, golden, view):
+    g = golden("torch_engine")
+    poses = _t(g["poses"]).requires_grad_(True)
+    img = engine(poses, view=view, out_res=20)
+    (img * _t(g[f"image_w_{view}"])).sum().backward()
+    grad = poses.grad.cpu().numpy()
+    m = _mask(grad)
+    spec = tc.spectrum(g["vol"], 2.0)
+    ref = tc.forward_image_grad(spec, g["poses"], g[f"image_w_{view}"], view, 20, 1.5)
+    assert rel_l2(grad[m], ref[m]) < 1e-4
+    assert rel_l2(grad[m], g[f"image_grad_{view}"][m]) < 1e-4
+
+
+@pytest.mark.parametrize("view", ["ap", "lateral"])
+def test_engine_image_domain_spectral_ncc(engine, golden, view):
+    g = golden("torch_engine")
+    pred = engine(_t(g["poses"]), view=view, out_res=20).detach().requires_grad_(True)
+    loss = engine.spectral_ncc_loss(pred, _t(g[f"target_{view}"]), high_pass=True)
+    loss.backward()
+    assert abs(float(loss) - float(g[f"incc_loss_{view}"])) < 3e-6
+    assert rel_l2(pred.grad.cpu().numpy(), g[f"incc_grad_{view}"]) < 1e-4
+
+
+def test_engine_bf16_storage(golden):
+    from fvr.torch_engine import TorchDiffFVREngine
+
+    g = golden("torch_engine")
+    eng = TorchDiffFVREngine(torch.from_numpy(g["vol"]), spacing=(1.5, 1.5, 1.5)).to_precision(torch.bfloat16)
+    assert eng.f_vol_5d.dtype == torch.bfloat16
+    assert rel_l2(eng.f_vol_5d[0].float().cpu().numpy(), g["bf16_spectrum"]) < 1e-6
+    img = eng(_t(g["poses"]), view="ap", out_res=20)
+    assert img.dtype == torch.float32
+    assert rel_l2(img.cpu().numpy(), g["bf16_image_ap"]) < 2e-5
+
+
+# --------------------------------------------- full-size properties (cfg 2)
+
+
+@pytest.fixture(scope="module")
+def big():
+    from fvr.torch_engine import TorchDiffFVREngine
+
+    vol = tc.make_ellipsoid_volume(128, 0)
+    eng = TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0)
+    spec = tc.spectrum(vol, 2.0)
+    return vol, eng, spec
+
+
+def test_full_size_spectral_ncc_subset_vs_oracle(big):
+    """128^3 -> 256^3 spectrum, R = 128: 4 of the 64 candidates against the oracle."""
+    vol, eng, spec = big
+    poses = tc.make_poses(4, 1)
+    tp = tc.make_poses(1, 2)
+    for view in ("ap", "lateral"):
+        tgt = tc.forward_image(spec, tp, view, 128, 1.0)
+        ft = tc.prepare_spectral_target(tgt)
+        f_t = eng.prepare_spectral_target(_t(tgt))
+        assert rel_l2(f_t.cpu().numpy(), ft) < 2e-6
+        p = _t(poses).requires_grad_(True)
+        loss = eng.forward_spectral_ncc(p, f_t, view=view)
+        loss.backward()
+        ref_loss, _ = tc.spectral_ncc(spec, poses, ft, view, True, 4.0, 1.0)
+        assert abs(float(loss) - ref_loss) < 2e-6
+        ref_grad = tc.spectral_ncc_grad(spec, poses, ft, view, True, 4.0, 1.0)
+        assert rel_l2(p.grad.cpu().numpy(), ref_grad) < 1e-4
+        img = eng(_t(poses), view=view, out_res=128).cpu().numpy()
+        assert rel_l2(img, tc.forward_image(spec, poses, view, 128, 1.0)) < 1e-5
+
+
+def test_batched_equals_single_candidate(big):
+    """Each candidate's loss and gradient are independent of the batch it rides in."""
+    vol, eng, spec = big
+    poses = _t(tc.make_poses(16, 3))
+    f_t = eng.prepare_spectral_target(eng(_t(tc.make_poses(1, 4)), view="ap", out_res=128))
+    pb = poses.clone().requires_grad_(True)
+    (eng.forward_spectral_ncc(pb, f_t) * 16).backward()
+    for i in (0, 7, 15):
+        ps = poses[i:i + 1].clone().requires_grad_(True)
+        eng.forward_spectral_ncc(ps, f_t).backward()
+        assert torch.allclose(pb.grad[i], ps.grad[0], rtol=1e-5, atol=1e-9)
+
+
+@pytest.mark.parametrize("dtype,bound", [(torch.bfloat16, 1e-3), (torch.float16, 1e-3)])
+def test_reduced_precision_error_bound_vs_fp64(big, dtype, bound):
+    """Reduced-precision spectrum: relative image error vs the FP64 oracle <= 1e-3."""
+    from fvr.torch_engine import TorchDiffFVREngine
+
+    vol, _, spec = big
+    eng = TorchDiffFVREngine(torch.from_numpy(vol)).to_precision(dtype)
+    poses = tc.make_poses(4, 5)
+    for view in ("ap", "lateral"):
+        img = eng(_t(poses), view=view, out_res=128).cpu().numpy()
+        err = rel_l2(img, tc.forward_image(spec, poses, view, 128, 1.0))
+        assert err < bound, (dtype, view, err)
+
+
+def test_reference_test_mirror_adam_descends(big):
+    """Mirror of tests/test_torch_engine.py:61-110 of the reference."""
+    _, eng, _ = big
+    true_pose = torch.zeros(1, 6, device=DEV)
+    with torch.no_grad():
+        target = eng(true_pose, view="ap", out_res=64)
+        f_targ = eng.prepare_spectral_target(target, high_pass=True)
+    est = torch.tensor([[2.5, -1.5, 0.5, 3.0, -2.5, 0.0]], device=DEV, requires_grad=True)
+    opt = torch.optim.Adam([est], lr=0.2)
+    losses = []
+    for _ in range(12):
+        opt.zero_grad()
+        loss = eng.forward_spectral_ncc(est, f_targ, view="ap", high_pass=True)
+        loss.backward()
+        opt.step()
+        losses.append(float(loss))
+    assert losses[-1] < losses[0]
+    est2 = torch.tensor([[2.0, -1.5, 0.0, 3.0, -2.0, 0.0]], device=DEV, requires_grad=True)
+    opt = torch.optim.Adam([est2], lr=0.15)
+    losses = []
+    for _ in range(12):
+        opt.zero_grad()
+        loss = eng.spectral_ncc_loss(eng(est2, view="ap", out_res=64), target, high_pass=True)
+        loss.backward()
+        opt.step()
+        losses.append(float(loss))
+    assert losses[-1] < losses[0]
+    assert bool(torch.all(torch.isfinite(est2.grad)))
+
+
+def test_cpu_inputs_are_moved_and_outputs_finite(big):
+    """Mirror of tests/test_torch_engine.py:29-59 with CPU poses."""
+    _, eng, _ = big
+    poses = torch.tensor([[0.0, 0, 0, 0, 0, 0], [5.0, 0, 0, 0, 0, 0], [0, 5.0, 0, 0, 0, 0],
+                          [2.0, -3.0, 1.5, 4.0, -2.0, 1.0]])
+    for view in ("ap", "lateral"):
+        d = eng(poses, view=view, out_res=64)
+        assert d.shape == (4, 1, 64, 64)
+        assert bool(torch.all(torch.isfinite(d))) and bool(torch.all(d >= 0))
+    pose = torch.tensor([[3.0, -2.0, 1.0, 5.0, -3.0, 2.0]], requires_grad=True)
+    (eng(pose, view="ap", out_res=64) ** 2).sum().backward()
+    assert pose.grad.shape == (1, 6) and bool(torch.all(torch.isfinite(pose.grad)))
+    assert not bool(torch.all(pose.grad == 0))
