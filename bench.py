@@ -111,41 +111,40 @@ class ClockSampler:
 
 
 def _setup(torch, dev):
-    from oracle import torch_convention as tc  # seeded inputs only (generator), not timed
     import fvr
-    from fvr import _runtime as RT
+    from fvr import synthetic
 
-    vol = tc.make_ellipsoid_volume(VOL_N, SEED)
-    poses = tc.make_poses(CANDIDATES, SEED + 1)
-    tpose = tc.make_poses(1, SEED + 2)
+    vol = synthetic.make_ellipsoid_volume(VOL_N, SEED)
+    poses = synthetic.make_poses(CANDIDATES, SEED + 1)
+    tpose = synthetic.make_poses(1, SEED + 2)
     eng = fvr.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0, device=dev)
     with torch.no_grad():
         t_ap = eng(torch.from_numpy(tpose).to(dev), view="ap", out_res=OUT_RES)
         t_lat = eng(torch.from_numpy(tpose).to(dev), view="lateral", out_res=OUT_RES)
     f_ap = eng.prepare_spectral_target(t_ap)
     f_lat = eng.prepare_spectral_target(t_lat)
-    return vol, poses, eng, f_ap, f_lat, (t_ap, t_lat), tc, RT
+    return vol, poses, eng, f_ap, f_lat
 
 
-def _time_steps(torch, fn, steps, flush, stream=None):
-    """Per-step device time with CUDA events; L2 flushed (256 MiB write) before each step."""
-    times = []
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    for k in range(steps):
+def _time_steps(torch, fn, steps, flush, timer=None, name=None):
+    """Per-step device time with CUDA events; L2 flushed (256 MiB write) before
+    each step.  With a LaunchTimer the named kernel's launches are timed too."""
+    step_ms, kern_ms = [], []
+    for _ in range(steps):
         flush.add_(1)
-        a, b = ev[k]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         fn()
         b.record()
-    torch.cuda.synchronize()
-    for a, b in ev:
-        times.append(a.elapsed_time(b))
-    return times
+        b.synchronize()
+        step_ms.append(a.elapsed_time(b))
+        if timer is not None:
+            kern_ms.extend(timer.durations_ms(name))
+    return step_ms, kern_ms
 
 
 def run_b200(args, torch):
     import torch.distributed as dist
-    from fvr import _lib as L
     from fvr import profiling
     from fvr.graphs import BiplanarSpectralNCCStep
 
@@ -156,128 +155,92 @@ def run_b200(args, torch):
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-    vol, poses_np, eng, f_ap, f_lat, targets, tc, RT = _setup(torch, dev)
+    vol, poses_np, eng, f_ap, f_lat = _setup(torch, dev)
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
     poses = torch.from_numpy(poses_np).to(dev)
+    sub = torch.from_numpy(poses_np[:4]).to(dev)
     K, W = args.steps, args.warmup
+    out = {}
 
-    # --- FP32 single-candidate eager path (the plain baseline of the target) -----------
-    def eager_step(e, p):
+    # FP32 single-candidate eager path through the reference API (the plain baseline)
+    def eager_step(p):
         pp = p.detach().requires_grad_(True)
-        loss = e.forward_spectral_ncc(pp, f_ap, view="ap") + e.forward_spectral_ncc(pp, f_lat, view="lateral")
+        loss = eng.forward_spectral_ncc(pp, f_ap, view="ap") + eng.forward_spectral_ncc(pp, f_lat, view="lateral")
         loss.backward()
         return loss, pp.grad
 
     p1 = poses[:1].clone()
     for _ in range(W):
-        eager_step(eng, p1)
-    t_single = _time_steps(torch, lambda: eager_step(eng, p1), K, flush)
+        eager_step(p1)
+    t_single, _ = _time_steps(torch, lambda: eager_step(p1), K, flush)
 
-    # --- FP32 batched, graph-captured ---------------------------------------------------------
-    step32 = BiplanarSpectralNCCStep(eng, f_ap, f_lat, CANDIDATES, warmup=W)
-    loss32, grad32 = step32(poses)
-    grad32 = grad32.clone()
-    t32 = _time_steps(torch, step32._g.replay, K, flush)
-    sub = poses_np[:4]
-    img32 = {v: eng(torch.from_numpy(sub).to(dev), view=v, out_res=OUT_RES).cpu().numpy() for v in ("ap", "lateral")}
-    del step32
+    # batched, graph-captured, per storage precision; the headline (16-bit
+    # brick-scaled f16) last, with the hot kernel timed inside the graph
+    results = {}
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
+        if name != "f32":
+            eng.to_precision(dt) if name == "bf16" else _f16_from_f32(eng, vol, dev, torch)
+        timer = profiling.LaunchTimer(["tc_sncc_moments"], capacity=4)
+        step = BiplanarSpectralNCCStep(eng, f_ap, f_lat, CANDIDATES, warmup=W, capture_context=timer)
+        loss, grad = step(poses)
+        res = {"loss": float(loss), "grad": grad.detach().cpu().numpy().copy(),
+               "img": {v: eng(sub, view=v, out_res=OUT_RES).cpu().numpy() for v in ("ap", "lateral")},
+               "kernels_per_step": step._g.kernels_per_replay}
+        for _ in range(W):
+            step._g.replay()
+        if name == "f16":
+            clocks = ClockSampler(local)
+            clocks.start()
+            if ws > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+        st, km = _time_steps(torch, step._g.replay, K, flush, timer, "tc_sncc_moments")
+        torch.cuda.synchronize()
+        if name == "f16":
+            if ws > 1:
+                dist.barrier()
+            res["clocks"] = clocks.stop()
+            res["step_obj"] = step
+        res["step_ms"], res["kern_ms"] = st, km
+        results[name] = res
 
-    # --- BF16 batched, graph-captured (headline) ----------------------------------------------
-    eng.to_precision(torch.bfloat16)
-    timer = profiling.LaunchTimer(["tc_sncc_moments"], capacity=4)
-    step16 = BiplanarSpectralNCCStep(eng, f_ap, f_lat, CANDIDATES, warmup=W, capture_context=timer)
-    kernels_per_step = step16._g.kernels_per_replay
-    loss16, grad16 = step16(poses)
-    grad16 = grad16.clone()
-    img16 = {v: eng(torch.from_numpy(sub).to(dev), view=v, out_res=OUT_RES).cpu().numpy() for v in ("ap", "lateral")}
-    for _ in range(W):
-        step16._g.replay()
-    clocks = ClockSampler(local)
-    clocks.start()
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    step_ms, kern_ms = [], []
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    for k in range(K):
-        flush.add_(1)
-        a, b = ev[k]
-        a.record()
-        step16._g.replay()
-        b.record()
-        b.synchronize()
-        step_ms.append(a.elapsed_time(b))
-        kern_ms.extend(timer.durations_ms("tc_sncc_moments"))
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    total_ms = float(sum(step_ms))
+    f16 = results["f16"]
+    total_ms = float(sum(f16["step_ms"]))
     if ws > 1:
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    ms_per_step = total_ms / K
     value = ws * CANDIDATES * K / (total_ms / 1e3)
+    step16 = f16.pop("step_obj")
 
-    # --- e2e through the public step API with host buffers ---------------------------------
+    # e2e through the public step API with pinned host buffers
     h_poses = torch.from_numpy(poses_np).pin_memory()
     h_loss = torch.empty((), dtype=torch.float32).pin_memory()
     h_grad = torch.empty((CANDIDATES, 6), dtype=torch.float32).pin_memory()
 
     def e2e_step():
-        loss, grad = step16(h_poses.to(dev, non_blocking=True))
-        h_loss.copy_(loss, non_blocking=True)
-        h_grad.copy_(grad, non_blocking=True)
+        lo, gr = step16(h_poses.to(dev, non_blocking=True))
+        h_loss.copy_(lo, non_blocking=True)
+        h_grad.copy_(gr, non_blocking=True)
 
     for _ in range(W):
         e2e_step()
-    t_e2e = _time_steps(torch, e2e_step, K, flush)
-    e2e_ms = statistics.mean(t_e2e)
+    t_e2e, _ = _time_steps(torch, e2e_step, K, flush)
 
-    # eager public API (no graph), host buffers, for reference
     def e2e_eager():
-        lo, gr = eager_step(eng, h_poses.to(dev, non_blocking=True))
+        lo, gr = eager_step(h_poses.to(dev, non_blocking=True))
         h_loss.copy_(lo.detach(), non_blocking=True)
         h_grad.copy_(gr, non_blocking=True)
 
     for _ in range(W):
         e2e_eager()
-    t_eager = _time_steps(torch, e2e_eager, K, flush)
+    t_eager, _ = _time_steps(torch, e2e_eager, K, flush)
 
     res = None
     if rank == 0:
-        # --- accuracy vs the FP64 oracle -------------------------------------------------
-        from oracle import c_oracle
-
-        spec = tc.spectrum(vol, 2.0)
-        hp = tc.hp_filter(OUT_RES, OUT_RES, 4.0)
-        ref_grad = np.zeros((CANDIDATES, 6))
-        ref_loss = 0.0
-        for view, ft in (("ap", f_ap), ("lateral", f_lat)):
-            lo, _, gr = c_oracle.sncc(spec, poses_np, ft.cpu().numpy(), view, hp, 1.0)
-            ref_grad += gr
-            ref_loss += lo
-
-        def rel(a, b):
-            return float(np.linalg.norm(a - b) / np.linalg.norm(b))
-
-        img_err = {}
-        for name, imgs in (("f32", img32), ("bf16", img16)):
-            img_err[name] = max(rel(imgs[v], tc.forward_image(spec, sub, v, OUT_RES, 1.0)) for v in ("ap", "lateral"))
-        acc = {
-            "bf16": {"grad_rel_l2": rel(grad16.cpu().numpy(), ref_grad), "loss_abs": abs(float(loss16) - ref_loss),
-                     "image_rel_l2": img_err["bf16"]},
-            "f32": {"grad_rel_l2": rel(grad32.cpu().numpy(), ref_grad), "loss_abs": abs(float(loss32) - ref_loss),
-                    "image_rel_l2": img_err["f32"]},
-            "oracle": "float64 C/NumPy oracle, all 64 candidates (gradient) / 4 candidates (image)",
-        }
-
-        # --- roofline of the dominant kernel --------------------------------------------
         peak, peak_kind = _peak_hbm()
-        kern_avg_ms = statistics.mean(kern_ms) if kern_ms else float("nan")
-        bytes_per_sample = 32 + 8  # bf16 stencil entry (8 complex corners) + complex64 target sample
-        alg_bytes = CANDIDATES * OUT_RES * OUT_RES * bytes_per_sample
+        kern_avg_ms = statistics.mean(f16["kern_ms"])
+        alg_bytes = 2 * CANDIDATES * OUT_RES * OUT_RES * (32 + 8)
         achieved = alg_bytes / (kern_avg_ms * 1e-3) / 1e9
         traffic = None
         tf = REPO / "profiles" / "tc_sncc_moments_cfg2_traffic.txt"
@@ -285,20 +248,7 @@ def run_b200(args, torch):
             for line in tf.read_text().splitlines():
                 if line.startswith("dram_bytes_per_launch:"):
                     traffic = float(line.split(":", 1)[1])
-
-        # --- CPU baseline: the C oracle on this host, one full step ------------------------
-        ncores = os.cpu_count() or 1
-        t0 = time.perf_counter()
-        reps = 0
-        while True:
-            for view, ft in (("ap", f_ap), ("lateral", f_lat)):
-                c_oracle.sncc(spec, poses_np, ft.cpu().numpy(), view, hp, 1.0, threads=ncores)
-            reps += 1
-            if time.perf_counter() - t0 > 5.0 or reps >= 10:
-                break
-        cpu_s = (time.perf_counter() - t0) / reps
-        cpu_value = CANDIDATES / cpu_s
-
+        cpu = _cpu_baseline_leg(vol, poses_np, f_ap, f_lat, results)
         single_value = 1.0 / (statistics.mean(t_single) / 1e3)
         res = {
             "metric": METRIC,
@@ -307,7 +257,7 @@ def run_b200(args, torch):
             "n_gpus": ws,
             "steps": K,
             "warmup": W,
-            "ms_per_step": ms_per_step,
+            "ms_per_step": total_ms / K,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -320,46 +270,105 @@ def run_b200(args, torch):
                 "candidates_per_gpu": CANDIDATES,
                 "views": 2,
                 "out_res": OUT_RES,
-                "spectrum_storage": "bf16 stencil (8 corners per 32-byte entry), f32 interpolation/accumulation",
-                "step": "CUDA-graph replay of forward_spectral_ncc(AP) + forward_spectral_ncc(lateral) + backward",
+                "spectrum_storage": "f16 stencil with per-16^3-brick power-of-two scales (32-byte entry of 8 "
+                                    "complex corners); f32 interpolation, fp64 positions and reductions",
+                "step": "CUDA-graph replay: fused gather+NCC moments for both views, fp64 finalize, fp64 pose "
+                        "gradient (3 kernels)",
                 "l2": "flushed before every timed step (256 MiB write)",
                 "parallelism": f"replicas x{ws}",
             },
-            "fp32": {"value": CANDIDATES * K / (sum(t32) / 1e3), "ms_per_step": statistics.mean(t32)},
+            "precisions": {
+                n: {"value": CANDIDATES * K / (sum(r["step_ms"]) / 1e3), "ms_per_step": statistics.mean(r["step_ms"]),
+                    "kernel_ms": statistics.mean(r["kern_ms"]), **cpu["accuracy"][n]}
+                for n, r in results.items()
+            },
             "fp32_single_candidate_eager": {"value": single_value, "ms_per_step": statistics.mean(t_single)},
-            "bf16_batched_over_fp32_single": value / ws / single_value,
-            "accuracy_vs_fp64": acc,
+            "f16_batched_over_fp32_single": value / ws / single_value,
             "roofline": {
                 "bound": "hbm",
-                "kernel": "tc_sncc_moments_kernel<bf16, grad>",
+                "kernel": "tc_sncc_moments_kernel<f16, grad> (both views, 64 candidates)",
                 "achieved": achieved,
                 "peak": peak,
                 "unit": "GB/s",
                 "frac": achieved / peak,
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6.65 TB/s",
                 "traffic": traffic,
                 "alg_bytes_per_launch": alg_bytes,
-                "alg_bytes_note": "64 candidates x 16384 samples x (32 B bf16 stencil entry + 8 B target)",
+                "alg_bytes_note": "2 views x 64 candidates x 16384 samples x (32 B stencil entry + 8 B target)",
                 "kernel_ms": kern_avg_ms,
-                "kernel_launches_timed": len(kern_ms),
+                "kernel_launches_timed": len(f16["kern_ms"]),
             },
-            "cpu_baseline": {"value": cpu_value, "unit": UNIT, "cores": ncores, "kind": "port",
-                             "sample": "one full step (64 candidates x 2 views, loss + gradient) of the float64 "
-                                       f"C/OpenMP oracle, mean of {reps} runs"},
-            "e2e": {"value": CANDIDATES * ws / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h_poses.numel() * 4),
-                    "d2h_bytes_per_step": int(4 + h_grad.numel() * 4),
+            "cpu_baseline": cpu["baseline"],
+            "e2e": {"value": CANDIDATES * ws / (statistics.mean(t_e2e) / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h_poses.numel() * 4), "d2h_bytes_per_step": int(4 + h_grad.numel() * 4),
                     "api": "fvr.graphs.BiplanarSpectralNCCStep (pinned host poses in, loss + grad out)",
-                    "eager_api_value": CANDIDATES / (statistics.mean(t_eager) / 1e3)},
-            "gpu_launches": int(kernels_per_step * K),
-            "kernels_per_step": int(kernels_per_step),
-            "clocks": clk,
+                    "eager_api_value": CANDIDATES / (statistics.mean(t_eager) / 1e3),
+                    "eager_api": "forward_spectral_ncc(ap) + forward_spectral_ncc(lateral) + backward()"},
+            "gpu_launches": int(f16["kernels_per_step"] * K),
+            "kernels_per_step": int(f16["kernels_per_step"]),
+            "clocks": f16["clocks"],
         }
     if ws > 1:
         dist.barrier()
         del step16
         dist.destroy_process_group()
     return res
+
+
+def _f16_from_f32(eng, vol, dev, torch):
+    """Brick-scaled f16 stencil built from the full-precision spectrum (the bf16
+    cast before this is lossy, so rebuild the engine's spectrum first)."""
+    import fvr
+
+    fresh = fvr.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0, device=dev)
+    fresh.to_precision(torch.float16)
+    eng._stencil = fresh._stencil
+    eng.f_vol_5d = fresh.f_vol_5d
+
+
+def _cpu_baseline_leg(vol, poses_np, f_ap, f_lat, results):
+    """The reference's CPU path on this host (float64 C/OpenMP oracle), timed on
+    one full step; the same FP64 run is the accuracy reference of every GPU
+    precision."""
+    from oracle import c_oracle
+    from oracle import torch_convention as tc
+
+    spec = tc.spectrum(vol, 2.0)
+    hp = tc.hp_filter(OUT_RES, OUT_RES, 4.0)
+    fts = {"ap": f_ap.cpu().numpy(), "lateral": f_lat.cpu().numpy()}
+    ncores = os.cpu_count() or 1
+    ref_grad = np.zeros((CANDIDATES, 6))
+    ref_loss = 0.0
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        ref_grad[:] = 0.0
+        ref_loss = 0.0
+        for view in ("ap", "lateral"):
+            lo, _, gr = c_oracle.sncc(spec, poses_np, fts[view], view, hp, 1.0, threads=ncores)
+            ref_grad += gr
+            ref_loss += lo
+        reps += 1
+        if time.perf_counter() - t0 > 5.0 or reps >= 10:
+            break
+    cpu_s = (time.perf_counter() - t0) / reps
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    sub = poses_np[:4]
+    ref_img = {v: tc.forward_image(spec, sub, v, OUT_RES, 1.0) for v in ("ap", "lateral")}
+    acc = {}
+    for n, r in results.items():
+        acc[n] = {"grad_rel_l2_vs_fp64": rel(r["grad"], ref_grad), "loss_abs_err": abs(r["loss"] - ref_loss),
+                  "image_rel_l2_vs_fp64": max(rel(r["img"][v], ref_img[v]) for v in ("ap", "lateral"))}
+    return {
+        "baseline": {"value": CANDIDATES / cpu_s, "unit": UNIT, "cores": ncores, "kind": "port",
+                     "sample": "one full step (64 candidates x 2 views, loss + gradient) of the float64 C/OpenMP "
+                               f"oracle, mean of {reps} runs"},
+        "accuracy": acc,
+    }
 
 
 def run_reference(args):
@@ -369,12 +378,13 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return None
+    from fvr import synthetic
     from oracle import c_oracle
     from oracle import torch_convention as tc
 
-    vol = tc.make_ellipsoid_volume(VOL_N, SEED)
-    poses = tc.make_poses(CANDIDATES, SEED + 1)
-    tpose = tc.make_poses(1, SEED + 2)
+    vol = synthetic.make_ellipsoid_volume(VOL_N, SEED)
+    poses = synthetic.make_poses(CANDIDATES, SEED + 1)
+    tpose = synthetic.make_poses(1, SEED + 2)
     spec = tc.spectrum(vol, 2.0)
     hp = tc.hp_filter(OUT_RES, OUT_RES, 4.0)
     fts = {v: tc.prepare_spectral_target(tc.forward_image(spec, tpose, v, OUT_RES, 1.0)) for v in ("ap", "lateral")}

@@ -33,41 +33,6 @@ struct Sample8 {
   float re[8], im[8];
 };
 
-template <int DT>
-__device__ __forceinline__ void stencil_load(const Stencil& s, int ez, int ey, int ex, Sample8& v) {
-  const int64_t e = (static_cast<int64_t>(ez) * (s.H + 1) + ey) * (s.W + 1) + ex;
-  if constexpr (DT == FVR_F32) {
-    const float4* p = static_cast<const float4*>(s.data) + e * 4;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      float4 f = __ldg(p + i);
-      v.re[2 * i] = f.x;
-      v.im[2 * i] = f.y;
-      v.re[2 * i + 1] = f.z;
-      v.im[2 * i + 1] = f.w;
-    }
-  } else {
-    const uint4* p = static_cast<const uint4*>(s.data) + e * 2;
-    uint4 a = __ldg(p), b = __ldg(p + 1);
-    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-    if constexpr (DT == FVR_BF16) {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        v.re[i] = bf_lo(w[i]);
-        v.im[i] = bf_hi(w[i]);
-      }
-    } else {
-      const int bx = (s.W + 1 + kBrick - 1) / kBrick, by = (s.H + 1 + kBrick - 1) / kBrick;
-      const float sc = __ldg(s.scales + (static_cast<int64_t>(ez / kBrick) * by + ey / kBrick) * bx + ex / kBrick);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        v.re[i] = h_lo(w[i]) * sc;
-        v.im[i] = h_hi(w[i]) * sc;
-      }
-    }
-  }
-}
-
 // Trilinear value and spatial derivatives from the 8 corners (nested lerps).
 struct Interp {
   float sr, si;                        // value
@@ -103,31 +68,125 @@ __device__ __forceinline__ void trilerp(const Sample8& v, float tx, float ty, fl
   }
 }
 
-// Sample the stencil spectrum at p (voxel coords x=W, y=H, z=D).
+// ---- split load / decode, so a thread can put several samples' loads in flight
+
+template <int DT>
+struct Raw;
+template <>
+struct Raw<FVR_F32> {
+  float4 q[4];
+};
+template <>
+struct Raw<FVR_BF16> {
+  uint4 q[2];
+};
+template <>
+struct Raw<FVR_F16> {
+  uint4 q[2];
+  float sc;
+};
+
+// Cell address of p (FP64 voxel coordinates; zero-padding partial or hard cut-off).
+struct Cell {
+  int64_t e;           // entry index, -1 when no corner is inside
+  float tx, ty, tz;    // fractional position inside the cell
+  int ez, ey, ex;      // entry coordinates (for the f16 brick scale)
+};
+
+template <bool HARD>
+__device__ __forceinline__ Cell stencil_cell(const Stencil& s, double px, double py, double pz) {
+  Cell c;
+  bool ok;
+  if (HARD) {
+    ok = (px >= 0.0) && (px <= static_cast<double>(s.W - 1)) && (py >= 0.0) &&
+         (py <= static_cast<double>(s.H - 1)) && (pz >= 0.0) && (pz <= static_cast<double>(s.D - 1));
+  } else {
+    ok = (px >= -1.0) && (px < static_cast<double>(s.W)) && (py >= -1.0) && (py < static_cast<double>(s.H)) &&
+         (pz >= -1.0) && (pz < static_cast<double>(s.D));
+  }
+  if (!ok) {
+    c.e = -1;
+    c.tx = c.ty = c.tz = 0.f;
+    c.ez = c.ey = c.ex = 0;
+    return c;
+  }
+  const double fx = floor(px), fy = floor(py), fz = floor(pz);
+  c.tx = static_cast<float>(px - fx);
+  c.ty = static_cast<float>(py - fy);
+  c.tz = static_cast<float>(pz - fz);
+  c.ex = static_cast<int>(fx) + 1;
+  c.ey = static_cast<int>(fy) + 1;
+  c.ez = static_cast<int>(fz) + 1;
+  c.e = (static_cast<int64_t>(c.ez) * (s.H + 1) + c.ey) * (s.W + 1) + c.ex;
+  return c;
+}
+
+template <int DT>
+__device__ __forceinline__ void raw_load(const Stencil& s, const Cell& c, Raw<DT>& r) {
+  if constexpr (DT == FVR_F32) {
+    if (c.e < 0) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      return;
+    }
+    const float4* p = static_cast<const float4*>(s.data) + c.e * 4;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r.q[i] = __ldg(p + i);
+  } else {
+    if (c.e < 0) {
+      r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
+      if constexpr (DT == FVR_F16) r.sc = 0.f;
+      return;
+    }
+    const uint4* p = static_cast<const uint4*>(s.data) + c.e * 2;
+    r.q[0] = __ldg(p);
+    r.q[1] = __ldg(p + 1);
+    if constexpr (DT == FVR_F16) {
+      const int bx = (s.W + 1 + kBrick - 1) / kBrick, by = (s.H + 1 + kBrick - 1) / kBrick;
+      r.sc = __ldg(s.scales + (static_cast<int64_t>(c.ez / kBrick) * by + c.ey / kBrick) * bx + c.ex / kBrick);
+    }
+  }
+}
+
+template <int DT>
+__device__ __forceinline__ void raw_decode(const Raw<DT>& r, Sample8& v) {
+  if constexpr (DT == FVR_F32) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      v.re[2 * i] = r.q[i].x;
+      v.im[2 * i] = r.q[i].y;
+      v.re[2 * i + 1] = r.q[i].z;
+      v.im[2 * i + 1] = r.q[i].w;
+    }
+  } else {
+    const uint32_t w[8] = {r.q[0].x, r.q[0].y, r.q[0].z, r.q[0].w, r.q[1].x, r.q[1].y, r.q[1].z, r.q[1].w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      if constexpr (DT == FVR_BF16) {
+        v.re[i] = bf_lo(w[i]);
+        v.im[i] = bf_hi(w[i]);
+      } else {
+        v.re[i] = h_lo(w[i]) * r.sc;
+        v.im[i] = h_hi(w[i]) * r.sc;
+      }
+    }
+  }
+}
+
+// Sample the stencil spectrum at p (FP64 voxel coords x=W, y=H, z=D): value
+// and, with DERIV, derivatives.
 // HARD=false: zero-padding partial interpolation (grid_sample padding 'zeros').
 // HARD=true : scipy map_coordinates(order=1, mode='constant'): zero unless
 //             0 <= p <= n-1 on every axis.
-// Returns false (and a zero sample) when nothing of the stencil is inside.
 template <int DT, bool DERIV, bool HARD>
-__device__ __forceinline__ bool stencil_sample(const Stencil& s, float px, float py, float pz, Interp& o) {
-  bool ok;
-  if (HARD) {
-    ok = (px >= 0.f) && (px <= static_cast<float>(s.W - 1)) && (py >= 0.f) &&
-         (py <= static_cast<float>(s.H - 1)) && (pz >= 0.f) && (pz <= static_cast<float>(s.D - 1));
-  } else {
-    ok = (px >= -1.f) && (px < static_cast<float>(s.W)) && (py >= -1.f) && (py < static_cast<float>(s.H)) &&
-         (pz >= -1.f) && (pz < static_cast<float>(s.D));
-  }
-  if (!ok) {
-    o = Interp{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    return false;
-  }
-  const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
-  const int ix = static_cast<int>(fx), iy = static_cast<int>(fy), iz = static_cast<int>(fz);
+__device__ __forceinline__ bool stencil_sample_d(const Stencil& s, double px, double py, double pz, Interp& o) {
+  const Cell c = stencil_cell<HARD>(s, px, py, pz);
+  Raw<DT> r;
+  raw_load<DT>(s, c, r);
   Sample8 v;
-  stencil_load<DT>(s, iz + 1, iy + 1, ix + 1, v);
-  trilerp<DERIV>(v, px - fx, py - fy, pz - fz, o);
-  return true;
+  raw_decode<DT>(r, v);
+  trilerp<DERIV>(v, c.tx, c.ty, c.tz, o);
+  return c.e >= 0;
 }
 
 }  // namespace fvr

@@ -1,320 +1,66 @@
 // Parallel-beam (torch-engine convention) kernels, sm_100a.
 //
-//  * stencil layout build from a centred complex spectrum (+ f16 brick scales)
-//  * drop-in fourier_slice_3d forward / adjoint on the reference's planar
-//    [B_vol, 2, D, H, W] layout        (src/fvr/triton_slice.py:37-339)
-//  * fused zero-IFFT spectral NCC: slice gather + phase ramp + high-pass +
-//    NCC moments (+ pose-gradient moments) in one pass over the samples
-//                                      (src/fvr/torch_engine.py:176-234, 269-307)
-//  * image path: modulated slice written in ifftshift order for the 2D IFFT,
-//    and the per-sample slice adjoint  (src/fvr/torch_engine.py:236-241)
+//  * fused zero-IFFT spectral NCC (src/fvr/torch_engine.py:176-234, 269-307):
+//    one pass per (candidate, view) that forms the slice axes from the pose in
+//    FP64, gathers the slice from the stencil spectrum at FP64 positions,
+//    applies the phase ramp and the high-pass filter, and reduces the NCC
+//    moments together with the 14 moments the pose gradient needs, so the
+//    adjoint is a per-candidate FP64 epilogue (no slice is stored and none is
+//    recomputed).  Several views share one launch.
+//  * image path (torch_engine.py:236-241): modulated slice written in
+//    ifftshift order for the 2D IFFT, and the per-sample slice adjoint.
 //  * FP64 pose maps: Euler (yaw Z, pitch Y, roll X) -> slice axes and the
-//    Euler Jacobian of the pose gradient (src/fvr/torch_engine.py:139-211)
+//    Euler vector-Jacobian product (torch_engine.py:139-211).
+#include "fvr_pose.cuh"
 #include "fvr_stencil.cuh"
 
 namespace fvr {
 
 // ----------------------------------------------------------------------------
-// stencil build
+// slice axes
 // ----------------------------------------------------------------------------
 
-// master spectrum: planar [2][D][H][W] (the reference's f_vol_5d[0]) or
-// interleaved [D][H][W][2]
-template <typename MT>
-__device__ __forceinline__ float2 master_load(const MT* m, int64_t idx, int64_t plane) {
-  return plane ? make_float2(ldf(m + idx), ldf(m + plane + idx)) : make_float2(ldf(m + 2 * idx), ldf(m + 2 * idx + 1));
+// u = R[0,:] * scale, v = R[1,:] * scale with R the (lateral-composed) rotation.
+__device__ __forceinline__ void slice_axes(const float* p, int lateral, double sx, double sy, double sz,
+                                           double* ax) {
+  Mat3 R = euler_R(p[0], p[1], p[2]);
+  if (lateral) R = mat_mul(R, lateral_rot());
+  ax[0] = R.m[0][0] * sx;
+  ax[1] = R.m[0][1] * sy;
+  ax[2] = R.m[0][2] * sz;
+  ax[3] = R.m[1][0] * sx;
+  ax[4] = R.m[1][1] * sy;
+  ax[5] = R.m[1][2] * sz;
+  ax[6] = p[3];
+  ax[7] = p[4];
 }
 
-template <typename MT>
-__device__ __forceinline__ void entry_values(const MT* m, int64_t plane, int D, int H, int W, int ez, int ey, int ex,
-                                             float (&re)[8], float (&im)[8]) {
-#pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int z = ez - 1 + (c >> 2), y = ey - 1 + ((c >> 1) & 1), x = ex - 1 + (c & 1);
-    if (z >= 0 && z < D && y >= 0 && y < H && x >= 0 && x < W) {
-      float2 v = master_load(m, (static_cast<int64_t>(z) * H + y) * W + x, plane);
-      re[c] = v.x;
-      im[c] = v.y;
-    } else {
-      re[c] = 0.f;
-      im[c] = 0.f;
-    }
-  }
-}
-
-template <typename MT>
-__global__ void stencil_brick_max_kernel(const MT* __restrict__ m, int64_t plane, int D, int H, int W,
-                                         unsigned int* bmax) {
-  const int64_t n = static_cast<int64_t>(D + 1) * (H + 1) * (W + 1);
-  const int bx = (W + 1 + kBrick - 1) / kBrick, by = (H + 1 + kBrick - 1) / kBrick;
-  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int ex = static_cast<int>(e % (W + 1));
-    const int ey = static_cast<int>((e / (W + 1)) % (H + 1));
-    const int ez = static_cast<int>(e / (static_cast<int64_t>(W + 1) * (H + 1)));
-    float re[8], im[8];
-    entry_values(m, plane, D, H, W, ez, ey, ex, re, im);
-    float mx = 0.f;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) mx = fmaxf(mx, fmaxf(fabsf(re[c]), fabsf(im[c])));
-    const int64_t b = (static_cast<int64_t>(ez / kBrick) * by + ey / kBrick) * bx + ex / kBrick;
-    atomicMax(bmax + b, __float_as_uint(mx));  // non-negative floats order like their bits
-  }
-}
-
-// scale = 2^e with max/scale <= 2^15 (half max is 65504); exact to apply.
-__global__ void stencil_scale_kernel(const unsigned int* bmax, float* scales, int64_t nb) {
-  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (i >= nb) return;
-  const float mx = __uint_as_float(bmax[i]);
-  float sc = 1.f;
-  if (mx > 0.f && isfinite(mx)) {
-    int e;
-    frexpf(mx, &e);  // mx = f * 2^e, f in [0.5, 1)
-    sc = ldexpf(1.f, e - 15);
-  }
-  scales[i] = sc;
-}
-
-template <typename MT, int DT>
-__global__ void stencil_build_kernel(const MT* __restrict__ m, int64_t plane, int D, int H, int W,
-                                     void* __restrict__ out, const float* __restrict__ scales) {
-  const int64_t n = static_cast<int64_t>(D + 1) * (H + 1) * (W + 1);
-  const int bx = (W + 1 + kBrick - 1) / kBrick, by = (H + 1 + kBrick - 1) / kBrick;
-  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int ex = static_cast<int>(e % (W + 1));
-    const int ey = static_cast<int>((e / (W + 1)) % (H + 1));
-    const int ez = static_cast<int>(e / (static_cast<int64_t>(W + 1) * (H + 1)));
-    float re[8], im[8];
-    entry_values(m, plane, D, H, W, ez, ey, ex, re, im);
-    if constexpr (DT == FVR_F32) {
-      float4* p = static_cast<float4*>(out) + e * 4;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) p[i] = make_float4(re[2 * i], im[2 * i], re[2 * i + 1], im[2 * i + 1]);
-    } else {
-      uint32_t w[8];
-      if constexpr (DT == FVR_BF16) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const uint32_t lo = __bfloat16_as_ushort(__float2bfloat16_rn(re[c]));
-          const uint32_t hi = __bfloat16_as_ushort(__float2bfloat16_rn(im[c]));
-          w[c] = lo | (hi << 16);
-        }
-      } else {
-        const float inv = 1.f / scales[(static_cast<int64_t>(ez / kBrick) * by + ey / kBrick) * bx + ex / kBrick];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const uint32_t lo = __half_as_ushort(__float2half_rn(re[c] * inv));
-          const uint32_t hi = __half_as_ushort(__float2half_rn(im[c] * inv));
-          w[c] = lo | (hi << 16);
-        }
-      }
-      uint4* p = static_cast<uint4*>(out) + e * 2;
-      p[0] = make_uint4(w[0], w[1], w[2], w[3]);
-      p[1] = make_uint4(w[4], w[5], w[6], w[7]);
-    }
-  }
-}
-
-// ----------------------------------------------------------------------------
-// drop-in planar gather  (triton_slice.py:46-143, 145-271)
-// ----------------------------------------------------------------------------
-
-template <typename VT>
-__device__ __forceinline__ float planar_at(const VT* ch, int D, int H, int W, int z, int y, int x) {
-  if (z < 0 || z >= D || y < 0 || y >= H || x < 0 || x >= W) return 0.f;
-  return ldf(ch + (static_cast<int64_t>(z) * H + y) * W + x);
-}
-
-template <typename VT>
-__device__ __forceinline__ void planar_corners(const VT* base, int64_t vol_dhw, int D, int H, int W, float px,
-                                               float py, float pz, Sample8& v, float& tx, float& ty, float& tz) {
-  const float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
-  tx = px - fx;
-  ty = py - fy;
-  tz = pz - fz;
-  // clamp the integer base far outside the volume (all corners then read as 0)
-  const float lo = -2.f;
-  const int ix = static_cast<int>(fminf(fmaxf(fx, lo), static_cast<float>(W)));
-  const int iy = static_cast<int>(fminf(fmaxf(fy, lo), static_cast<float>(H)));
-  const int iz = static_cast<int>(fminf(fmaxf(fz, lo), static_cast<float>(D)));
-#pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int z = iz + (c >> 2), y = iy + ((c >> 1) & 1), x = ix + (c & 1);
-    v.re[c] = planar_at(base, D, H, W, z, y, x);
-    v.im[c] = planar_at(base + vol_dhw, D, H, W, z, y, x);
-  }
-}
-
-template <typename VT>
-__global__ void __launch_bounds__(256) slice3d_fwd_kernel(const VT* __restrict__ vol, int D, int H, int W,
-                                                          const float* __restrict__ u, const float* __restrict__ v,
-                                                          int N, const float* __restrict__ fx,
-                                                          const float* __restrict__ fy, int K, float cx, float cy,
-                                                          float cz, VT* __restrict__ out) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  const int bn = blockIdx.y;
-  if (q >= K) return;
-  const int b = bn / N, n = bn - b * N;
-  const float a = __ldg(fx + q), bb = __ldg(fy + q);
-  const float px = fmaf(bb, __ldg(v + 3 * n + 0), fmaf(a, __ldg(u + 3 * n + 0), cx));
-  const float py = fmaf(bb, __ldg(v + 3 * n + 1), fmaf(a, __ldg(u + 3 * n + 1), cy));
-  const float pz = fmaf(bb, __ldg(v + 3 * n + 2), fmaf(a, __ldg(u + 3 * n + 2), cz));
-  const int64_t dhw = static_cast<int64_t>(D) * H * W;
-  Sample8 s;
-  float tx, ty, tz;
-  planar_corners(vol + static_cast<int64_t>(b) * 2 * dhw, dhw, D, H, W, px, py, pz, s, tx, ty, tz);
-  Interp o;
-  trilerp<false>(s, tx, ty, tz, o);
-  VT* dst = out + static_cast<int64_t>(bn) * 2 * K;
-  stf(dst + q, o.sr);
-  stf(dst + K + q, o.si);
-}
-
-// Per (pose, tile) partial sums of dL/du, dL/dv (6 values) in fp64.
-template <typename VT, typename GT>
-__global__ void __launch_bounds__(256) slice3d_bwd_kernel(const VT* __restrict__ vol, int B, int D, int H, int W,
-                                                          const GT* __restrict__ go, const float* __restrict__ u,
-                                                          const float* __restrict__ v, int N,
-                                                          const float* __restrict__ fx, const float* __restrict__ fy,
-                                                          int K, float cx, float cy, float cz,
-                                                          double* __restrict__ partial) {
-  __shared__ double red[6 * 8];
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = blockIdx.y;
-  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if (q < K) {
-    const float a = __ldg(fx + q), bb = __ldg(fy + q);
-    const float px = fmaf(bb, __ldg(v + 3 * n + 0), fmaf(a, __ldg(u + 3 * n + 0), cx));
-    const float py = fmaf(bb, __ldg(v + 3 * n + 1), fmaf(a, __ldg(u + 3 * n + 1), cy));
-    const float pz = fmaf(bb, __ldg(v + 3 * n + 2), fmaf(a, __ldg(u + 3 * n + 2), cz));
-    const int64_t dhw = static_cast<int64_t>(D) * H * W;
-    float gx = 0.f, gy = 0.f, gz = 0.f;
-    for (int b = 0; b < B; ++b) {
-      Sample8 s;
-      float tx, ty, tz;
-      planar_corners(vol + static_cast<int64_t>(b) * 2 * dhw, dhw, D, H, W, px, py, pz, s, tx, ty, tz);
-      Interp o;
-      trilerp<true>(s, tx, ty, tz, o);
-      const GT* g = go + (static_cast<int64_t>(b) * N + n) * 2 * K;
-      const float gr = ldf(g + q), gi = ldf(g + K + q);
-      gx = fmaf(gr, o.dxr, fmaf(gi, o.dxi, gx));
-      gy = fmaf(gr, o.dyr, fmaf(gi, o.dyi, gy));
-      gz = fmaf(gr, o.dzr, fmaf(gi, o.dzi, gz));
-    }
-    acc[0] = gx * a;
-    acc[1] = gy * a;
-    acc[2] = gz * a;
-    acc[3] = gx * bb;
-    acc[4] = gy * bb;
-    acc[5] = gz * bb;
-  }
-  double tot;
-  block_reduce_to_f64<6>(acc, red, &tot);
-  if (threadIdx.x < 6) partial[(static_cast<int64_t>(n) * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = tot;
-}
-
-__global__ void slice3d_bwd_finalize_kernel(const double* __restrict__ partial, int N, int tiles, float* gu,
-                                            float* gv) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N * 6) return;
-  const int n = i / 6, m = i - n * 6;
-  double s = 0.0;
-  for (int t = 0; t < tiles; ++t) s += partial[(static_cast<int64_t>(n) * tiles + t) * 6 + m];
-  if (m < 3)
-    gu[n * 3 + m] = static_cast<float>(s);
-  else
-    gv[n * 3 + m - 3] = static_cast<float>(s);
-}
-
-// ----------------------------------------------------------------------------
-// FP64 pose maps  (torch_engine.py:139-211)
-// ----------------------------------------------------------------------------
-
-constexpr double kDeg = 0.017453292519943295769236907684886;
-
-struct Mat3 {
-  double m[3][3];
-};
-
-__device__ __forceinline__ Mat3 mat_mul(const Mat3& a, const Mat3& b) {
-  Mat3 r;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[i][0] * b.m[0][j] + a.m[i][1] * b.m[1][j] + a.m[i][2] * b.m[2][j];
-  return r;
-}
-
-__device__ __forceinline__ Mat3 rot_z(double c, double s) { return Mat3{{{c, -s, 0.0}, {s, c, 0.0}, {0.0, 0.0, 1.0}}}; }
-__device__ __forceinline__ Mat3 rot_y(double c, double s) { return Mat3{{{c, 0.0, s}, {0.0, 1.0, 0.0}, {-s, 0.0, c}}}; }
-__device__ __forceinline__ Mat3 rot_x(double c, double s) { return Mat3{{{1.0, 0.0, 0.0}, {0.0, c, -s}, {0.0, s, c}}}; }
-__device__ __forceinline__ Mat3 drot_z(double c, double s) {
-  return Mat3{{{-s, -c, 0.0}, {c, -s, 0.0}, {0.0, 0.0, 0.0}}};
-}
-__device__ __forceinline__ Mat3 drot_y(double c, double s) {
-  return Mat3{{{-s, 0.0, c}, {0.0, 0.0, 0.0}, {-c, 0.0, -s}}};
-}
-__device__ __forceinline__ Mat3 drot_x(double c, double s) {
-  return Mat3{{{0.0, 0.0, 0.0}, {0.0, -s, -c}, {0.0, c, -s}}};
-}
-
-// Rz(90 deg) exactly as the reference forms it: angle and cos/sin in float32,
-// so the off-axis zeros are -4.37e-8 (torch_engine.py:194-198).
-__device__ __forceinline__ Mat3 lateral_rot() {
-  const float a = __fmul_rn(90.0f, 0.0174532925199432957692f);
-  const double c = static_cast<double>(cosf(a)), s = static_cast<double>(sinf(a));
-  return rot_z(c, s);
-}
-
-struct EulerJac {
-  Mat3 R, dz, dy, dx;  // R and dR/d(yaw, pitch, roll) per degree
-};
-
-__device__ __forceinline__ EulerJac euler_jac(double yaw, double pitch, double roll) {
-  double sz, cz, sy, cy, sx, cx;
-  sincos(yaw * kDeg, &sz, &cz);
-  sincos(pitch * kDeg, &sy, &cy);
-  sincos(roll * kDeg, &sx, &cx);
-  const Mat3 Z = rot_z(cz, sz), Y = rot_y(cy, sy), X = rot_x(cx, sx);
-  EulerJac j;
-  j.R = mat_mul(Z, mat_mul(Y, X));
-  j.dz = mat_mul(drot_z(cz, sz), mat_mul(Y, X));
-  j.dy = mat_mul(Z, mat_mul(drot_y(cy, sy), X));
-  j.dx = mat_mul(Z, mat_mul(Y, drot_x(cx, sx)));
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      j.dz.m[a][b] *= kDeg;
-      j.dy.m[a][b] *= kDeg;
-      j.dx.m[a][b] *= kDeg;
-    }
-  return j;
-}
-
-// axes[c] = (u_xyz, v_xyz, tx, ty): u = R[0,:]*scale, v = R[1,:]*scale.
 __global__ void tc_axes_kernel(const float* __restrict__ poses, int C, int lateral, double sx, double sy, double sz,
-                               float* __restrict__ axes) {
+                               double* __restrict__ axes) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= C) return;
-  const float* p = poses + 6 * c;
-  EulerJac j = euler_jac(p[0], p[1], p[2]);
-  Mat3 R = lateral ? mat_mul(j.R, lateral_rot()) : j.R;
-  float* a = axes + 8 * c;
-  a[0] = static_cast<float>(R.m[0][0] * sx);
-  a[1] = static_cast<float>(R.m[0][1] * sy);
-  a[2] = static_cast<float>(R.m[0][2] * sz);
-  a[3] = static_cast<float>(R.m[1][0] * sx);
-  a[4] = static_cast<float>(R.m[1][1] * sy);
-  a[5] = static_cast<float>(R.m[1][2] * sz);
-  a[6] = p[3];
-  a[7] = p[4];
+  slice_axes(poses + 6 * c, lateral, sx, sy, sz, axes + 8 * c);
+}
+
+// dL/d(yaw, pitch, roll) from dL/du, dL/dv (slice axes) for one view.
+__device__ __forceinline__ void axes_vjp(const float* p, int lateral, double sx, double sy, double sz,
+                                         const double du[3], const double dv[3], double out[3]) {
+  Mat3 G{{{du[0] * sx, du[1] * sy, du[2] * sz}, {dv[0] * sx, dv[1] * sy, dv[2] * sz}, {0.0, 0.0, 0.0}}};
+  if (lateral) G = mat_mul_bt(G, lateral_rot());  // R_total = R_pose . L -> dR_pose = dR_total . L^T
+  euler_vjp(p[0], p[1], p[2], G, out);
+}
+
+// Compensated phase / pi: the products of the float32 grid values and
+// translations are exact in FP64; one rounding to float before sincospif.
+__device__ __forceinline__ void phase_sincos(double kpi, float ku, float kv, float tx, float ty, float* sn,
+                                             float* cs) {
+  const double arg =
+      kpi * fma(static_cast<double>(ku), static_cast<double>(tx), static_cast<double>(kv) * static_cast<double>(ty));
+  sincospif(static_cast<float>(arg), sn, cs);
 }
 
 // ----------------------------------------------------------------------------
-// fused zero-IFFT spectral NCC  (torch_engine.py:176-234, 269-290)
+// fused zero-IFFT spectral NCC
 // ----------------------------------------------------------------------------
 
 enum {
@@ -329,173 +75,213 @@ enum {
   M_BV = 14,  // 3
   M_NGRAD = 17
 };
+constexpr int kMomStride = 18;  // mom[v][c][18]: 17 moments + ncc
+constexpr int kMaxViews = 4;
 constexpr int kSnccThreads = 256;
-constexpr int kSnccSpt = 4;  // samples per thread per tile
-constexpr int kSnccTile = kSnccThreads * kSnccSpt;
+constexpr int kSnccGroup = 4;  // samples with loads in flight per thread
 
 struct SnccArgs {
   Stencil st;
-  const float* axes;    // [C][8]
-  const float2* ftarg;  // [R*R] complex target spectrum (already high-passed)
-  const float* hp;      // [R*R] or null
-  const float* lin;     // [R] torch.linspace(-1, 1, R)
-  int R;
-  float kpi;  // kappa / pi, phase/pi = kpi * (ku*tx + kv*ty)
-  float cx, cy, cz;
-  double* partial;  // [C][tiles][NM]
+  const float* poses;  // [C][6]
+  const float2* ftarg[kMaxViews];
+  int lateral[kMaxViews];
+  const float* hp;   // [R*R] or null
+  const float* lin;  // [R]
+  int R, C, tile;    // tile = samples per CTA, multiple of 256
+  double kpi;        // kappa / pi
+  double sx, sy, sz;
+  double* partial;  // [nv][C][tiles][NM]
 };
 
+// CTA sum of per-thread partials; every cross-lane / cross-warp step in fp64
+// (the pose-gradient moments are small residuals of large cancelling sums).
+template <int NV, typename T>
+__device__ __forceinline__ void block_reduce_d(T (&acc)[NV], double* red, double* out_m) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int m = 0; m < NV; ++m) {
+    const double v = warp_sum(static_cast<double>(acc[m]));
+    if (lane == 0) red[m * nw + wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += red[threadIdx.x * nw + w];
+    *out_m = s;
+  }
+}
+
 template <int DT, bool GRAD>
-__global__ void __launch_bounds__(kSnccThreads) tc_sncc_moments_kernel(SnccArgs a) {
+__global__ void __launch_bounds__(kSnccThreads, 2) tc_sncc_moments_kernel(SnccArgs a) {
   constexpr int NM = GRAD ? M_NGRAD : 3;
   __shared__ double red[NM * (kSnccThreads / 32)];
-  const int c = blockIdx.y;
-  const float* ax = a.axes + 8 * c;
-  const float ux = __ldg(ax + 0), uy = __ldg(ax + 1), uz = __ldg(ax + 2);
-  const float vx = __ldg(ax + 3), vy = __ldg(ax + 4), vz = __ldg(ax + 5);
-  const float tx = __ldg(ax + 6), ty = __ldg(ax + 7);
-  const int R = a.R;
-  const int K = R * R;
-  float acc[NM];
+  __shared__ double ax_s[8];
+  const int tile = blockIdx.x, c = blockIdx.y, v = blockIdx.z;
+  // select the view's parameters without dynamic indexing of the parameter space
+  const int lateral = v == 0 ? a.lateral[0] : v == 1 ? a.lateral[1] : v == 2 ? a.lateral[2] : a.lateral[3];
+  const float2* __restrict__ ft = v == 0 ? a.ftarg[0] : v == 1 ? a.ftarg[1] : v == 2 ? a.ftarg[2] : a.ftarg[3];
+  if (threadIdx.x == 0) slice_axes(a.poses + 6 * c, lateral, a.sx, a.sy, a.sz, ax_s);
+  __syncthreads();
+  const double ux = ax_s[0], uy = ax_s[1], uz = ax_s[2], vx = ax_s[3], vy = ax_s[4], vz = ax_s[5];
+  const float tx = static_cast<float>(ax_s[6]), ty = static_cast<float>(ax_s[7]);
+  const int R = a.R, K = R * R;
+  const int q_begin = tile * a.tile;
+  const int q_end = min(q_begin + a.tile, K);
+  float acc[NM];  // per-thread partial over ~K*C*nv/(2*SMs*256) samples
 #pragma unroll
   for (int m = 0; m < NM; ++m) acc[m] = 0.f;
+
+  for (int base = q_begin; base < q_end; base += kSnccThreads * kSnccGroup) {
+    Raw<DT> raw[kSnccGroup];
+    Cell cell[kSnccGroup];
+    float kus[kSnccGroup], kvs[kSnccGroup], hs[kSnccGroup];
+    float2 Ts[kSnccGroup];
+    // issue every load of the group before using any of them
 #pragma unroll
-  for (int s = 0; s < kSnccSpt; ++s) {
-    const int q = blockIdx.x * kSnccTile + s * kSnccThreads + threadIdx.x;
-    if (q >= K) break;
-    const int i = q / R, j = q - (q / R) * R;
-    const float ku = __ldg(a.lin + i), kv = __ldg(a.lin + j);
-    const float px = fmaf(kv, vx, fmaf(ku, ux, a.cx));
-    const float py = fmaf(kv, vy, fmaf(ku, uy, a.cy));
-    const float pz = fmaf(kv, vz, fmaf(ku, uz, a.cz));
-    Interp o;
-    stencil_sample<DT, GRAD, false>(a.st, px, py, pz, o);
-    float sn, cs;
-    sincospif(a.kpi * fmaf(ku, tx, kv * ty), &sn, &cs);
-    const float h = a.hp ? __ldg(a.hp + q) : 1.f;
-    const float2 T = __ldg(a.ftarg + q);
-    const float shr = h * (o.sr * cs - o.si * sn);
-    const float shi = h * (o.sr * sn + o.si * cs);
-    acc[M_CROSS] = fmaf(shr, T.x, fmaf(shi, T.y, acc[M_CROSS]));
-    acc[M_EP] = fmaf(shr, shr, fmaf(shi, shi, acc[M_EP]));
-    acc[M_ET] = fmaf(T.x, T.x, fmaf(T.y, T.y, acc[M_ET]));
-    if constexpr (GRAD) {
-      // dL/dphi direction: Re(conj(T) i S_hat) = T.y*shr - T.x*shi
-      const float ph = T.y * shr - T.x * shi;
-      acc[M_PHU] = fmaf(ku, ph, acc[M_PHU]);
-      acc[M_PHV] = fmaf(kv, ph, acc[M_PHV]);
-      // M_T = h e^{-i phi} T ;  A_k = <M_T, dS/dp_k>
-      const float mtr = h * (cs * T.x + sn * T.y);
-      const float mti = h * (cs * T.y - sn * T.x);
-      const float a0 = mtr * o.dxr + mti * o.dxi;
-      const float a1 = mtr * o.dyr + mti * o.dyi;
-      const float a2 = mtr * o.dzr + mti * o.dzi;
-      // B_k = h^2 <S, dS/dp_k>
-      const float h2 = h * h;
-      const float b0 = h2 * (o.sr * o.dxr + o.si * o.dxi);
-      const float b1 = h2 * (o.sr * o.dyr + o.si * o.dyi);
-      const float b2 = h2 * (o.sr * o.dzr + o.si * o.dzi);
-      acc[M_AU + 0] = fmaf(ku, a0, acc[M_AU + 0]);
-      acc[M_AU + 1] = fmaf(ku, a1, acc[M_AU + 1]);
-      acc[M_AU + 2] = fmaf(ku, a2, acc[M_AU + 2]);
-      acc[M_AV + 0] = fmaf(kv, a0, acc[M_AV + 0]);
-      acc[M_AV + 1] = fmaf(kv, a1, acc[M_AV + 1]);
-      acc[M_AV + 2] = fmaf(kv, a2, acc[M_AV + 2]);
-      acc[M_BU + 0] = fmaf(ku, b0, acc[M_BU + 0]);
-      acc[M_BU + 1] = fmaf(ku, b1, acc[M_BU + 1]);
-      acc[M_BU + 2] = fmaf(ku, b2, acc[M_BU + 2]);
-      acc[M_BV + 0] = fmaf(kv, b0, acc[M_BV + 0]);
-      acc[M_BV + 1] = fmaf(kv, b1, acc[M_BV + 1]);
-      acc[M_BV + 2] = fmaf(kv, b2, acc[M_BV + 2]);
+    for (int g = 0; g < kSnccGroup; ++g) {
+      const int q = base + g * kSnccThreads + threadIdx.x;
+      const bool ok = q < q_end;
+      const int i = ok ? q / R : 0, j = ok ? q - i * R : 0;
+      kus[g] = __ldg(a.lin + i);
+      kvs[g] = __ldg(a.lin + j);
+      const double ku = kus[g], kv = kvs[g];
+      if (ok) {
+        cell[g] = stencil_cell<false>(a.st, fma(kv, vx, fma(ku, ux, a.sx)), fma(kv, vy, fma(ku, uy, a.sy)),
+                                      fma(kv, vz, fma(ku, uz, a.sz)));
+      } else {
+        cell[g] = Cell{-1, 0.f, 0.f, 0.f, 0, 0, 0};
+      }
+      raw_load<DT>(a.st, cell[g], raw[g]);
+      Ts[g] = ok ? __ldg(ft + q) : make_float2(0.f, 0.f);
+      hs[g] = ok ? (a.hp ? __ldg(a.hp + q) : 1.f) : 0.f;
+    }
+#pragma unroll
+    for (int g = 0; g < kSnccGroup; ++g) {
+      Sample8 sm;
+      raw_decode<DT>(raw[g], sm);
+      Interp o;
+      trilerp<GRAD>(sm, cell[g].tx, cell[g].ty, cell[g].tz, o);
+      const float ku = kus[g], kv = kvs[g], h = hs[g];
+      const float2 T = Ts[g];
+      float sn, cs;
+      phase_sincos(a.kpi, ku, kv, tx, ty, &sn, &cs);
+      const float shr = h * (o.sr * cs - o.si * sn);
+      const float shi = h * (o.sr * sn + o.si * cs);
+      acc[M_CROSS] = fmaf(shr, T.x, fmaf(shi, T.y, acc[M_CROSS]));
+      acc[M_EP] = fmaf(shr, shr, fmaf(shi, shi, acc[M_EP]));
+      acc[M_ET] = fmaf(T.x, T.x, fmaf(T.y, T.y, acc[M_ET]));
+      if constexpr (GRAD) {
+        // dL/dphi direction: Re(conj(T) i S_hat) = T.y*shr - T.x*shi
+        const float ph = T.y * shr - T.x * shi;
+        acc[M_PHU] += ku * ph;
+        acc[M_PHV] += kv * ph;
+        // M_T = h e^{-i phi} T ;  A_k = <M_T, dS/dp_k> ;  B_k = h^2 <S, dS/dp_k>
+        const float mtr = h * (cs * T.x + sn * T.y);
+        const float mti = h * (cs * T.y - sn * T.x);
+        const float h2 = h * h;
+        const float a0 = mtr * o.dxr + mti * o.dxi, a1 = mtr * o.dyr + mti * o.dyi, a2 = mtr * o.dzr + mti * o.dzi;
+        const float b0 = h2 * (o.sr * o.dxr + o.si * o.dxi), b1 = h2 * (o.sr * o.dyr + o.si * o.dyi),
+                    b2 = h2 * (o.sr * o.dzr + o.si * o.dzi);
+        acc[M_AU + 0] += ku * a0;
+        acc[M_AU + 1] += ku * a1;
+        acc[M_AU + 2] += ku * a2;
+        acc[M_AV + 0] += kv * a0;
+        acc[M_AV + 1] += kv * a1;
+        acc[M_AV + 2] += kv * a2;
+        acc[M_BU + 0] += ku * b0;
+        acc[M_BU + 1] += ku * b1;
+        acc[M_BU + 2] += ku * b2;
+        acc[M_BV + 0] += kv * b0;
+        acc[M_BV + 1] += kv * b1;
+        acc[M_BV + 2] += kv * b2;
+      }
     }
   }
   double tot;
-  block_reduce_to_f64<NM>(acc, red, &tot);
-  if (threadIdx.x < NM) a.partial[(static_cast<int64_t>(c) * gridDim.x + blockIdx.x) * NM + threadIdx.x] = tot;
+  block_reduce_d<NM, float>(acc, red, &tot);
+  if (threadIdx.x < NM)
+    a.partial[((static_cast<int64_t>(v) * a.C + c) * gridDim.x + tile) * NM + threadIdx.x] = tot;
 }
 
-// Sum tiles (fp64, fixed order) -> mom[c][NM]; loss = 1 - mean_c ncc_c.
-__global__ void __launch_bounds__(256) tc_sncc_finalize_kernel(const double* __restrict__ partial, int C, int tiles,
-                                                               int NM, double* __restrict__ mom,
-                                                               float* __restrict__ loss, float* __restrict__ ncc_out) {
-  __shared__ double red[8];
-  double nsum = 0.0;
-  for (int c = threadIdx.x; c < C; c += blockDim.x) {
-    double v[M_NGRAD];
-    for (int m = 0; m < NM; ++m) {
-      double s = 0.0;
-      for (int t = 0; t < tiles; ++t) s += partial[(static_cast<int64_t>(c) * tiles + t) * NM + m];
-      v[m] = s;
-      mom[static_cast<int64_t>(c) * NM + m] = s;
-    }
-    const double ncc = v[M_CROSS] / (sqrt(v[M_EP] * v[M_ET]) + 1e-8);
-    if (ncc_out) ncc_out[c] = static_cast<float>(ncc);
-    nsum += ncc;
-  }
-  nsum = warp_sum(nsum);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nsum;
-  __syncthreads();
-  if (threadIdx.x == 0) {
+// Tile sums (fp64, fixed order) -> mom[v][c][0..NM), ncc in mom[v][c][17];
+// loss[v] = 1 - mean_c ncc, loss[nv] = sum_v loss[v].  One CTA, warp per (v, c).
+__global__ void __launch_bounds__(1024) tc_sncc_finalize_kernel(const double* __restrict__ partial, int C, int nv,
+                                                                int tiles, int NM, double* __restrict__ mom,
+                                                                float* __restrict__ loss,
+                                                                float* __restrict__ ncc_out) {
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int item = w; item < nv * C; item += nw) {
     double s = 0.0;
-    for (int w = 0; w < (blockDim.x >> 5); ++w) s += red[w];
-    *loss = static_cast<float>(1.0 - s / static_cast<double>(C));
+    if (lane < NM) {
+      for (int t = 0; t < tiles; ++t) s += partial[(static_cast<int64_t>(item) * tiles + t) * NM + lane];
+      mom[static_cast<int64_t>(item) * kMomStride + lane] = s;
+    }
+    const double cross = __shfl_sync(0xffffffffu, s, 0), ep = __shfl_sync(0xffffffffu, s, 1),
+                 et = __shfl_sync(0xffffffffu, s, 2);
+    if (lane == 0) {
+      const double n = cross / (sqrt(ep * et) + 1e-8);
+      mom[static_cast<int64_t>(item) * kMomStride + 17] = n;
+      if (ncc_out) ncc_out[item] = static_cast<float>(n);
+    }
   }
+  __syncthreads();
+  double total = 0.0;
+  for (int v = 0; v < nv; ++v) {
+    double s = 0.0;
+    for (int c = threadIdx.x; c < C; c += blockDim.x) s += mom[(static_cast<int64_t>(v) * C + c) * kMomStride + 17];
+    s = warp_sum(s);
+    if (lane == 0) red[w] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < nw; ++k) t += red[k];
+      const double l = 1.0 - t / C;
+      loss[v] = static_cast<float>(l);
+      total += l;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) loss[nv] = static_cast<float>(total);
 }
 
-// Pose gradient from per-candidate slice-axis gradients.
-//  mode 0: spectral NCC moments mom[c][17] and upstream dL/dloss (*g)
-//  mode 1: adjoint partials part[c][tiles][8] = (dU[3], dV[3], PHU, PHV)
-__global__ void tc_pose_grad_kernel(int mode, const double* __restrict__ src, int tiles, const float* __restrict__ g,
-                                    const float* __restrict__ poses, int C, int lateral, double sx, double sy,
-                                    double sz, double kappa, float* __restrict__ grad, int accumulate) {
+struct SnccGradArgs {
+  const double* mom;  // [nv][C][18]
+  const float* g;     // dL/dloss_v at g[v * g_stride]
+  int g_stride;
+  const float* poses;
+  int C, nv;
+  int lateral[kMaxViews];
+  double sx, sy, sz, kappa;
+  float* grad;  // [C][6]
+  int accumulate;
+};
+
+__global__ void tc_sncc_grad_kernel(SnccGradArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= C) return;
-  double du[3], dv[3], dtx, dty;
-  if (mode == 0) {
-    const double* v = src + static_cast<int64_t>(c) * M_NGRAD;
-    const double gl = static_cast<double>(*g);
-    const double s = sqrt(v[M_EP] * v[M_ET]);
+  if (c >= a.C) return;
+  const float* p = a.poses + 6 * c;
+  double gang[3] = {0.0, 0.0, 0.0}, gtx = 0.0, gty = 0.0;
+  for (int v = 0; v < a.nv; ++v) {
+    const double* m = a.mom + (static_cast<int64_t>(v) * a.C + c) * kMomStride;
+    const double s = sqrt(m[M_EP] * m[M_ET]);
     const double aa = 1.0 / (s + 1e-8);
-    const double bb = s > 0.0 ? -v[M_CROSS] * v[M_ET] / (2.0 * s * (s + 1e-8) * (s + 1e-8)) : 0.0;
-    const double gc = -gl / static_cast<double>(C);
+    const double bb = s > 0.0 ? -m[M_CROSS] * m[M_ET] / (2.0 * s * (s + 1e-8) * (s + 1e-8)) : 0.0;
+    const double gc = -static_cast<double>(a.g[v * a.g_stride]) / a.C;
+    double du[3], dv[3], ga[3];
     for (int k = 0; k < 3; ++k) {
-      du[k] = gc * (aa * v[M_AU + k] + 2.0 * bb * v[M_BU + k]);
-      dv[k] = gc * (aa * v[M_AV + k] + 2.0 * bb * v[M_BV + k]);
+      du[k] = gc * (aa * m[M_AU + k] + 2.0 * bb * m[M_BU + k]);
+      dv[k] = gc * (aa * m[M_AV + k] + 2.0 * bb * m[M_BV + k]);
     }
-    dtx = gc * aa * kappa * v[M_PHU];
-    dty = gc * aa * kappa * v[M_PHV];
-  } else {
-    double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = 0; i < tiles; ++i)
-      for (int m = 0; m < 8; ++m) t[m] += src[(static_cast<int64_t>(c) * tiles + i) * 8 + m];
-    for (int k = 0; k < 3; ++k) {
-      du[k] = t[k];
-      dv[k] = t[3 + k];
-    }
-    dtx = kappa * t[6];
-    dty = kappa * t[7];
+    axes_vjp(p, a.lateral[v], a.sx, a.sy, a.sz, du, dv, ga);
+    for (int k = 0; k < 3; ++k) gang[k] += ga[k];
+    gtx += gc * aa * a.kappa * m[M_PHU];
+    gty += gc * aa * a.kappa * m[M_PHV];
   }
-  const float* p = poses + 6 * c;
-  EulerJac j = euler_jac(p[0], p[1], p[2]);
-  Mat3 gR{{{du[0] * sx, du[1] * sy, du[2] * sz}, {dv[0] * sx, dv[1] * sy, dv[2] * sz}, {0.0, 0.0, 0.0}}};
-  if (lateral) {  // R_total = R_pose . R_lat  ->  dL/dR_pose = dL/dR_total . R_lat^T
-    const Mat3 L = lateral_rot();
-    Mat3 t;
-    for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) t.m[a][b] = gR.m[a][0] * L.m[b][0] + gR.m[a][1] * L.m[b][1] + gR.m[a][2] * L.m[b][2];
-    gR = t;
-  }
-  double gyaw = 0.0, gpitch = 0.0, groll = 0.0;
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) {
-      gyaw += gR.m[a][b] * j.dz.m[a][b];
-      gpitch += gR.m[a][b] * j.dy.m[a][b];
-      groll += gR.m[a][b] * j.dx.m[a][b];
-    }
-  float* o = grad + 6 * c;
-  const float r[6] = {static_cast<float>(gyaw), static_cast<float>(gpitch), static_cast<float>(groll),
-                      static_cast<float>(dtx), static_cast<float>(dty), 0.f};
-  for (int k = 0; k < 6; ++k) o[k] = accumulate ? o[k] + r[k] : r[k];
+  float* o = a.grad + 6 * c;
+  const float r[6] = {static_cast<float>(gang[0]), static_cast<float>(gang[1]), static_cast<float>(gang[2]),
+                      static_cast<float>(gtx), static_cast<float>(gty), 0.f};
+  for (int k = 0; k < 6; ++k) o[k] = a.accumulate ? o[k] + r[k] : r[k];
 }
 
 // ----------------------------------------------------------------------------
@@ -504,75 +290,68 @@ __global__ void tc_pose_grad_kernel(int mode, const double* __restrict__ src, in
 
 struct SliceArgs {
   Stencil st;
-  const float* axes;
+  const double* axes;  // [C][8]
   const float* lin;
   int R;
-  float kpi;
-  float cx, cy, cz;
-  int shift;  // 1: write/read position ifftshift(q) (image path), 0: natural order
+  double kpi;
+  double sx, sy, sz;
+  int shift;  // 1: position ifftshift(q) (image path), 0: natural order
 };
 
 __device__ __forceinline__ int shifted_pos(int i, int j, int R, int shift) {
-  if (shift) {
-    // ifftshift: element (i, j) lands at ((i - R/2) mod R, (j - R/2) mod R)
+  if (shift) {  // ifftshift: element (i, j) lands at ((i - R/2) mod R, (j - R/2) mod R)
     const int h = R / 2;
-    i = i - h;
+    i -= h;
     if (i < 0) i += R;
-    j = j - h;
+    j -= h;
     if (j < 0) j += R;
   }
   return i * R + j;
 }
 
+template <int DT, bool DERIV>
+__device__ __forceinline__ void slice_sample(const SliceArgs& a, const double* ax, float ku, float kv, Interp& o,
+                                             float& sn, float& cs) {
+  const double dku = ku, dkv = kv;
+  stencil_sample_d<DT, DERIV, false>(a.st, fma(dkv, ax[3], fma(dku, ax[0], a.sx)),
+                                     fma(dkv, ax[4], fma(dku, ax[1], a.sy)), fma(dkv, ax[5], fma(dku, ax[2], a.sz)),
+                                     o);
+  phase_sincos(a.kpi, ku, kv, static_cast<float>(ax[6]), static_cast<float>(ax[7]), &sn, &cs);
+}
+
 template <int DT>
 __global__ void __launch_bounds__(256) tc_slice_kernel(SliceArgs a, float2* __restrict__ out) {
-  const int c = blockIdx.y;
-  const int R = a.R;
+  const int c = blockIdx.y, R = a.R;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= R * R) return;
-  const float* ax = a.axes + 8 * c;
   const int i = q / R, j = q - (q / R) * R;
-  const float ku = __ldg(a.lin + i), kv = __ldg(a.lin + j);
-  const float px = fmaf(kv, __ldg(ax + 3), fmaf(ku, __ldg(ax + 0), a.cx));
-  const float py = fmaf(kv, __ldg(ax + 4), fmaf(ku, __ldg(ax + 1), a.cy));
-  const float pz = fmaf(kv, __ldg(ax + 5), fmaf(ku, __ldg(ax + 2), a.cz));
   Interp o;
-  stencil_sample<DT, false, false>(a.st, px, py, pz, o);
   float sn, cs;
-  sincospif(a.kpi * fmaf(ku, __ldg(ax + 6), kv * __ldg(ax + 7)), &sn, &cs);
+  slice_sample<DT, false>(a, a.axes + 8 * c, __ldg(a.lin + i), __ldg(a.lin + j), o, sn, cs);
   out[static_cast<int64_t>(c) * R * R + shifted_pos(i, j, R, a.shift)] =
       make_float2(o.sr * cs - o.si * sn, o.sr * sn + o.si * cs);
 }
 
-// Given G = dL/dS_hat per sample, per-candidate partials
-// (dU[3], dV[3], PHU, PHV) with dL/dS = e^{-i phi} G and
-// dL/dphi = Re(conj(G) i S_hat).
+// Given G = dL/dS_hat per sample: partials (dU[3], dV[3], PHU, PHV) per
+// (candidate, tile) with dL/dS = e^{-i phi} G and dL/dphi = Re(conj(G) i S_hat).
 template <int DT>
 __global__ void __launch_bounds__(256) tc_slice_adjoint_kernel(SliceArgs a, const float2* __restrict__ G,
                                                                double* __restrict__ partial) {
   __shared__ double red[8 * 8];
-  const int c = blockIdx.y;
-  const int R = a.R;
+  const int c = blockIdx.y, R = a.R;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (q < R * R) {
-    const float* ax = a.axes + 8 * c;
     const int i = q / R, j = q - (q / R) * R;
     const float ku = __ldg(a.lin + i), kv = __ldg(a.lin + j);
-    const float px = fmaf(kv, __ldg(ax + 3), fmaf(ku, __ldg(ax + 0), a.cx));
-    const float py = fmaf(kv, __ldg(ax + 4), fmaf(ku, __ldg(ax + 1), a.cy));
-    const float pz = fmaf(kv, __ldg(ax + 5), fmaf(ku, __ldg(ax + 2), a.cz));
     Interp o;
-    stencil_sample<DT, true, false>(a.st, px, py, pz, o);
     float sn, cs;
-    sincospif(a.kpi * fmaf(ku, __ldg(ax + 6), kv * __ldg(ax + 7)), &sn, &cs);
+    slice_sample<DT, true>(a, a.axes + 8 * c, ku, kv, o, sn, cs);
     const float2 g = __ldg(G + static_cast<int64_t>(c) * R * R + shifted_pos(i, j, R, a.shift));
     const float shr = o.sr * cs - o.si * sn, shi = o.sr * sn + o.si * cs;
     const float ph = g.y * shr - g.x * shi;
     const float dr = cs * g.x + sn * g.y, di = cs * g.y - sn * g.x;  // e^{-i phi} G
-    const float e0 = dr * o.dxr + di * o.dxi;
-    const float e1 = dr * o.dyr + di * o.dyi;
-    const float e2 = dr * o.dzr + di * o.dzi;
+    const float e0 = dr * o.dxr + di * o.dxi, e1 = dr * o.dyr + di * o.dyi, e2 = dr * o.dzr + di * o.dzi;
     acc[0] = ku * e0;
     acc[1] = ku * e1;
     acc[2] = ku * e2;
@@ -583,40 +362,25 @@ __global__ void __launch_bounds__(256) tc_slice_adjoint_kernel(SliceArgs a, cons
     acc[7] = kv * ph;
   }
   double tot;
-  block_reduce_to_f64<8>(acc, red, &tot);
+  block_reduce_d<8, double>(acc, red, &tot);
   if (threadIdx.x < 8) partial[(static_cast<int64_t>(c) * gridDim.x + blockIdx.x) * 8 + threadIdx.x] = tot;
 }
 
-// relu mask of the saved image, as complex: G = (img > 0) * g
-__global__ void relu_mask_kernel(const float* __restrict__ img, const float* __restrict__ g, float* __restrict__ out,
-                                 int64_t n) {
-  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (i >= n) return;
-  out[i] = img[i] > 0.f ? g[i] : 0.f;
-}
-
-// complex * real table (per image), e.g. the high-pass filter of a target spectrum
-__global__ void cmul_table_kernel(float2* __restrict__ x, const float* __restrict__ t, int64_t per, int64_t n) {
-  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (i >= n) return;
-  const float w = t[i % per];
-  x[i] = make_float2(x[i].x * w, x[i].y * w);
-}
-
-// HP = 1 - exp(-r^2 / (2 sigma^2)) on linspace(-H/2, H/2, H) x linspace(-W/2, W/2, W)
-// (torch_engine.py:123-136), evaluated in fp64.
-__global__ void hp_filter_kernel(float* __restrict__ out, int H, int W, double sigma) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= H * W) return;
-  const int r = i / W, c = i - r * W;
-  const double y = H > 1 ? -0.5 * H + r * (static_cast<double>(H) / (H - 1)) : -0.5 * H;
-  const double x = W > 1 ? -0.5 * W + c * (static_cast<double>(W) / (W - 1)) : -0.5 * W;
-  out[i] = static_cast<float>(1.0 - exp(-(x * x + y * y) / (2.0 * sigma * sigma)));
-}
-
-__global__ void linspace_kernel(float* out, float start, float end, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = linspace_f32(start, end, n, i);
+__global__ void tc_adjoint_grad_kernel(const double* __restrict__ part, int tiles, const float* __restrict__ poses,
+                                       int C, int lateral, double sx, double sy, double sz, double kappa,
+                                       float* __restrict__ grad, int accumulate) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < tiles; ++i)
+    for (int m = 0; m < 8; ++m) t[m] += part[(static_cast<int64_t>(c) * tiles + i) * 8 + m];
+  const double du[3] = {t[0], t[1], t[2]}, dv[3] = {t[3], t[4], t[5]};
+  double ga[3];
+  axes_vjp(poses + 6 * c, lateral, sx, sy, sz, du, dv, ga);
+  float* o = grad + 6 * c;
+  const float r[6] = {static_cast<float>(ga[0]), static_cast<float>(ga[1]), static_cast<float>(ga[2]),
+                      static_cast<float>(kappa * t[6]), static_cast<float>(kappa * t[7]), 0.f};
+  for (int k = 0; k < 6; ++k) o[k] = accumulate ? o[k] + r[k] : r[k];
 }
 
 static int stencil_from(int dtype, const void* data, const float* scales, int64_t D, int64_t H, int64_t W,
@@ -629,177 +393,79 @@ static int stencil_from(int dtype, const void* data, const float* scales, int64_
   return FVR_OK;
 }
 
+static double half_extent(int64_t n) { return 0.5 * static_cast<double>(n > 1 ? n - 1 : 1); }
+
+// Samples per CTA: fill about two resident CTAs per SM in one wave.
+static int sncc_tile(int64_t C, int64_t K, int nv) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  const int64_t items = C * nv;
+  int64_t tiles = (2LL * sms + items - 1) / items;
+  const int64_t max_tiles = cdiv64(K, kSnccThreads * kSnccGroup);
+  if (tiles > max_tiles) tiles = max_tiles;
+  if (tiles < 1) tiles = 1;
+  int64_t tile = cdiv64(K, tiles);
+  tile = cdiv64(tile, kSnccThreads) * kSnccThreads;
+  return static_cast<int>(tile);
+}
+
 }  // namespace fvr
 
 using namespace fvr;
 
 extern "C" {
 
-int64_t fvr_stencil_bytes(int64_t D, int64_t H, int64_t W, int dtype) {
-  const int64_t n = (D + 1) * (H + 1) * (W + 1);
-  if (dtype == FVR_F32) return n * 64;
-  if (dtype == FVR_BF16 || dtype == FVR_F16) return n * 32;
-  return -1;
-}
-
-int64_t fvr_stencil_scale_count(int64_t D, int64_t H, int64_t W) {
-  return fvr::cdiv64(D + 1, kBrick) * fvr::cdiv64(H + 1, kBrick) * fvr::cdiv64(W + 1, kBrick);
-}
-
-int fvr_stencil_build(const void* master, int master_dtype, int master_planar, int64_t D, int64_t H, int64_t W,
-                      int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream) {
-  if (!master || !out || D < 1 || H < 1 || W < 1 || D > 8192 || H > 8192 || W > 8192) return FVR_ERR_ARG;
-  if ((reinterpret_cast<uintptr_t>(out) & 15) != 0) return FVR_ERR_ARG;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int64_t n = (D + 1) * (H + 1) * (W + 1);
-  const int64_t nblk = cdiv64(n, 256);
-  const unsigned grid = static_cast<unsigned>(nblk < 148 * 64 ? nblk : 148 * 64);
-  const int d = (int)D, h = (int)H, w = (int)W;
-  const int64_t plane = master_planar ? D * H * W : 0;
-  if (out_dtype == FVR_F16) {
-    if (!scales || !scratch_max) return FVR_ERR_ARG;
-    const int64_t nb = fvr_stencil_scale_count(D, H, W);
-    if (cudaMemsetAsync(scratch_max, 0, nb * sizeof(unsigned int), s) != cudaSuccess) return FVR_ERR_CUDA;
-    if (master_dtype == FVR_F32)
-      stencil_brick_max_kernel<float>
-          <<<grid, 256, 0, s>>>(static_cast<const float*>(master), plane, d, h, w, scratch_max);
-    else if (master_dtype == FVR_BF16)
-      stencil_brick_max_kernel<__nv_bfloat16>
-          <<<grid, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(master), plane, d, h, w, scratch_max);
-    else
-      return FVR_ERR_DTYPE;
-    stencil_scale_kernel<<<static_cast<unsigned>(cdiv64(nb, 256)), 256, 0, s>>>(scratch_max, scales, nb);
-  }
-#define FVR_BUILD(MT, DT)                                                                                  \
-  stencil_build_kernel<MT, DT><<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, d, h, w, out, scales); \
-  break;
-  if (master_dtype == FVR_F32) {
-    switch (out_dtype) {
-      case FVR_F32: FVR_BUILD(float, FVR_F32)
-      case FVR_BF16: FVR_BUILD(float, FVR_BF16)
-      case FVR_F16: FVR_BUILD(float, FVR_F16)
-      default: return FVR_ERR_DTYPE;
-    }
-  } else if (master_dtype == FVR_BF16) {
-    switch (out_dtype) {
-      case FVR_F32: FVR_BUILD(__nv_bfloat16, FVR_F32)
-      case FVR_BF16: FVR_BUILD(__nv_bfloat16, FVR_BF16)
-      case FVR_F16: FVR_BUILD(__nv_bfloat16, FVR_F16)
-      default: return FVR_ERR_DTYPE;
-    }
-  } else {
-    return FVR_ERR_DTYPE;
-  }
-#undef FVR_BUILD
-  FVR_LAUNCH_CHECK();
-  return FVR_OK;
-}
-
-int fvr_slice3d_fwd(const void* vol, int dtype, int64_t B, int64_t D, int64_t H, int64_t W, const float* u,
-                    const float* v, int64_t N, const float* fx, const float* fy, int64_t K, float cx, float cy,
-                    float cz, void* out, void* stream) {
-  if (!vol || !u || !v || !fx || !fy || !out) return FVR_ERR_ARG;
-  if (B < 1 || N < 1 || K < 1 || D < 1 || H < 1 || W < 1) return FVR_ERR_ARG;
-  if (B * N > 65535 || K > (int64_t)1 << 30) return FVR_ERR_ARG;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  dim3 grid(static_cast<unsigned>(cdiv64(K, 256)), static_cast<unsigned>(B * N));
-  switch (dtype) {
-    case FVR_F32:
-      slice3d_fwd_kernel<float><<<grid, 256, 0, s>>>(static_cast<const float*>(vol), (int)D, (int)H, (int)W, u, v,
-                                                     (int)N, fx, fy, (int)K, cx, cy, cz, static_cast<float*>(out));
-      break;
-    case FVR_BF16:
-      slice3d_fwd_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(vol), (int)D, (int)H,
-                                                             (int)W, u, v, (int)N, fx, fy, (int)K, cx, cy, cz,
-                                                             static_cast<__nv_bfloat16*>(out));
-      break;
-    case FVR_F16:
-      slice3d_fwd_kernel<__half><<<grid, 256, 0, s>>>(static_cast<const __half*>(vol), (int)D, (int)H, (int)W, u, v,
-                                                      (int)N, fx, fy, (int)K, cx, cy, cz, static_cast<__half*>(out));
-      break;
-    default:
-      return FVR_ERR_DTYPE;
-  }
-  FVR_LAUNCH_CHECK();
-  return FVR_OK;
-}
-
-int64_t fvr_slice3d_bwd_workspace(int64_t N, int64_t K) { return N * cdiv64(K, 256) * 6 * (int64_t)sizeof(double); }
-
-int fvr_slice3d_bwd(const void* vol, int dtype, int64_t B, int64_t D, int64_t H, int64_t W, const void* grad_out,
-                    const float* u, const float* v, int64_t N, const float* fx, const float* fy, int64_t K, float cx,
-                    float cy, float cz, float* gu, float* gv, void* workspace, int64_t ws_bytes, void* stream) {
-  if (!vol || !grad_out || !u || !v || !fx || !fy || !gu || !gv || !workspace) return FVR_ERR_ARG;
-  if (B < 1 || N < 1 || K < 1 || D < 1 || H < 1 || W < 1 || N > 65535) return FVR_ERR_ARG;
-  if (ws_bytes < fvr_slice3d_bwd_workspace(N, K)) return FVR_ERR_WORKSPACE;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int tiles = static_cast<int>(cdiv64(K, 256));
-  dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(N));
-  double* part = static_cast<double*>(workspace);
-  switch (dtype) {
-    case FVR_F32:
-      slice3d_bwd_kernel<float, float><<<grid, 256, 0, s>>>(static_cast<const float*>(vol), (int)B, (int)D, (int)H,
-                                                            (int)W, static_cast<const float*>(grad_out), u, v, (int)N,
-                                                            fx, fy, (int)K, cx, cy, cz, part);
-      break;
-    case FVR_BF16:
-      slice3d_bwd_kernel<__nv_bfloat16, __nv_bfloat16><<<grid, 256, 0, s>>>(
-          static_cast<const __nv_bfloat16*>(vol), (int)B, (int)D, (int)H, (int)W,
-          static_cast<const __nv_bfloat16*>(grad_out), u, v, (int)N, fx, fy, (int)K, cx, cy, cz, part);
-      break;
-    case FVR_F16:
-      slice3d_bwd_kernel<__half, __half><<<grid, 256, 0, s>>>(static_cast<const __half*>(vol), (int)B, (int)D,
-                                                              (int)H, (int)W, static_cast<const __half*>(grad_out), u,
-                                                              v, (int)N, fx, fy, (int)K, cx, cy, cz, part);
-      break;
-    default:
-      return FVR_ERR_DTYPE;
-  }
-  FVR_LAUNCH_CHECK();
-  slice3d_bwd_finalize_kernel<<<static_cast<unsigned>(cdiv64(N * 6, 256)), 256, 0, s>>>(part, (int)N, tiles, gu, gv);
-  FVR_LAUNCH_CHECK();
-  return FVR_OK;
-}
-
-int fvr_tc_axes(const float* poses, int64_t C, int view, int64_t D, int64_t H, int64_t W, float* axes,
+int fvr_tc_axes(const float* poses, int64_t C, int view, int64_t D, int64_t H, int64_t W, double* axes,
                 void* stream) {
   if (!poses || !axes || C < 1 || (view != 0 && view != 1)) return FVR_ERR_ARG;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const double sx = 0.5 * static_cast<double>(W > 1 ? W - 1 : 1);
-  const double sy = 0.5 * static_cast<double>(H > 1 ? H - 1 : 1);
-  const double sz = 0.5 * static_cast<double>(D > 1 ? D - 1 : 1);
-  tc_axes_kernel<<<static_cast<unsigned>(cdiv64(C, 128)), 128, 0, s>>>(poses, (int)C, view, sx, sy, sz, axes);
+  tc_axes_kernel<<<static_cast<unsigned>(cdiv64(C, 128)), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      poses, (int)C, view, half_extent(W), half_extent(H), half_extent(D), axes);
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }
 
-int64_t fvr_tc_sncc_workspace(int64_t C, int64_t R) {
-  return C * cdiv64(R * R, kSnccTile) * M_NGRAD * (int64_t)sizeof(double);
+int64_t fvr_tc_sncc_workspace(int64_t C, int64_t R, int64_t nviews) {
+  return nviews * C * cdiv64(R * R, kSnccThreads) * M_NGRAD * (int64_t)sizeof(double);
 }
 
+int64_t fvr_tc_sncc_mom_stride(void) { return kMomStride; }
+
 int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
-                        const float* axes, int64_t C, const void* ftarg, const float* hp, const float* lin,
-                        int64_t R, double kappa, int with_grad, void* workspace, int64_t ws_bytes, void* stream) {
+                        const float* poses, int64_t C, int nviews, const int* views, const void* const* ftargs,
+                        const float* hp, const float* lin, int64_t R, double kappa, int with_grad, void* workspace,
+                        int64_t ws_bytes, void* stream) {
   Stencil st;
   int rc = stencil_from(dtype, stencil, scales, D, H, W, &st);
   if (rc) return rc;
-  if (!axes || !ftarg || !lin || !workspace || C < 1 || R < 1 || C > 65535) return FVR_ERR_ARG;
-  if (R * R > (int64_t)1 << 30) return FVR_ERR_ARG;
-  if (ws_bytes < fvr_tc_sncc_workspace(C, R)) return FVR_ERR_WORKSPACE;
+  if (!poses || !views || !ftargs || !lin || !workspace || C < 1 || R < 1 || C > 65535) return FVR_ERR_ARG;
+  if (nviews < 1 || nviews > kMaxViews || R * R > (int64_t)1 << 30) return FVR_ERR_ARG;
+  if (ws_bytes < fvr_tc_sncc_workspace(C, R, nviews)) return FVR_ERR_WORKSPACE;
+  const int64_t K = R * R;
+  const int tile = sncc_tile(C, K, nviews);
+  SnccArgs a{};
+  a.st = st;
+  a.poses = poses;
+  for (int v = 0; v < nviews; ++v) {
+    if (!ftargs[v] || (views[v] != 0 && views[v] != 1)) return FVR_ERR_ARG;
+    a.ftarg[v] = static_cast<const float2*>(ftargs[v]);
+    a.lateral[v] = views[v];
+  }
+  a.hp = hp;
+  a.lin = lin;
+  a.R = (int)R;
+  a.C = (int)C;
+  a.tile = tile;
+  a.kpi = kappa / 3.14159265358979323846;
+  a.sx = half_extent(W);
+  a.sy = half_extent(H);
+  a.sz = half_extent(D);
+  a.partial = static_cast<double*>(workspace);
+  dim3 grid(static_cast<unsigned>(cdiv64(K, tile)), static_cast<unsigned>(C), static_cast<unsigned>(nviews));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int tiles = static_cast<int>(cdiv64(R * R, kSnccTile));
-  SnccArgs a{st,
-             axes,
-             static_cast<const float2*>(ftarg),
-             hp,
-             lin,
-             (int)R,
-             static_cast<float>(kappa / 3.14159265358979323846),
-             static_cast<float>(0.5 * (W > 1 ? W - 1 : 1)),
-             static_cast<float>(0.5 * (H > 1 ? H - 1 : 1)),
-             static_cast<float>(0.5 * (D > 1 ? D - 1 : 1)),
-             static_cast<double*>(workspace)};
-  dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(C));
 #define FVR_SNCC(DT)                                                    \
   if (with_grad)                                                        \
     tc_sncc_moments_kernel<DT, true><<<grid, kSnccThreads, 0, s>>>(a);  \
@@ -816,45 +482,55 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
   return FVR_OK;
 }
 
-int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int with_grad, double* mom, float* loss,
-                         float* ncc_out, void* stream) {
-  if (!workspace || !mom || !loss || C < 1 || R < 1) return FVR_ERR_ARG;
-  const int tiles = static_cast<int>(cdiv64(R * R, kSnccTile));
-  tc_sncc_finalize_kernel<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      static_cast<const double*>(workspace), (int)C, tiles, with_grad ? M_NGRAD : 3, mom, loss, ncc_out);
+int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews, int with_grad, double* mom,
+                         float* loss, float* ncc_out, void* stream) {
+  if (!workspace || !mom || !loss || C < 1 || R < 1 || nviews < 1 || nviews > kMaxViews) return FVR_ERR_ARG;
+  const int64_t K = R * R;
+  const int tiles = static_cast<int>(cdiv64(K, sncc_tile(C, K, nviews)));
+  tc_sncc_finalize_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const double*>(workspace), (int)C, nviews, tiles, with_grad ? M_NGRAD : 3, mom, loss, ncc_out);
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }
 
-int fvr_tc_sncc_backward(const double* mom, const float* g, const float* poses, int64_t C, int view, int64_t D,
-                         int64_t H, int64_t W, double kappa, float* grad_poses, int accumulate, void* stream) {
-  if (!mom || !g || !poses || !grad_poses || C < 1 || (view != 0 && view != 1)) return FVR_ERR_ARG;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  tc_pose_grad_kernel<<<static_cast<unsigned>(cdiv64(C, 128)), 128, 0, s>>>(
-      0, mom, 1, g, poses, (int)C, view, 0.5 * (W > 1 ? W - 1 : 1), 0.5 * (H > 1 ? H - 1 : 1),
-      0.5 * (D > 1 ? D - 1 : 1), kappa, grad_poses, accumulate);
+int fvr_tc_sncc_backward(const double* mom, int nviews, const int* views, const float* g, int64_t g_stride,
+                         const float* poses, int64_t C, int64_t D, int64_t H, int64_t W, double kappa,
+                         float* grad_poses, int accumulate, void* stream) {
+  if (!mom || !views || !g || !poses || !grad_poses || C < 1 || nviews < 1 || nviews > kMaxViews)
+    return FVR_ERR_ARG;
+  SnccGradArgs a{};
+  a.mom = mom;
+  a.g = g;
+  a.g_stride = (int)g_stride;
+  a.poses = poses;
+  a.C = (int)C;
+  a.nv = nviews;
+  for (int v = 0; v < nviews; ++v) {
+    if (views[v] != 0 && views[v] != 1) return FVR_ERR_ARG;
+    a.lateral[v] = views[v];
+  }
+  a.sx = half_extent(W);
+  a.sy = half_extent(H);
+  a.sz = half_extent(D);
+  a.kappa = kappa;
+  a.grad = grad_poses;
+  a.accumulate = accumulate;
+  tc_sncc_grad_kernel<<<static_cast<unsigned>(cdiv64(C, 128)), 128, 0, static_cast<cudaStream_t>(stream)>>>(a);
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }
 
 int fvr_tc_slice(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
-                 const float* axes, int64_t C, const float* lin, int64_t R, double kappa, int shift, void* out,
+                 const double* axes, int64_t C, const float* lin, int64_t R, double kappa, int shift, void* out,
                  void* stream) {
   Stencil st;
   int rc = stencil_from(dtype, stencil, scales, D, H, W, &st);
   if (rc) return rc;
   if (!axes || !lin || !out || C < 1 || R < 1 || C > 65535 || R * R > (int64_t)1 << 30) return FVR_ERR_ARG;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  SliceArgs a{st,
-              axes,
-              lin,
-              (int)R,
-              static_cast<float>(kappa / 3.14159265358979323846),
-              static_cast<float>(0.5 * (W > 1 ? W - 1 : 1)),
-              static_cast<float>(0.5 * (H > 1 ? H - 1 : 1)),
-              static_cast<float>(0.5 * (D > 1 ? D - 1 : 1)),
-              shift ? 1 : 0};
+  SliceArgs a{st, axes, lin, (int)R, kappa / 3.14159265358979323846, half_extent(W), half_extent(H),
+              half_extent(D), shift ? 1 : 0};
   dim3 grid(static_cast<unsigned>(cdiv64(R * R, 256)), static_cast<unsigned>(C));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   float2* o = static_cast<float2*>(out);
   switch (dtype) {
     case FVR_F32: tc_slice_kernel<FVR_F32><<<grid, 256, 0, s>>>(a, o); break;
@@ -870,27 +546,21 @@ int64_t fvr_tc_slice_adjoint_workspace(int64_t C, int64_t R) {
 }
 
 int fvr_tc_slice_adjoint(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
-                         const float* axes, const float* poses, int64_t C, int view, const float* lin, int64_t R,
+                         const double* axes, const float* poses, int64_t C, int view, const float* lin, int64_t R,
                          double kappa, int shift, const void* G, void* workspace, int64_t ws_bytes,
                          float* grad_poses, int accumulate, void* stream) {
   Stencil st;
   int rc = stencil_from(dtype, stencil, scales, D, H, W, &st);
   if (rc) return rc;
-  if (!axes || !poses || !lin || !G || !workspace || !grad_poses || C < 1 || R < 1 || C > 65535) return FVR_ERR_ARG;
+  if (!axes || !poses || !lin || !G || !workspace || !grad_poses || C < 1 || R < 1 || C > 65535)
+    return FVR_ERR_ARG;
   if (view != 0 && view != 1) return FVR_ERR_ARG;
   if (ws_bytes < fvr_tc_slice_adjoint_workspace(C, R)) return FVR_ERR_WORKSPACE;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  SliceArgs a{st,
-              axes,
-              lin,
-              (int)R,
-              static_cast<float>(kappa / 3.14159265358979323846),
-              static_cast<float>(0.5 * (W > 1 ? W - 1 : 1)),
-              static_cast<float>(0.5 * (H > 1 ? H - 1 : 1)),
-              static_cast<float>(0.5 * (D > 1 ? D - 1 : 1)),
-              shift ? 1 : 0};
+  SliceArgs a{st, axes, lin, (int)R, kappa / 3.14159265358979323846, half_extent(W), half_extent(H),
+              half_extent(D), shift ? 1 : 0};
   const int tiles = static_cast<int>(cdiv64(R * R, 256));
   dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(C));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* part = static_cast<double*>(workspace);
   const float2* g = static_cast<const float2*>(G);
   switch (dtype) {
@@ -899,41 +569,9 @@ int fvr_tc_slice_adjoint(int dtype, const void* stencil, const float* scales, in
     case FVR_F16: tc_slice_adjoint_kernel<FVR_F16><<<grid, 256, 0, s>>>(a, g, part); break;
   }
   FVR_LAUNCH_CHECK();
-  tc_pose_grad_kernel<<<static_cast<unsigned>(cdiv64(C, 128)), 128, 0, s>>>(
-      1, part, tiles, nullptr, poses, (int)C, view, 0.5 * (W > 1 ? W - 1 : 1), 0.5 * (H > 1 ? H - 1 : 1),
-      0.5 * (D > 1 ? D - 1 : 1), kappa, grad_poses, accumulate);
-  FVR_LAUNCH_CHECK();
-  return FVR_OK;
-}
-
-int fvr_relu_mask(const float* img, const float* g, float* out, int64_t n, void* stream) {
-  if (!img || !g || !out || n < 1) return FVR_ERR_ARG;
-  relu_mask_kernel<<<static_cast<unsigned>(cdiv64(n, 256)), 256, 0, static_cast<cudaStream_t>(stream)>>>(img, g,
-                                                                                                          out, n);
-  FVR_LAUNCH_CHECK();
-  return FVR_OK;
-}
-
-int fvr_cmul_table(void* x, const float* table, int64_t per, int64_t n, void* stream) {
-  if (!x || !table || per < 1 || n < 1) return FVR_ERR_ARG;
-  cmul_table_kernel<<<static_cast<unsigned>(cdiv64(n, 256)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      static_cast<float2*>(x), table, per, n);
-  FVR_LAUNCH_CHECK();
-  return FVR_OK;
-}
-
-int fvr_hp_filter(float* out, int64_t H, int64_t W, double sigma, void* stream) {
-  if (!out || H < 1 || W < 1 || H * W > (int64_t)1 << 30) return FVR_ERR_ARG;
-  hp_filter_kernel<<<static_cast<unsigned>(cdiv64(H * W, 256)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      out, (int)H, (int)W, sigma);
-  FVR_LAUNCH_CHECK();
-  return FVR_OK;
-}
-
-int fvr_linspace(float* out, float start, float end, int64_t n, void* stream) {
-  if (!out || n < 1 || n > (int64_t)1 << 30) return FVR_ERR_ARG;
-  linspace_kernel<<<static_cast<unsigned>(cdiv64(n, 256)), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      out, start, end, (int)n);
+  tc_adjoint_grad_kernel<<<static_cast<unsigned>(cdiv64(C, 128)), 128, 0, s>>>(
+      part, tiles, poses, (int)C, view, half_extent(W), half_extent(H), half_extent(D), kappa, grad_poses,
+      accumulate);
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }

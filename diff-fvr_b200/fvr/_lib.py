@@ -42,11 +42,12 @@ SIGNATURES = {
     "fvr_slice3d_bwd_workspace": (I64, [I64, I64]),
     "fvr_slice3d_bwd": (I32, [P, I32, I64, I64, I64, I64, P, P, P, I64, P, P, I64, F32, F32, F32, P, P, P, I64, P]),
     "fvr_tc_axes": (I32, [P, I64, I32, I64, I64, I64, P, P]),
-    "fvr_tc_sncc_workspace": (I64, [I64, I64]),
-    "fvr_tc_sncc_moments": (I32, [I32, P, P, I64, I64, I64, P, I64, P, P, P, I64, F64, I32, P, I64, P]),
-    "fvr_tc_sncc_finalize": (I32, [P, I64, I64, I32, P, P, P, P]),
+    "fvr_tc_sncc_workspace": (I64, [I64, I64, I64]),
+    "fvr_tc_sncc_mom_stride": (I64, []),
+    "fvr_tc_sncc_moments": (I32, [I32, P, P, I64, I64, I64, P, I64, I32, P, P, P, P, I64, F64, I32, P, I64, P]),
+    "fvr_tc_sncc_finalize": (I32, [P, I64, I64, I32, I32, P, P, P, P]),
     "fvr_event_record": (I32, [P, P, I32]),
-    "fvr_tc_sncc_backward": (I32, [P, P, P, I64, I32, I64, I64, I64, F64, P, I32, P]),
+    "fvr_tc_sncc_backward": (I32, [P, I32, P, P, I64, P, I64, I64, I64, I64, F64, P, I32, P]),
     "fvr_tc_slice": (I32, [I32, P, P, I64, I64, I64, P, I64, P, I64, F64, I32, P, P]),
     "fvr_tc_slice_adjoint_workspace": (I64, [I64, I64]),
     "fvr_tc_slice_adjoint": (I32, [I32, P, P, I64, I64, I64, P, P, I64, I32, P, I64, F64, I32, P, P, I64, P, I32, P]),

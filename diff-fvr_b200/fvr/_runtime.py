@@ -14,6 +14,7 @@ from . import _lib as L
 _tw_cache = {}
 _lin_cache = {}
 _hp_cache = {}
+_one_cache = {}
 
 
 def device_of(device):
@@ -35,6 +36,16 @@ def twiddles(n, prec, device):
         t = torch.empty((int(n), 2), dtype=torch.float64 if prec == L.F64_ else torch.float32, device=device)
         L.call("fvr_fft_twiddles", int(n), prec, L.ptr(t), L.stream_ptr(device))
         _tw_cache[key] = t
+    return t
+
+
+def ones(device):
+    """A device-resident float32 1.0 (upstream gradient of a loss that is not
+    differentiated further)."""
+    t = _one_cache.get(device.index)
+    if t is None:
+        t = torch.ones(1, dtype=torch.float32, device=device)
+        _one_cache[device.index] = t
     return t
 
 

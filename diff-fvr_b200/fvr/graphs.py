@@ -52,7 +52,9 @@ class GraphedCallable:
 class BiplanarSpectralNCCStep:
     """``loss = forward_spectral_ncc(AP) + forward_spectral_ncc(lateral)`` and
     ``dloss/dposes`` for a batch of candidate poses on a
-    :class:`fvr.torch_engine.TorchDiffFVREngine`, as one callable.
+    :class:`fvr.torch_engine.TorchDiffFVREngine`, as one callable: one fused
+    gather pass over both views, an fp64 finalize, an fp64 pose-gradient
+    epilogue.
 
     With ``graph=True`` (default) the whole step is a single CUDA-graph replay
     that uses the engine's spectrum storage of the time of capture (the step
@@ -72,13 +74,8 @@ class BiplanarSpectralNCCStep:
         self._g = GraphedCallable(self._step, ex, warmup=warmup, capture_context=capture_context) if graph else None
 
     def _step(self, poses):
-        p = poses.detach().requires_grad_(True)
-        e = self.engine
-        loss = e.forward_spectral_ncc(p, self.f_ap, view="ap", high_pass=self.hp, cutoff_sigma=self.sigma)
-        loss = loss + e.forward_spectral_ncc(p, self.f_lat, view="lateral", high_pass=self.hp,
-                                             cutoff_sigma=self.sigma)
-        (grad,) = torch.autograd.grad(loss, p)
-        return loss.detach(), grad
+        return self.engine.spectral_ncc_value_and_grad(poses, (self.f_ap, self.f_lat), ("ap", "lateral"),
+                                                       high_pass=self.hp, cutoff_sigma=self.sigma)
 
     def __call__(self, poses):
         if self._g is None:

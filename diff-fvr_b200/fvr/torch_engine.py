@@ -24,6 +24,8 @@ from __future__ import annotations
 
 from typing import Optional, Tuple, Union
 
+import ctypes
+
 import numpy as np
 import torch
 import torch.nn as nn
@@ -39,46 +41,63 @@ def _view_code(view: str) -> int:
     return VIEW_LATERAL if str(view).lower() == "lateral" else VIEW_AP
 
 
+def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
+    """Launch the fused moments pass + finalize for len(views) views.
+    Returns (mom [nv, C, 18] fp64, loss [nv + 1] f32: per view, then the sum)."""
+    dev = eng._dev
+    C = int(p.shape[0])
+    nv = len(views)
+    st = eng._stencil
+    ws_bytes = L.query("fvr_tc_sncc_workspace", C, R, nv)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    mom = torch.empty((nv, C, int(L.query("fvr_tc_sncc_mom_stride"))), dtype=torch.float64, device=dev)
+    loss = torch.empty(nv + 1, dtype=torch.float32, device=dev)
+    fts = [f.detach().to(device=dev, dtype=torch.complex64).contiguous() for f in ftargs]
+    for f in fts:
+        if f.numel() != R * R:
+            raise L.FvrError(f"target spectrum has {f.numel()} elements, expected {R}x{R}")
+    vcodes = (ctypes.c_int * nv)(*views)
+    fptrs = (ctypes.c_void_p * nv)(*[f.data_ptr() for f in fts])
+    kap = RT.kappa(R, eng.spacing[0])
+    s = L.stream_ptr(dev)
+    with profiling.section("tc_sncc_moments"):
+        L.call("fvr_tc_sncc_moments", *st.args(), L.ptr(p), C, nv, vcodes, fptrs, L.ptr(hp),
+               L.ptr(RT.linspace(R, dev)), R, kap, int(with_grad), L.ptr(ws), ws_bytes, s)
+    L.call("fvr_tc_sncc_finalize", L.ptr(ws), C, R, nv, int(with_grad), L.ptr(mom), L.ptr(loss), None, s)
+    return mom, loss
+
+
+def _sncc_backward(eng, p, views, mom, g, g_stride, R, out=None):
+    dev = p.device
+    C = int(p.shape[0])
+    D, H, W = eng._stencil.dims
+    grad = torch.empty((C, 6), dtype=torch.float32, device=dev) if out is None else out
+    nv = len(views)
+    L.call("fvr_tc_sncc_backward", L.ptr(mom), nv, (ctypes.c_int * nv)(*views), L.ptr(g), int(g_stride), L.ptr(p),
+           C, D, H, W, RT.kappa(R, eng.spacing[0]), L.ptr(grad), 0, L.stream_ptr(dev))
+    return grad
+
+
 class _SpectralNCCFn(torch.autograd.Function):
-    """Zero-IFFT spectral NCC (torch_engine.py:269-307) with a moment-based adjoint."""
+    """Zero-IFFT spectral NCC (torch_engine.py:269-307), summed over the given
+    views, with a moment-based adjoint."""
 
     @staticmethod
-    def forward(ctx, poses, f_targ, eng, view, hp, R):
-        dev = eng._dev
-        p = poses.detach().to(device=dev, dtype=torch.float32).contiguous()
-        C = int(p.shape[0])
-        st = eng._stencil
-        D, H, W = st.dims
-        axes = torch.empty((C, 8), dtype=torch.float32, device=dev)
-        s = L.stream_ptr(dev)
-        L.call("fvr_tc_axes", L.ptr(p), C, view, D, H, W, L.ptr(axes), s)
+    def forward(ctx, poses, eng, views, hp, R, *ftargs):
+        p = poses.detach().to(device=eng._dev, dtype=torch.float32).contiguous()
         with_grad = bool(ctx.needs_input_grad[0])
-        nm = 17 if with_grad else 3
-        ws_bytes = L.query("fvr_tc_sncc_workspace", C, R)
-        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
-        mom = torch.empty((C, nm), dtype=torch.float64, device=dev)
-        loss = torch.empty((), dtype=torch.float32, device=dev)
-        ft = f_targ.detach().to(device=dev, dtype=torch.complex64).contiguous()
-        kap = RT.kappa(R, eng.spacing[0])
-        with profiling.section("tc_sncc_moments"):
-            L.call("fvr_tc_sncc_moments", *st.args(), L.ptr(axes), C, L.ptr(ft), L.ptr(hp),
-                   L.ptr(RT.linspace(R, dev)), R, kap, int(with_grad), L.ptr(ws), ws_bytes, s)
-        L.call("fvr_tc_sncc_finalize", L.ptr(ws), C, R, int(with_grad), L.ptr(mom), L.ptr(loss), None, s)
+        mom, loss = _sncc_forward(eng, p, views, ftargs, hp, R, with_grad)
         ctx.save_for_backward(p, mom)
-        ctx.meta = (eng._stencil.dims, view, kap, poses.dtype)
-        return loss
+        ctx.meta = (eng, views, R, poses.dtype)
+        return loss[len(views)]
 
     @staticmethod
     def backward(ctx, g):
         p, mom = ctx.saved_tensors
-        (D, H, W), view, kap, pdt = ctx.meta
-        C = int(p.shape[0])
-        dev = p.device
-        grad = torch.empty((C, 6), dtype=torch.float32, device=dev)
-        gg = g.detach().to(device=dev, dtype=torch.float32).contiguous()
-        L.call("fvr_tc_sncc_backward", L.ptr(mom), L.ptr(gg), L.ptr(p), C, view, D, H, W, kap, L.ptr(grad), 0,
-               L.stream_ptr(dev))
-        return grad.to(pdt), None, None, None, None, None
+        eng, views, R, pdt = ctx.meta
+        gg = g.detach().to(device=p.device, dtype=torch.float32).reshape(1).contiguous()
+        grad = _sncc_backward(eng, p, views, mom, gg, 0, R)
+        return (grad.to(pdt), None, None, None, None) + (None,) * len(views)
 
 
 class _SliceFn(torch.autograd.Function):
@@ -92,7 +111,7 @@ class _SliceFn(torch.autograd.Function):
         C = int(p.shape[0])
         st = eng._stencil
         D, H, W = st.dims
-        axes = torch.empty((C, 8), dtype=torch.float32, device=dev)
+        axes = torch.empty((C, 8), dtype=torch.float64, device=dev)
         s = L.stream_ptr(dev)
         L.call("fvr_tc_axes", L.ptr(p), C, view, D, H, W, L.ptr(axes), s)
         out = torch.empty((C, R, R), dtype=torch.complex64, device=dev)
@@ -135,7 +154,7 @@ class _ImageFn(torch.autograd.Function):
         C = int(p.shape[0])
         st = eng._stencil
         D, H, W = st.dims
-        axes = torch.empty((C, 8), dtype=torch.float32, device=dev)
+        axes = torch.empty((C, 8), dtype=torch.float64, device=dev)
         s = L.stream_ptr(dev)
         L.call("fvr_tc_axes", L.ptr(p), C, view, D, H, W, L.ptr(axes), s)
         buf = torch.empty((C, R, R), dtype=torch.complex64, device=dev)
@@ -308,13 +327,35 @@ class TorchDiffFVREngine(nn.Module):
     def _spectral_ncc_core(self, poses, f_targ_precomputed, view="ap", high_pass=True, cutoff_sigma=4.0):
         R = int(f_targ_precomputed.shape[-1])
         hp = RT.hp_filter(R, R, cutoff_sigma, self._dev) if high_pass else None
-        return _SpectralNCCFn.apply(self._prep_poses(poses), f_targ_precomputed, self, _view_code(view), hp, R)
+        return _SpectralNCCFn.apply(self._prep_poses(poses), self, (_view_code(view),), hp, R, f_targ_precomputed)
 
     def forward_spectral_ncc(self, poses: torch.Tensor, f_targ_precomputed: torch.Tensor, view: str = "ap",
                              high_pass: bool = True, cutoff_sigma: float = 4.0) -> torch.Tensor:
         """Zero-IFFT Parseval spectral-NCC loss ``1 - mean_B NCC`` (torch_engine.py:292-307)."""
         return self._spectral_ncc_core(poses, f_targ_precomputed, view=view, high_pass=high_pass,
                                        cutoff_sigma=cutoff_sigma)
+
+    def forward_spectral_ncc_multiview(self, poses, f_targs, views=("ap", "lateral"), high_pass=True,
+                                       cutoff_sigma=4.0):
+        """``sum_v forward_spectral_ncc(poses, f_targs[v], views[v])`` in one fused launch
+        (all views of all candidates share the gather pass); differentiable in poses."""
+        R = int(f_targs[0].shape[-1])
+        hp = RT.hp_filter(R, R, cutoff_sigma, self._dev) if high_pass else None
+        codes = tuple(_view_code(v) for v in views)
+        return _SpectralNCCFn.apply(self._prep_poses(poses), self, codes, hp, R, *f_targs)
+
+    def spectral_ncc_value_and_grad(self, poses, f_targs, views=("ap", "lateral"), high_pass=True,
+                                    cutoff_sigma=4.0, out_grad=None):
+        """``(sum_v loss_v, dloss/dposes [C, 6])`` without autograd: one fused gather pass
+        for every candidate and view, an fp64 finalize and an fp64 pose-gradient epilogue
+        (three kernel launches; capturable in a CUDA graph)."""
+        p = self._prep_poses(poses).detach().to(torch.float32).contiguous()
+        R = int(f_targs[0].shape[-1])
+        hp = RT.hp_filter(R, R, cutoff_sigma, self._dev) if high_pass else None
+        codes = tuple(_view_code(v) for v in views)
+        mom, loss = _sncc_forward(self, p, codes, f_targs, hp, R, True)
+        grad = _sncc_backward(self, p, codes, mom, RT.ones(self._dev), 0, R, out=out_grad)
+        return loss[len(codes)], grad
 
     def spectral_ncc_loss(self, pred_drr: torch.Tensor, target_drr: torch.Tensor, high_pass: bool = True,
                           cutoff_sigma: float = 4.0) -> torch.Tensor:

@@ -99,44 +99,53 @@ int fvr_slice3d_bwd(const void* vol, int dtype, int64_t B, int64_t D, int64_t H,
                     float cy, float cz, float* gu, float* gv, void* workspace, int64_t ws_bytes, void* stream);
 
 /* -------------------------------------- parallel-beam (torch engine) ---- */
-/* Slice axes for poses[C][6] (yaw, pitch, roll deg; tx, ty, tz): axes[C][8] =
- * (u_xyz, v_xyz, tx, ty), u = R[0,:]*((W-1)/2,(H-1)/2,(D-1)/2), v = R[1,:]*(..),
- * R = Rz(yaw) Ry(pitch) Rx(roll) in fp64, lateral view R . Rz(90 deg).
- * view 0 = 'ap', 1 = 'lateral'.  src/fvr/torch_engine.py:139-211. */
-int fvr_tc_axes(const float* poses, int64_t C, int view, int64_t D, int64_t H, int64_t W, float* axes,
+/* Slice axes for poses[C][6] (yaw, pitch, roll deg; tx, ty, tz): axes[C][8]
+ * (fp64) = (u_xyz, v_xyz, tx, ty), u = R[0,:]*((W-1)/2,(H-1)/2,(D-1)/2),
+ * v = R[1,:]*(..), R = Rz(yaw) Ry(pitch) Rx(roll) in fp64, lateral view
+ * R . Rz(90 deg).  view 0 = 'ap', 1 = 'lateral'.  src/fvr/torch_engine.py:139-211. */
+int fvr_tc_axes(const float* poses, int64_t C, int view, int64_t D, int64_t H, int64_t W, double* axes,
                 void* stream);
-int64_t fvr_tc_sncc_workspace(int64_t C, int64_t R);
-/* Fused zero-IFFT spectral NCC, pass 1: per candidate one pass gathering the
- * slice, applying the phase ramp kappa*(ku tx + kv ty) and the high-pass
- * table hp (NULL = none), and reducing the NCC moments against ftarg[R][R]
- * (complex); with_grad also reduces the 14 pose-gradient moments.  Per-tile
- * partial sums go to `workspace`.  lin = torch.linspace(-1, 1, R).
+int64_t fvr_tc_sncc_workspace(int64_t C, int64_t R, int64_t nviews);
+/* Per-(view, candidate) record length of `mom` (17 moments + ncc). */
+int64_t fvr_tc_sncc_mom_stride(void);
+/* Fused zero-IFFT spectral NCC, pass 1: for every candidate and each of
+ * nviews (<= 4) views (views[v] = 0 'ap' / 1 'lateral', ftargs[v] the
+ * complex [R][R] target spectrum of that view, host arrays of device
+ * pointers) one pass forms the slice axes from the pose in fp64, gathers the
+ * slice at fp64 positions, applies the phase ramp kappa*(ku tx + kv ty) and
+ * the high-pass table hp (NULL = none), and reduces the NCC moments; with
+ * with_grad also the 14 pose-gradient moments.  Per-tile partial sums go to
+ * `workspace`.  lin = torch.linspace(-1, 1, R).
  * Replaces TorchDiffFVREngine._spectral_ncc_core / forward_spectral_ncc,
  * src/fvr/torch_engine.py:269-307 (the gather of :176-234 included). */
 int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
-                        const float* axes, int64_t C, const void* ftarg, const float* hp, const float* lin,
-                        int64_t R, double kappa, int with_grad, void* workspace, int64_t ws_bytes, void* stream);
-/* Pass 2: tile sums in fp64 -> mom[C][17 or 3] (kept for the backward);
- * loss = 1 - mean_c ncc_c (f32 scalar); ncc_out[C] optional. */
-int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int with_grad, double* mom, float* loss,
-                         float* ncc_out, void* stream);
-/* dL/dposes[C][6] from the saved moments and the device scalar g = dL/dloss
- * (tz column is zero: the reference never reads poses[:, 5]).  accumulate != 0
- * adds into grad_poses.  Autograd backward of torch_engine.py:269-307. */
-int fvr_tc_sncc_backward(const double* mom, const float* g, const float* poses, int64_t C, int view, int64_t D,
-                         int64_t H, int64_t W, double kappa, float* grad_poses, int accumulate, void* stream);
-/* Modulated slice S*exp(i phase) -> out[C][R][R] complex; shift != 0 writes it
- * in ifftshift order (input of the image IFFT).
+                        const float* poses, int64_t C, int nviews, const int* views, const void* const* ftargs,
+                        const float* hp, const float* lin, int64_t R, double kappa, int with_grad, void* workspace,
+                        int64_t ws_bytes, void* stream);
+/* Pass 2: tile sums in fp64 -> mom[nviews][C][stride] (kept for the
+ * backward); loss[v] = 1 - mean_c ncc (f32), loss[nviews] = sum of the view
+ * losses; ncc_out[nviews][C] optional. */
+int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews, int with_grad, double* mom,
+                         float* loss, float* ncc_out, void* stream);
+/* dL/dposes[C][6] from the saved moments and the device scalars
+ * g[v * g_stride] = dL/dloss_v (tz column is zero: the reference never reads
+ * poses[:, 5]); accumulate != 0 adds into grad_poses.
+ * Autograd backward of torch_engine.py:269-307. */
+int fvr_tc_sncc_backward(const double* mom, int nviews, const int* views, const float* g, int64_t g_stride,
+                         const float* poses, int64_t C, int64_t D, int64_t H, int64_t W, double kappa,
+                         float* grad_poses, int accumulate, void* stream);
+/* Modulated slice S*exp(i phase) -> out[C][R][R] complex from fp64 axes;
+ * shift != 0 writes it in ifftshift order (input of the image IFFT).
  * Replaces TorchDiffFVREngine._extract_slice_spectrum, torch_engine.py:176-234. */
 int fvr_tc_slice(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
-                 const float* axes, int64_t C, const float* lin, int64_t R, double kappa, int shift, void* out,
+                 const double* axes, int64_t C, const float* lin, int64_t R, double kappa, int shift, void* out,
                  void* stream);
 int64_t fvr_tc_slice_adjoint_workspace(int64_t C, int64_t R);
 /* Pose gradient for an upstream gradient G[C][R][R] (complex) with respect to
  * the modulated slice (same order as fvr_tc_slice with the same shift).
  * Autograd backward of torch_engine.py:176-241. */
 int fvr_tc_slice_adjoint(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
-                         const float* axes, const float* poses, int64_t C, int view, const float* lin, int64_t R,
+                         const double* axes, const float* poses, int64_t C, int view, const float* lin, int64_t R,
                          double kappa, int shift, const void* G, void* workspace, int64_t ws_bytes,
                          float* grad_poses, int accumulate, void* stream);
 /* out = (img > 0) ? g : 0  (ReLU adjoint of torch_engine.py:240) */

@@ -126,3 +126,11 @@ def test_c_oracle_matches_numpy_oracle_and_golden(golden, view):
     assert rel_l2(grad, ref_grad) < 1e-10
     m = _grad_mask(grad)
     assert rel_l2(grad[m], g[f"sncc_grad_{view}"][m]) < 2e-5
+
+
+def test_product_and_oracle_generators_agree():
+    """bench.py draws its inputs from fvr.synthetic; the oracle has its own copy."""
+    from fvr import synthetic
+
+    assert np.array_equal(synthetic.make_ellipsoid_volume(20, 3), tc.make_ellipsoid_volume(20, 3))
+    assert np.array_equal(synthetic.make_poses(7, 4), tc.make_poses(7, 4))
