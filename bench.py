@@ -56,58 +56,77 @@ def _peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+_SAMPLER = r"""
+import sys, time
+import pynvml
+pynvml.nvmlInit()
+ident = sys.argv[1]
+h = pynvml.nvmlDeviceGetHandleByUUID(ident) if ident.startswith("GPU-") else pynvml.nvmlDeviceGetHandleByIndex(int(ident))
+print("max", pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM), flush=True)
+get_r = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+while True:
+    t = time.time()
+    print(f"{t:.6f} {pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)} {int(get_r(h))}", flush=True)
+    time.sleep(0.002)
+"""
+
+_REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+            0x80: "hw_power_brake_slowdown"}
+
+
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and clock-event reasons sampled by NVML every ~2 ms in a
+    separate process; only the samples inside the marked window are kept."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, gpu_index):
-        self.idx = gpu_index
+    def __init__(self, torch, dev):
+        try:
+            ident = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+        except Exception:
+            ident = str(dev.index or 0)
+        self.ident = ident
         self.proc = None
-        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"fvr_clocks_{os.getpid()}.csv"
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
-                                         stderr=subprocess.DEVNULL)
+            self.proc = subprocess.Popen([sys.executable, "-c", _SAMPLER, self.ident], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            line = self.proc.stdout.readline()  # "max <MHz>": the sampler is running
+            self.max_mhz = float(line.split()[1]) if line.startswith("max") else None
         except Exception:
             self.proc = None
+
+    def mark(self, begin):
+        if begin:
+            self.t0 = time.time()
+        else:
+            self.t1 = time.time()
 
     def stop(self):
         if self.proc is None:
             return None
+        time.sleep(0.01)
         self.proc.terminate()
         try:
-            self.proc.wait(timeout=5)
+            out, _ = self.proc.communicate(timeout=5)
         except Exception:
             self.proc.kill()
-        self.fh.close()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        try:
-            self.path.unlink()
-        except Exception:
-            pass
-        if not sm:
+            out, _ = self.proc.communicate()
+        rows = []
+        for line in out.splitlines():
+            f = line.split()
+            if len(f) == 3:
+                rows.append((float(f[0]), float(f[1]), int(f[2])))
+        inside = [r for r in rows if self.t0 is not None and self.t0 <= r[0] <= self.t1]
+        window = "timed region"
+        if len(inside) < 3:  # timed region shorter than a few sampling periods
+            inside = [r for r in rows if self.t0 - 0.05 <= r[0] <= self.t1 + 0.05]
+            window = "timed region +- 50 ms"
+        if not inside:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted({name for _, _, m in inside for bit, name in _REASONS.items() if m & bit})
+        return {"sm_mhz": statistics.median(r[1] for r in inside), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(inside), "window": window, "source": "NVML, 2 ms polling"}
 
 
 def _setup(torch, dev):
@@ -189,14 +208,16 @@ def run_b200(args, torch):
         for _ in range(W):
             step._g.replay()
         if name == "f16":
-            clocks = ClockSampler(local)
+            clocks = ClockSampler(torch, dev)
             clocks.start()
             if ws > 1:
                 dist.barrier()
             torch.cuda.synchronize()
+            clocks.mark(True)
         st, km = _time_steps(torch, step._g.replay, K, flush, timer, "tc_sncc_moments")
         torch.cuda.synchronize()
         if name == "f16":
+            clocks.mark(False)
             if ws > 1:
                 dist.barrier()
             res["clocks"] = clocks.stop()
@@ -415,8 +436,8 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

@@ -1,0 +1,766 @@
+// PoU-FVR cone-beam kernels (src/fvr/cone_beam_fvr.py, src/fvr/triton_slice.py:341-591), sm_100a.
+//
+// Precompute: partition-of-unity block extraction (window product, centring
+// in an M^3 cube, trilinear resize to block_res^3, sinc^2 pre-compensation,
+// zero pad to P^3) straight from the volume on the device; the block spectra
+// then come from the batched 3D FFT and are stored in the stencil layout.
+//
+// Per step, for N poses and B blocks:
+//   pose kernel     rigid matrices -> source / detector axes (fp64), slice
+//                   axes and per-(block, pose) offsets d_b, cu, cv (fp64)
+//   slice kernel    every block sliced along the pose's detector plane, written
+//                   in ifftshift order -> batched 2D IFFT -> real block images
+//   warp kernel     per detector pixel, sum over blocks of the bilinear sample
+//                   of each block image at its magnified position, x 1/cos
+// and the adjoint chain warp -> IFFT -> slice -> pose.
+#include "fvr_pose.cuh"
+#include "fvr_stencil.cuh"
+
+namespace fvr {
+
+// ----------------------------------------------------------------------------
+// block extraction  (cone_beam_fvr.py:208-290)
+// ----------------------------------------------------------------------------
+
+struct PouAxisTables {
+  const float* w;    // windows [k][n] (float32, as the reference builds them)
+  const int* sup;    // supports [k][2]: first index, length
+  int k, n;
+};
+
+// sum over the support of vol * w0 * w1 * w2 for candidate block kb (fp64)
+__global__ void __launch_bounds__(256) pou_block_sums_kernel(const float* __restrict__ vol, PouAxisTables a0,
+                                                             PouAxisTables a1, PouAxisTables a2,
+                                                             double* __restrict__ sums) {
+  __shared__ double red[8];
+  const int kb = blockIdx.x;
+  const int i0 = kb / (a1.k * a2.k), i1 = (kb / a2.k) % a1.k, i2 = kb % a2.k;
+  const int s0 = a0.sup[2 * i0], l0 = a0.sup[2 * i0 + 1];
+  const int s1 = a1.sup[2 * i1], l1 = a1.sup[2 * i1 + 1];
+  const int s2 = a2.sup[2 * i2], l2 = a2.sup[2 * i2 + 1];
+  const int64_t tot = static_cast<int64_t>(l0) * l1 * l2;
+  double acc = 0.0;
+  for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+    const int z = static_cast<int>(e / (static_cast<int64_t>(l1) * l2));
+    const int y = static_cast<int>((e / l2) % l1), x = static_cast<int>(e % l2);
+    const int gz = s0 + z, gy = s1 + y, gx = s2 + x;
+    const float wv = a0.w[i0 * a0.n + gz] * a1.w[i1 * a1.n + gy] * a2.w[i2 * a2.n + gx];
+    acc += static_cast<double>(vol[(static_cast<int64_t>(gz) * a1.n + gy) * a2.n + gx] * wv);
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) s += red[w];
+    sums[kb] = s;
+  }
+}
+
+struct PouBuildArgs {
+  const float* vol;
+  PouAxisTables ax[3];
+  const int* blocks;  // [B] candidate block index kb of each active block
+  const float* w3;    // [block_res] sinc^2 pre-compensation (cone_beam_fvr.py:64-68)
+  int M, br, P, pad_b;
+  float ds;           // ds_block (resize intensity factor)
+  float* out;         // [B][P][P][P]
+};
+
+// windowed sub-volume value at M-cube index (z, y, x) of block kb
+__device__ __forceinline__ float pou_cube(const PouBuildArgs& a, const int (&ib)[3], const int (&s)[3],
+                                          const int (&l)[3], const int (&m)[3], int z, int y, int x) {
+  const int c[3] = {z - m[0], y - m[1], x - m[2]};
+  if (c[0] < 0 || c[0] >= l[0] || c[1] < 0 || c[1] >= l[1] || c[2] < 0 || c[2] >= l[2]) return 0.f;
+  const int g0 = s[0] + c[0], g1 = s[1] + c[1], g2 = s[2] + c[2];
+  const float wv = a.ax[0].w[ib[0] * a.ax[0].n + g0] * a.ax[1].w[ib[1] * a.ax[1].n + g1] *
+                   a.ax[2].w[ib[2] * a.ax[2].n + g2];
+  return a.vol[(static_cast<int64_t>(g0) * a.ax[1].n + g1) * a.ax[2].n + g2] * wv;
+}
+
+// F.interpolate(..., mode='trilinear', align_corners=False) source index along one axis
+__device__ __forceinline__ void resize_src(int dst, int in, int out, int& i0, int& i1, float& lam) {
+  const float scale = static_cast<float>(in) / static_cast<float>(out);
+  float src = scale * (static_cast<float>(dst) + 0.5f) - 0.5f;
+  if (src < 0.f) src = 0.f;
+  i0 = static_cast<int>(src);
+  i1 = i0 < in - 1 ? i0 + 1 : i0;
+  lam = src - static_cast<float>(i0);
+}
+
+__global__ void __launch_bounds__(256) pou_block_build_kernel(PouBuildArgs a, int64_t total) {
+  const int64_t P3 = static_cast<int64_t>(a.P) * a.P * a.P;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int b = static_cast<int>(e / P3);
+    const int64_t r = e - b * P3;
+    const int z = static_cast<int>(r / (static_cast<int64_t>(a.P) * a.P)) - a.pad_b;
+    const int y = static_cast<int>((r / a.P) % a.P) - a.pad_b;
+    const int x = static_cast<int>(r % a.P) - a.pad_b;
+    float val = 0.f;
+    if (z >= 0 && z < a.br && y >= 0 && y < a.br && x >= 0 && x < a.br) {
+      const int kb = a.blocks[b];
+      const int ib[3] = {kb / (a.ax[1].k * a.ax[2].k), (kb / a.ax[2].k) % a.ax[1].k, kb % a.ax[2].k};
+      int s[3], l[3], m[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        s[d] = a.ax[d].sup[2 * ib[d]];
+        l[d] = a.ax[d].sup[2 * ib[d] + 1];
+        m[d] = (a.M - l[d]) / 2;
+      }
+      float cube;
+      if (a.M == a.br) {
+        cube = pou_cube(a, ib, s, l, m, z, y, x);
+      } else {
+        int z0, z1, y0, y1, x0, x1;
+        float lz, ly, lx;
+        resize_src(z, a.M, a.br, z0, z1, lz);
+        resize_src(y, a.M, a.br, y0, y1, ly);
+        resize_src(x, a.M, a.br, x0, x1, lx);
+        const float c000 = pou_cube(a, ib, s, l, m, z0, y0, x0), c001 = pou_cube(a, ib, s, l, m, z0, y0, x1);
+        const float c010 = pou_cube(a, ib, s, l, m, z0, y1, x0), c011 = pou_cube(a, ib, s, l, m, z0, y1, x1);
+        const float c100 = pou_cube(a, ib, s, l, m, z1, y0, x0), c101 = pou_cube(a, ib, s, l, m, z1, y0, x1);
+        const float c110 = pou_cube(a, ib, s, l, m, z1, y1, x0), c111 = pou_cube(a, ib, s, l, m, z1, y1, x1);
+        const float mz = 1.f - lz, my = 1.f - ly, mx = 1.f - lx;
+        cube = mz * (my * (mx * c000 + lx * c001) + ly * (mx * c010 + lx * c011)) +
+               lz * (my * (mx * c100 + lx * c101) + ly * (mx * c110 + lx * c111));
+      }
+      val = cube * a.ds * (a.w3[z] * a.w3[y] * a.w3[x]);
+    }
+    a.out[e] = val;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// pose geometry  (cone_beam_fvr.py:485-488, 507-521, 670-682)
+// ----------------------------------------------------------------------------
+
+constexpr int kGeo = 18;  // per pose: src[3], u[3], v[3], n[3], u_xyz[3], v_xyz[3]
+
+struct PouBase {
+  double src0[3], u0[3], v0[3], n0[3];
+};
+
+__global__ void pou_pose_kernel(const float* __restrict__ mats, const float* __restrict__ vecs, int N, PouBase base,
+                                double vscale, const float* __restrict__ centers, int B, double* __restrict__ geo,
+                                double* __restrict__ offs) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double g[kGeo];
+  if (mats) {
+    const float* M = mats + 16 * n;
+    double R[3][3], t[3];
+    for (int i = 0; i < 3; ++i) {
+      for (int j = 0; j < 3; ++j) R[i][j] = M[4 * i + j];
+      t[i] = M[4 * i + 3];
+    }
+    for (int i = 0; i < 3; ++i) {
+      g[i] = R[i][0] * base.src0[0] + R[i][1] * base.src0[1] + R[i][2] * base.src0[2] + t[i];
+      g[3 + i] = R[i][0] * base.u0[0] + R[i][1] * base.u0[1] + R[i][2] * base.u0[2];
+      g[6 + i] = R[i][0] * base.v0[0] + R[i][1] * base.v0[1] + R[i][2] * base.v0[2];
+      g[9 + i] = R[i][0] * base.n0[0] + R[i][1] * base.n0[1] + R[i][2] * base.n0[2];
+    }
+  } else {  // explicit source / detector axes [N][12] = (s, u, v, n)
+    for (int k = 0; k < 12; ++k) g[k] = vecs[12 * n + k];
+  }
+  // slice axes in (x, y, z) voxel order = world (axis2, axis1, axis0), scaled by P * ds
+  for (int i = 0; i < 3; ++i) {
+    g[12 + i] = g[3 + 2 - i] * vscale;
+    g[15 + i] = g[6 + 2 - i] * vscale;
+  }
+  for (int k = 0; k < kGeo; ++k) geo[n * kGeo + k] = g[k];
+  for (int b = 0; b < B; ++b) {
+    const double d0 = centers[3 * b] - g[0], d1 = centers[3 * b + 1] - g[1], d2 = centers[3 * b + 2] - g[2];
+    double* o = offs + 3 * (static_cast<int64_t>(b) * N + n);
+    o[0] = d0 * g[9] + d1 * g[10] + d2 * g[11];  // d_b  = (c_b - s) . n0
+    o[1] = d0 * g[3] + d1 * g[4] + d2 * g[5];    // cu   = (c_b - s) . u
+    o[2] = d0 * g[6] + d1 * g[7] + d2 * g[8];    // cv   = (c_b - s) . v
+  }
+}
+
+// Explicit rays (cone_beam_fvr.py:451-457): per pose and pixel
+// rx = (r.u)/cos, ry = (r.v)/cos, ic = 1/cos with r the unit ray, cos = max(r.n, 0.1).
+__global__ void pou_rays_prep_kernel(const float* __restrict__ trg, const double* __restrict__ geo, int N, int K,
+                                     float* __restrict__ rx, float* __restrict__ ry, float* __restrict__ ic) {
+  const int n = blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= K) return;
+  const double* g = geo + n * kGeo;
+  const float* t = trg + (static_cast<int64_t>(n) * K + q) * 3;
+  const double r0 = t[0] - g[0], r1 = t[1] - g[1], r2 = t[2] - g[2];
+  const double inv = 1.0 / sqrt(fmax(r0 * r0 + r1 * r1 + r2 * r2, 1e-12));
+  const double h0 = r0 * inv, h1 = r1 * inv, h2 = r2 * inv;
+  const double c = fmax(h0 * g[9] + h1 * g[10] + h2 * g[11], 0.1);
+  const double icv = 1.0 / c;
+  const int64_t o = static_cast<int64_t>(n) * K + q;
+  rx[o] = static_cast<float>((h0 * g[3] + h1 * g[4] + h2 * g[5]) * icv);
+  ry[o] = static_cast<float>((h0 * g[6] + h1 * g[7] + h2 * g[8]) * icv);
+  ic[o] = static_cast<float>(icv);
+}
+
+// ----------------------------------------------------------------------------
+// block slices  (cone_beam_fvr.py:480-505; triton_slice.py:46-143)
+// ----------------------------------------------------------------------------
+
+struct PouSliceArgs {
+  Stencil st;            // block 0; block b at data + b*item_bytes, scales + b*item_scales
+  int64_t item_bytes, item_scales;
+  const double* geo;     // [N][18]
+  const float* freqs;    // [P] fftshift(fftfreq(P, d=ds))
+  int P, N;
+  double c;              // P // 2
+};
+
+__device__ __forceinline__ Stencil pou_block_stencil(const PouSliceArgs& a, int b) {
+  Stencil s = a.st;
+  s.data = static_cast<const char*>(a.st.data) + b * a.item_bytes;
+  if (a.st.scales) s.scales = a.st.scales + b * a.item_scales;
+  return s;
+}
+
+template <int DT>
+__global__ void __launch_bounds__(256) pou_slice_kernel(PouSliceArgs a, float2* __restrict__ out) {
+  const int n = blockIdx.y, b = blockIdx.z, P = a.P;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= P * P) return;
+  const int i = q / P, j = q - (q / P) * P;  // i: fy index (rows), j: fx index
+  const double* g = a.geo + n * kGeo;
+  const double fx = __ldg(a.freqs + j), fy = __ldg(a.freqs + i);
+  const Stencil st = pou_block_stencil(a, b);
+  Interp o;
+  stencil_sample_d<DT, false, false>(st, fma(fy, g[15], fma(fx, g[12], a.c)), fma(fy, g[16], fma(fx, g[13], a.c)),
+                                     fma(fy, g[17], fma(fx, g[14], a.c)), o);
+  // ifftshift position for the IFFT input
+  const int h = P / 2;
+  int ii = i - h, jj = j - h;
+  if (ii < 0) ii += P;
+  if (jj < 0) jj += P;
+  out[(static_cast<int64_t>(b) * a.N + n) * P * P + ii * P + jj] = make_float2(o.sr, o.si);
+}
+
+// Slice adjoint: G[b][n][P*P] (natural order) -> partial[n][b][tile][6] = sums
+// of (fx, fy) x <G, dS/dp_k> over the tile.
+template <int DT>
+__global__ void __launch_bounds__(256) pou_slice_adjoint_kernel(PouSliceArgs a, const float2* __restrict__ G,
+                                                                double* __restrict__ partial) {
+  __shared__ double red[6 * 8];
+  const int n = blockIdx.y, b = blockIdx.z, P = a.P;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (q < P * P) {
+    const int i = q / P, j = q - (q / P) * P;
+    const double* g = a.geo + n * kGeo;
+    const float fxf = __ldg(a.freqs + j), fyf = __ldg(a.freqs + i);
+    const double fx = fxf, fy = fyf;
+    const Stencil st = pou_block_stencil(a, b);
+    Interp o;
+    stencil_sample_d<DT, true, false>(st, fma(fy, g[15], fma(fx, g[12], a.c)), fma(fy, g[16], fma(fx, g[13], a.c)),
+                                      fma(fy, g[17], fma(fx, g[14], a.c)), o);
+    const float2 gg = __ldg(G + (static_cast<int64_t>(b) * a.N + n) * P * P + q);
+    const float e0 = gg.x * o.dxr + gg.y * o.dxi, e1 = gg.x * o.dyr + gg.y * o.dyi, e2 = gg.x * o.dzr + gg.y * o.dzi;
+    acc[0] = fxf * e0;
+    acc[1] = fxf * e1;
+    acc[2] = fxf * e2;
+    acc[3] = fyf * e0;
+    acc[4] = fyf * e1;
+    acc[5] = fyf * e2;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const double v = warp_sum(static_cast<double>(acc[m]));
+    if (lane == 0) red[m * nw + wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += red[threadIdx.x * nw + w];
+    partial[((static_cast<int64_t>(n) * gridDim.z + b) * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = s;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// pinhole warp + sum  (triton_slice.py:348-407 / 409-496)
+// ----------------------------------------------------------------------------
+
+template <typename OT>
+struct WarpArgs {
+  const float* imgs;  // [B][N][P][P]
+  const OT* db;       // d_b[b][n] at db[(b*N + n) * ostride]
+  const OT* cu;
+  const OT* cv;
+  int ostride;
+  const float *rx, *ry, *ic;  // [K], or [N][K] with ray_stride = K
+  double inv_ds, c_idx;
+  int B, N, P, K;
+  int64_t ray_stride;
+};
+
+template <typename OT>
+__global__ void __launch_bounds__(256) pou_warp_kernel(WarpArgs<OT> a, float* __restrict__ out) {
+  const int n = blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.K) return;
+  const int64_t rq = n * a.ray_stride + q;
+  const double rx = __ldg(a.rx + rq), ry = __ldg(a.ry + rq);
+  const int P = a.P;
+  float acc = 0.f;
+  for (int b = 0; b < a.B; ++b) {
+    const int64_t bn = static_cast<int64_t>(b) * a.N + n;
+    const double db = static_cast<double>(a.db[bn * a.ostride]);
+    const double px = (db * rx - static_cast<double>(a.cu[bn * a.ostride])) * a.inv_ds + a.c_idx;
+    const double py = (db * ry - static_cast<double>(a.cv[bn * a.ostride])) * a.inv_ds + a.c_idx;
+    if (!(px > -1.0 && px < static_cast<double>(P) && py > -1.0 && py < static_cast<double>(P))) continue;
+    const double fx = floor(px), fy = floor(py);
+    const int ix = static_cast<int>(fx), iy = static_cast<int>(fy);
+    const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
+    const float* img = a.imgs + bn * P * P;
+    const bool x0 = ix >= 0, x1 = ix + 1 < P, y0 = iy >= 0, y1 = iy + 1 < P;
+    const float v00 = (x0 && y0) ? __ldg(img + iy * P + ix) : 0.f;
+    const float v01 = (x1 && y0) ? __ldg(img + iy * P + ix + 1) : 0.f;
+    const float v10 = (x0 && y1) ? __ldg(img + (iy + 1) * P + ix) : 0.f;
+    const float v11 = (x1 && y1) ? __ldg(img + (iy + 1) * P + ix + 1) : 0.f;
+    acc += (v00 * (1.f - tx) + v01 * tx) * (1.f - ty) + (v10 * (1.f - tx) + v11 * tx) * ty;
+  }
+  out[static_cast<int64_t>(n) * a.K + q] = acc * __ldg(a.ic + rq);
+}
+
+// Adjoint: grad_imgs (scatter, red.global.add) and per-(b, n) partial sums of
+// dL/d(d_b, cu, cv) reduced warp -> CTA (fp64 in shared memory) ->
+// partial[n][tile][b][3].
+template <typename OT>
+__global__ void __launch_bounds__(256) pou_warp_bwd_kernel(WarpArgs<OT> a, const float* __restrict__ gout,
+                                                           float* __restrict__ grad_imgs,
+                                                           double* __restrict__ partial,
+                                                           float* __restrict__ gray) {
+  extern __shared__ double sacc[];  // [B][3]
+  const int n = blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int i = threadIdx.x; i < 3 * a.B; i += blockDim.x) sacc[i] = 0.0;
+  __syncthreads();
+  const bool live = q < a.K;
+  const int64_t rq = n * a.ray_stride + q;
+  const double rx = live ? __ldg(a.rx + rq) : 0.0, ry = live ? __ldg(a.ry + rq) : 0.0;
+  const float g = live ? __ldg(gout + static_cast<int64_t>(n) * a.K + q) * __ldg(a.ic + rq) : 0.f;
+  const int P = a.P;
+  const float inv_ds = static_cast<float>(a.inv_ds);
+  float grx = 0.f, gry = 0.f, ssum = 0.f;  // explicit rays: dL/drx, dL/dry, sum_b sample
+  for (int b = 0; b < a.B; ++b) {
+    const int64_t bn = static_cast<int64_t>(b) * a.N + n;
+    float gdb = 0.f, gcu = 0.f, gcv = 0.f;
+    if (live) {
+      const double db = static_cast<double>(a.db[bn * a.ostride]);
+      const double px = (db * rx - static_cast<double>(a.cu[bn * a.ostride])) * a.inv_ds + a.c_idx;
+      const double py = (db * ry - static_cast<double>(a.cv[bn * a.ostride])) * a.inv_ds + a.c_idx;
+      if (px > -1.0 && px < static_cast<double>(P) && py > -1.0 && py < static_cast<double>(P)) {
+        const double fx = floor(px), fy = floor(py);
+        const int ix = static_cast<int>(fx), iy = static_cast<int>(fy);
+        const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
+        const float* img = a.imgs + bn * P * P;
+        const bool x0 = ix >= 0, x1 = ix + 1 < P, y0 = iy >= 0, y1 = iy + 1 < P;
+        const float v00 = (x0 && y0) ? __ldg(img + iy * P + ix) : 0.f;
+        const float v01 = (x1 && y0) ? __ldg(img + iy * P + ix + 1) : 0.f;
+        const float v10 = (x0 && y1) ? __ldg(img + (iy + 1) * P + ix) : 0.f;
+        const float v11 = (x1 && y1) ? __ldg(img + (iy + 1) * P + ix + 1) : 0.f;
+        if (grad_imgs) {
+          float* gi = grad_imgs + bn * P * P;
+          if (x0 && y0) atomicAdd(gi + iy * P + ix, g * (1.f - tx) * (1.f - ty));
+          if (x1 && y0) atomicAdd(gi + iy * P + ix + 1, g * tx * (1.f - ty));
+          if (x0 && y1) atomicAdd(gi + (iy + 1) * P + ix, g * (1.f - tx) * ty);
+          if (x1 && y1) atomicAdd(gi + (iy + 1) * P + ix + 1, g * tx * ty);
+        }
+        const float dpx = ((v01 - v00) * (1.f - ty) + (v11 - v10) * ty) * inv_ds;
+        const float dpy = ((v10 - v00) * (1.f - tx) + (v11 - v01) * tx) * inv_ds;
+        gdb = g * (dpx * static_cast<float>(rx) + dpy * static_cast<float>(ry));
+        gcu = -g * dpx;
+        gcv = -g * dpy;
+        if (gray) {
+          const float dbf = static_cast<float>(db);
+          grx += g * dpx * dbf;
+          gry += g * dpy * dbf;
+          ssum += (v00 * (1.f - tx) + v01 * tx) * (1.f - ty) + (v10 * (1.f - tx) + v11 * tx) * ty;
+        }
+      }
+    }
+    const double s0 = warp_sum(static_cast<double>(gdb)), s1 = warp_sum(static_cast<double>(gcu)),
+                 s2 = warp_sum(static_cast<double>(gcv));
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(sacc + 3 * b, s0);
+      atomicAdd(sacc + 3 * b + 1, s1);
+      atomicAdd(sacc + 3 * b + 2, s2);
+    }
+  }
+  if (gray && live) {
+    float* o = gray + (static_cast<int64_t>(n) * a.K + q) * 3;
+    o[0] = grx;
+    o[1] = gry;
+    o[2] = __ldg(gout + static_cast<int64_t>(n) * a.K + q) * ssum;  // direct dL/dic
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * a.B; i += blockDim.x)
+    partial[(static_cast<int64_t>(n) * gridDim.x + blockIdx.x) * 3 * a.B + i] = sacc[i];
+}
+
+// Explicit-ray adjoint per pixel: from dL/d(rx, ry, ic) (gray) to dL/dtrg
+// (written) and per-(pose, tile) partials of dL/d(src, u, v, n) [12].
+__global__ void __launch_bounds__(256) pou_rays_bwd_kernel(const float* __restrict__ trg,
+                                                           const double* __restrict__ geo, int N, int K,
+                                                           const float* __restrict__ gray, float* __restrict__ gtrg,
+                                                           double* __restrict__ partial) {
+  __shared__ double red[12 * 8];
+  const int n = blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (q < K) {
+    const double* g = geo + n * kGeo;
+    const float* t = trg + (static_cast<int64_t>(n) * K + q) * 3;
+    const double r[3] = {t[0] - g[0], t[1] - g[1], t[2] - g[2]};
+    const double len2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    const double inv = 1.0 / sqrt(fmax(len2, 1e-12));
+    const double h[3] = {r[0] * inv, r[1] * inv, r[2] * inv};
+    const double cr = h[0] * g[9] + h[1] * g[10] + h[2] * g[11];
+    const double c = fmax(cr, 0.1), icv = 1.0 / c;
+    const double ru = h[0] * g[3] + h[1] * g[4] + h[2] * g[5], rv = h[0] * g[6] + h[1] * g[7] + h[2] * g[8];
+    const float* gr = gray + (static_cast<int64_t>(n) * K + q) * 3;
+    const double grx = gr[0], gry = gr[1];
+    const double gic = gr[2] + grx * ru + gry * rv;  // rx = ru * ic, ry = rv * ic
+    const double gru = grx * icv, grv = gry * icv;
+    const double gcos = cr > 0.1 ? -gic * icv * icv : 0.0;
+    double gh[3];
+    for (int k = 0; k < 3; ++k) {
+      gh[k] = gru * g[3 + k] + grv * g[6 + k] + gcos * g[9 + k];
+      acc[3 + k] = gru * h[k];   // dL/du
+      acc[6 + k] = grv * h[k];   // dL/dv
+      acc[9 + k] = gcos * h[k];  // dL/dn
+    }
+    const double gdot = gh[0] * h[0] + gh[1] * h[1] + gh[2] * h[2];
+    float* o = gtrg + (static_cast<int64_t>(n) * K + q) * 3;
+    for (int k = 0; k < 3; ++k) {
+      const double gray_k = len2 > 1e-12 ? (gh[k] - gdot * h[k]) * inv : gh[k] * inv;
+      o[k] = static_cast<float>(gray_k);
+      acc[k] = -gray_k;  // dL/dsrc
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int m = 0; m < 12; ++m) {
+    const double v = warp_sum(acc[m]);
+    if (lane == 0) red[m * nw + wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 12) {
+    double s2 = 0.0;
+    for (int w = 0; w < nw; ++w) s2 += red[threadIdx.x * nw + w];
+    partial[(static_cast<int64_t>(n) * gridDim.x + blockIdx.x) * 12 + threadIdx.x] = s2;
+  }
+}
+
+// partial[n][tiles][B][3] -> goffs[3][B][N] (fp64, fixed order)
+__global__ void pou_warp_bwd_finalize_kernel(const double* __restrict__ partial, int N, int B, int tiles,
+                                             double* __restrict__ goffs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N * B * 3) return;
+  const int n = i / (3 * B), r = i - n * 3 * B;  // r = b*3 + m
+  double s = 0.0;
+  for (int t = 0; t < tiles; ++t) s += partial[(static_cast<int64_t>(n) * tiles + t) * 3 * B + r];
+  const int b = r / 3, m = r - 3 * (r / 3);
+  goffs[(static_cast<int64_t>(m) * B + b) * N + n] = s;
+}
+
+// pose adjoint: slice-axis partials [N][B][tiles][6], offset gradients
+// goffs[3][B][N] and (explicit rays) per-(pose, tile) partials [N][rtiles][12]
+// -> dL/d(src, u, v, n) [N][12] (gvec) and / or dL/dmats [N][4][4]
+// (cone_beam_fvr.py:485-521, 676-682)
+__global__ void pou_pose_bwd_kernel(const double* __restrict__ sl_part, int tiles, const double* __restrict__ goffs,
+                                    const double* __restrict__ ray_part, int rtiles, const double* __restrict__ geo,
+                                    const float* __restrict__ centers, int B, int N, PouBase base, double vscale,
+                                    float* __restrict__ gmats, float* __restrict__ gvec) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double gux[3] = {0, 0, 0}, gvx[3] = {0, 0, 0};
+  for (int b = 0; b < B; ++b)
+    for (int t = 0; t < tiles; ++t) {
+      const double* p = sl_part + ((static_cast<int64_t>(n) * B + b) * tiles + t) * 6;
+      for (int k = 0; k < 3; ++k) {
+        gux[k] += p[k];
+        gvx[k] += p[3 + k];
+      }
+    }
+  const double* g = geo + n * kGeo;
+  const double s[3] = {g[0], g[1], g[2]}, u[3] = {g[3], g[4], g[5]}, v[3] = {g[6], g[7], g[8]},
+               nn[3] = {g[9], g[10], g[11]};
+  // u_xyz = flip(u) * vscale
+  double gu[3], gv[3], gn[3] = {0, 0, 0}, gs[3] = {0, 0, 0};
+  for (int k = 0; k < 3; ++k) {
+    gu[k] = gux[2 - k] * vscale;
+    gv[k] = gvx[2 - k] * vscale;
+  }
+  if (goffs) {
+    for (int b = 0; b < B; ++b) {
+      const double gdb = goffs[(0 * static_cast<int64_t>(B) + b) * N + n];
+      const double gcu = goffs[(1 * static_cast<int64_t>(B) + b) * N + n];
+      const double gcv = goffs[(2 * static_cast<int64_t>(B) + b) * N + n];
+      for (int k = 0; k < 3; ++k) {
+        const double d = static_cast<double>(centers[3 * b + k]) - s[k];
+        gn[k] += gdb * d;
+        gu[k] += gcu * d;
+        gv[k] += gcv * d;
+        gs[k] -= gdb * nn[k] + gcu * u[k] + gcv * v[k];
+      }
+    }
+  }
+  if (ray_part) {
+    for (int t = 0; t < rtiles; ++t) {
+      const double* p = ray_part + (static_cast<int64_t>(n) * rtiles + t) * 12;
+      for (int k = 0; k < 3; ++k) {
+        gs[k] += p[k];
+        gu[k] += p[3 + k];
+        gv[k] += p[6 + k];
+        gn[k] += p[9 + k];
+      }
+    }
+  }
+  if (gvec) {
+    float* o = gvec + 12 * n;
+    for (int k = 0; k < 3; ++k) {
+      o[k] = static_cast<float>(gs[k]);
+      o[3 + k] = static_cast<float>(gu[k]);
+      o[6 + k] = static_cast<float>(gv[k]);
+      o[9 + k] = static_cast<float>(gn[k]);
+    }
+  }
+  if (gmats) {
+    float* o = gmats + 16 * n;
+    for (int i = 0; i < 3; ++i) {
+      for (int j = 0; j < 3; ++j)
+        o[4 * i + j] = static_cast<float>(gs[i] * base.src0[j] + gu[i] * base.u0[j] + gv[i] * base.v0[j] +
+                                          gn[i] * base.n0[j]);
+      o[4 * i + 3] = static_cast<float>(gs[i]);
+    }
+    for (int j = 0; j < 4; ++j) o[12 + j] = 0.f;
+  }
+}
+
+static int pou_stencil(int dtype, const void* data, const float* scales, int64_t P, Stencil* s) {
+  if (!data || P < 2 || P > 4096) return FVR_ERR_ARG;
+  if (dtype != FVR_F32 && dtype != FVR_BF16 && dtype != FVR_F16) return FVR_ERR_DTYPE;
+  if (dtype == FVR_F16 && !scales) return FVR_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(data) & 15) != 0) return FVR_ERR_ARG;
+  *s = Stencil{data, scales, static_cast<int>(P), static_cast<int>(P), static_cast<int>(P), dtype};
+  return FVR_OK;
+}
+
+static PouBase make_base(const double* base12) {
+  PouBase b;
+  for (int k = 0; k < 3; ++k) {
+    b.src0[k] = base12[k];
+    b.u0[k] = base12[3 + k];
+    b.v0[k] = base12[6 + k];
+    b.n0[k] = base12[9 + k];
+  }
+  return b;
+}
+
+}  // namespace fvr
+
+using namespace fvr;
+
+extern "C" {
+
+int fvr_pou_block_sums(const float* vol, int64_t n0, int64_t n1, int64_t n2, const float* w0, const int* sup0,
+                       int64_t k0, const float* w1, const int* sup1, int64_t k1, const float* w2, const int* sup2,
+                       int64_t k2, double* sums, void* stream) {
+  if (!vol || !w0 || !w1 || !w2 || !sup0 || !sup1 || !sup2 || !sums) return FVR_ERR_ARG;
+  if (k0 < 1 || k1 < 1 || k2 < 1 || n0 < 1 || n1 < 1 || n2 < 1 || k0 * k1 * k2 > 65535) return FVR_ERR_ARG;
+  PouAxisTables a0{w0, sup0, (int)k0, (int)n0}, a1{w1, sup1, (int)k1, (int)n1}, a2{w2, sup2, (int)k2, (int)n2};
+  pou_block_sums_kernel<<<static_cast<unsigned>(k0 * k1 * k2), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      vol, a0, a1, a2, sums);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int fvr_pou_build_blocks(const float* vol, int64_t n0, int64_t n1, int64_t n2, const float* w0, const int* sup0,
+                         int64_t k0, const float* w1, const int* sup1, int64_t k1, const float* w2, const int* sup2,
+                         int64_t k2, const int* blocks, int64_t B, const float* w3, int64_t M, int64_t block_res,
+                         int64_t P, double ds_block, float* out, void* stream) {
+  if (!vol || !blocks || !w3 || !out || B < 1 || M < 1 || block_res < 1 || P < block_res) return FVR_ERR_ARG;
+  PouBuildArgs a;
+  a.vol = vol;
+  a.ax[0] = PouAxisTables{w0, sup0, (int)k0, (int)n0};
+  a.ax[1] = PouAxisTables{w1, sup1, (int)k1, (int)n1};
+  a.ax[2] = PouAxisTables{w2, sup2, (int)k2, (int)n2};
+  a.blocks = blocks;
+  a.w3 = w3;
+  a.M = (int)M;
+  a.br = (int)block_res;
+  a.P = (int)P;
+  a.pad_b = (int)((P - block_res) / 2);
+  a.ds = static_cast<float>(ds_block);
+  a.out = out;
+  const int64_t total = B * P * P * P;
+  const int64_t nblk = cdiv64(total, 256);
+  pou_block_build_kernel<<<static_cast<unsigned>(nblk < 148 * 64 ? nblk : 148 * 64), 256, 0,
+                           static_cast<cudaStream_t>(stream)>>>(a, total);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int64_t fvr_pou_geo_stride(void) { return kGeo; }
+
+int fvr_pou_pose(const float* mats, const float* vecs, int64_t N, const double* base12, double vscale,
+                 const float* centers, int64_t B, double* geo, double* offs, void* stream) {
+  if ((!mats && !vecs) || (mats && !base12) || !centers || !geo || !offs || N < 1 || B < 1) return FVR_ERR_ARG;
+  const double zero12[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  pou_pose_kernel<<<static_cast<unsigned>(cdiv64(N, 64)), 64, 0, static_cast<cudaStream_t>(stream)>>>(
+      mats, vecs, (int)N, make_base(mats ? base12 : zero12), vscale, centers, (int)B, geo, offs);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int fvr_pou_slice(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P, const double* geo,
+                  int64_t N, const float* freqs, void* out, void* stream) {
+  Stencil st;
+  int rc = pou_stencil(dtype, stencil, scales, P, &st);
+  if (rc) return rc;
+  if (!geo || !freqs || !out || B < 1 || N < 1 || B > 65535 || N > 65535) return FVR_ERR_ARG;
+  PouSliceArgs a{st, fvr_stencil_bytes(P, P, P, dtype), fvr_stencil_scale_count(P, P, P), geo, freqs, (int)P, (int)N,
+                 static_cast<double>(P / 2)};
+  dim3 grid(static_cast<unsigned>(cdiv64(P * P, 256)), static_cast<unsigned>(N), static_cast<unsigned>(B));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  float2* o = static_cast<float2*>(out);
+  switch (dtype) {
+    case FVR_F32: pou_slice_kernel<FVR_F32><<<grid, 256, 0, s>>>(a, o); break;
+    case FVR_BF16: pou_slice_kernel<FVR_BF16><<<grid, 256, 0, s>>>(a, o); break;
+    case FVR_F16: pou_slice_kernel<FVR_F16><<<grid, 256, 0, s>>>(a, o); break;
+  }
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int64_t fvr_pou_slice_adjoint_workspace(int64_t B, int64_t P, int64_t N) {
+  return N * B * cdiv64(P * P, 256) * 6 * (int64_t)sizeof(double);
+}
+
+int fvr_pou_slice_adjoint(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
+                          const double* geo, int64_t N, const float* freqs, const void* G, void* workspace,
+                          int64_t ws_bytes, void* stream) {
+  Stencil st;
+  int rc = pou_stencil(dtype, stencil, scales, P, &st);
+  if (rc) return rc;
+  if (!geo || !freqs || !G || !workspace || B < 1 || N < 1 || B > 65535 || N > 65535) return FVR_ERR_ARG;
+  if (ws_bytes < fvr_pou_slice_adjoint_workspace(B, P, N)) return FVR_ERR_WORKSPACE;
+  PouSliceArgs a{st, fvr_stencil_bytes(P, P, P, dtype), fvr_stencil_scale_count(P, P, P), geo, freqs, (int)P, (int)N,
+                 static_cast<double>(P / 2)};
+  dim3 grid(static_cast<unsigned>(cdiv64(P * P, 256)), static_cast<unsigned>(N), static_cast<unsigned>(B));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float2* g = static_cast<const float2*>(G);
+  double* part = static_cast<double*>(workspace);
+  switch (dtype) {
+    case FVR_F32: pou_slice_adjoint_kernel<FVR_F32><<<grid, 256, 0, s>>>(a, g, part); break;
+    case FVR_BF16: pou_slice_adjoint_kernel<FVR_BF16><<<grid, 256, 0, s>>>(a, g, part); break;
+    case FVR_F16: pou_slice_adjoint_kernel<FVR_F16><<<grid, 256, 0, s>>>(a, g, part); break;
+  }
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int fvr_pou_warp(const float* imgs, int64_t B, int64_t N, int64_t P, const void* db, const void* cu, const void* cv,
+                 int offs_f64, int64_t ostride, const float* rx, const float* ry, const float* ic, int64_t K,
+                 int64_t ray_stride, double inv_ds, double c_idx, float* out, void* stream) {
+  if (!imgs || !db || !cu || !cv || !rx || !ry || !ic || !out || B < 1 || N < 1 || P < 2 || K < 1 || N > 65535)
+    return FVR_ERR_ARG;
+  dim3 grid(static_cast<unsigned>(cdiv64(K, 256)), static_cast<unsigned>(N));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (offs_f64) {
+    WarpArgs<double> a{imgs, static_cast<const double*>(db), static_cast<const double*>(cu),
+                       static_cast<const double*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
+                       (int)P, (int)K, ray_stride};
+    pou_warp_kernel<double><<<grid, 256, 0, s>>>(a, out);
+  } else {
+    WarpArgs<float> a{imgs, static_cast<const float*>(db), static_cast<const float*>(cu),
+                      static_cast<const float*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
+                      (int)P, (int)K, ray_stride};
+    pou_warp_kernel<float><<<grid, 256, 0, s>>>(a, out);
+  }
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int64_t fvr_pou_warp_bwd_workspace(int64_t B, int64_t N, int64_t K) {
+  return N * cdiv64(K, 256) * 3 * B * (int64_t)sizeof(double);
+}
+
+int fvr_pou_warp_bwd(const float* imgs, int64_t B, int64_t N, int64_t P, const void* db, const void* cu,
+                     const void* cv, int offs_f64, int64_t ostride, const float* rx, const float* ry, const float* ic,
+                     int64_t K, int64_t ray_stride, double inv_ds, double c_idx, const float* gout, float* grad_imgs,
+                     double* goffs, float* gray, void* workspace, int64_t ws_bytes, void* stream) {
+  if (!imgs || !db || !cu || !cv || !rx || !ry || !ic || !gout || !goffs || !workspace || B < 1 || N < 1 || P < 2 ||
+      K < 1 || N > 65535 || B > 4096)
+    return FVR_ERR_ARG;
+  if (ws_bytes < fvr_pou_warp_bwd_workspace(B, N, K)) return FVR_ERR_WORKSPACE;
+  const int tiles = static_cast<int>(cdiv64(K, 256));
+  dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(N));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t sm = 3 * B * sizeof(double);
+  double* part = static_cast<double*>(workspace);
+  if (offs_f64) {
+    WarpArgs<double> a{imgs, static_cast<const double*>(db), static_cast<const double*>(cu),
+                       static_cast<const double*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
+                       (int)P, (int)K, ray_stride};
+    if (sm > 48 * 1024 &&
+        cudaFuncSetAttribute(pou_warp_bwd_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
+            cudaSuccess)
+      return FVR_ERR_CUDA;
+    pou_warp_bwd_kernel<double><<<grid, 256, sm, s>>>(a, gout, grad_imgs, part, gray);
+  } else {
+    WarpArgs<float> a{imgs, static_cast<const float*>(db), static_cast<const float*>(cu),
+                      static_cast<const float*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
+                      (int)P, (int)K, ray_stride};
+    if (sm > 48 * 1024 &&
+        cudaFuncSetAttribute(pou_warp_bwd_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
+            cudaSuccess)
+      return FVR_ERR_CUDA;
+    pou_warp_bwd_kernel<float><<<grid, 256, sm, s>>>(a, gout, grad_imgs, part, gray);
+  }
+  FVR_LAUNCH_CHECK();
+  pou_warp_bwd_finalize_kernel<<<static_cast<unsigned>(cdiv64(N * B * 3, 256)), 256, 0, s>>>(part, (int)N, (int)B,
+                                                                                             tiles, goffs);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int fvr_pou_pose_backward(const double* sl_part, int64_t tiles, const double* goffs, const double* ray_part,
+                          int64_t rtiles, const double* geo, const float* centers, int64_t B, int64_t N,
+                          const double* base12, double vscale, float* gmats, float* gvec, void* stream) {
+  if (!sl_part || !geo || !centers || (!gmats && !gvec) || (gmats && !base12) || B < 1 || N < 1 || tiles < 1)
+    return FVR_ERR_ARG;
+  const double zero12[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  pou_pose_bwd_kernel<<<static_cast<unsigned>(cdiv64(N, 64)), 64, 0, static_cast<cudaStream_t>(stream)>>>(
+      sl_part, (int)tiles, goffs, ray_part, (int)rtiles, geo, centers, (int)B, (int)N,
+      make_base(base12 ? base12 : zero12), vscale, gmats, gvec);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int fvr_pou_rays_prep(const float* trg, const double* geo, int64_t N, int64_t K, float* rx, float* ry, float* ic,
+                      void* stream) {
+  if (!trg || !geo || !rx || !ry || !ic || N < 1 || K < 1 || N > 65535) return FVR_ERR_ARG;
+  pou_rays_prep_kernel<<<dim3((unsigned)cdiv64(K, 256), (unsigned)N), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      trg, geo, (int)N, (int)K, rx, ry, ic);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int64_t fvr_pou_rays_bwd_workspace(int64_t N, int64_t K) { return N * cdiv64(K, 256) * 12 * (int64_t)sizeof(double); }
+
+int fvr_pou_rays_bwd(const float* trg, const double* geo, int64_t N, int64_t K, const float* gray, float* gtrg,
+                     void* workspace, int64_t ws_bytes, void* stream) {
+  if (!trg || !geo || !gray || !gtrg || !workspace || N < 1 || K < 1 || N > 65535) return FVR_ERR_ARG;
+  if (ws_bytes < fvr_pou_rays_bwd_workspace(N, K)) return FVR_ERR_WORKSPACE;
+  pou_rays_bwd_kernel<<<dim3((unsigned)cdiv64(K, 256), (unsigned)N), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      trg, geo, (int)N, (int)K, gray, gtrg, static_cast<double*>(workspace));
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+}  // extern "C"

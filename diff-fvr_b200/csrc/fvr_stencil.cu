@@ -33,12 +33,17 @@ __device__ __forceinline__ void entry_values(const MT* m, int64_t plane, int D, 
 }
 
 template <typename MT>
-__global__ void stencil_brick_max_kernel(const MT* __restrict__ m, int64_t plane, int D, int H, int W,
-                                         unsigned int* bmax) {
-  const int64_t n = static_cast<int64_t>(D + 1) * (H + 1) * (W + 1);
+__global__ void stencil_brick_max_kernel(const MT* __restrict__ m0, int64_t plane, int64_t items, int D, int H,
+                                         int W, unsigned int* bmax0) {
+  const int64_t n1 = static_cast<int64_t>(D + 1) * (H + 1) * (W + 1);
+  const int64_t n = n1 * items;
   const int bx = (W + 1 + kBrick - 1) / kBrick, by = (H + 1 + kBrick - 1) / kBrick;
-  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  const int64_t nb1 = static_cast<int64_t>(bx) * by * ((D + 1 + kBrick - 1) / kBrick);
+  for (int64_t ee = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; ee < n;
+       ee += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t item = ee / n1, e = ee - item * n1;
+    const MT* m = m0 + item * 2 * static_cast<int64_t>(D) * H * W;
+    unsigned int* bmax = bmax0 + item * nb1;
     const int ex = static_cast<int>(e % (W + 1));
     const int ey = static_cast<int>((e / (W + 1)) % (H + 1));
     const int ez = static_cast<int>(e / (static_cast<int64_t>(W + 1) * (H + 1)));
@@ -67,12 +72,18 @@ __global__ void stencil_scale_kernel(const unsigned int* bmax, float* scales, in
 }
 
 template <typename MT, int DT>
-__global__ void stencil_build_kernel(const MT* __restrict__ m, int64_t plane, int D, int H, int W,
-                                     void* __restrict__ out, const float* __restrict__ scales) {
-  const int64_t n = static_cast<int64_t>(D + 1) * (H + 1) * (W + 1);
+__global__ void stencil_build_kernel(const MT* __restrict__ m0, int64_t plane, int64_t items, int D, int H, int W,
+                                     void* __restrict__ out0, const float* __restrict__ scales0) {
+  const int64_t n1 = static_cast<int64_t>(D + 1) * (H + 1) * (W + 1);
+  const int64_t n = n1 * items;
   const int bx = (W + 1 + kBrick - 1) / kBrick, by = (H + 1 + kBrick - 1) / kBrick;
-  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  const int64_t nb1 = static_cast<int64_t>(bx) * by * ((D + 1 + kBrick - 1) / kBrick);
+  for (int64_t ee = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; ee < n;
+       ee += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t item = ee / n1, e = ee - item * n1;
+    const MT* m = m0 + item * 2 * static_cast<int64_t>(D) * H * W;
+    const float* scales = scales0 ? scales0 + item * nb1 : nullptr;
+    void* out = static_cast<char*>(out0) + item * n1 * (DT == FVR_F32 ? 64 : 32);
     const int ex = static_cast<int>(e % (W + 1));
     const int ey = static_cast<int>((e / (W + 1)) % (H + 1));
     const int ez = static_cast<int>(e / (static_cast<int64_t>(W + 1) * (H + 1)));
@@ -156,32 +167,34 @@ int64_t fvr_stencil_scale_count(int64_t D, int64_t H, int64_t W) {
   return fvr::cdiv64(D + 1, kBrick) * fvr::cdiv64(H + 1, kBrick) * fvr::cdiv64(W + 1, kBrick);
 }
 
-int fvr_stencil_build(const void* master, int master_dtype, int master_planar, int64_t D, int64_t H, int64_t W,
-                      int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream) {
+int fvr_stencil_build(const void* master, int master_dtype, int master_planar, int64_t items, int64_t D, int64_t H,
+                      int64_t W, int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream) {
   if (!master || !out || D < 1 || H < 1 || W < 1 || D > 8192 || H > 8192 || W > 8192) return FVR_ERR_ARG;
   if ((reinterpret_cast<uintptr_t>(out) & 15) != 0) return FVR_ERR_ARG;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int64_t n = (D + 1) * (H + 1) * (W + 1);
+  if (items < 1) return FVR_ERR_ARG;
+  const int64_t n = (D + 1) * (H + 1) * (W + 1) * items;
   const int64_t nblk = cdiv64(n, 256);
   const unsigned grid = static_cast<unsigned>(nblk < 148 * 64 ? nblk : 148 * 64);
   const int d = (int)D, h = (int)H, w = (int)W;
   const int64_t plane = master_planar ? D * H * W : 0;
   if (out_dtype == FVR_F16) {
     if (!scales || !scratch_max) return FVR_ERR_ARG;
-    const int64_t nb = fvr_stencil_scale_count(D, H, W);
+    const int64_t nb = fvr_stencil_scale_count(D, H, W) * items;
     if (cudaMemsetAsync(scratch_max, 0, nb * sizeof(unsigned int), s) != cudaSuccess) return FVR_ERR_CUDA;
     if (master_dtype == FVR_F32)
       stencil_brick_max_kernel<float>
-          <<<grid, 256, 0, s>>>(static_cast<const float*>(master), plane, d, h, w, scratch_max);
+          <<<grid, 256, 0, s>>>(static_cast<const float*>(master), plane, items, d, h, w, scratch_max);
     else if (master_dtype == FVR_BF16)
       stencil_brick_max_kernel<__nv_bfloat16>
-          <<<grid, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(master), plane, d, h, w, scratch_max);
+          <<<grid, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(master), plane, items, d, h, w, scratch_max);
     else
       return FVR_ERR_DTYPE;
     stencil_scale_kernel<<<static_cast<unsigned>(cdiv64(nb, 256)), 256, 0, s>>>(scratch_max, scales, nb);
   }
 #define FVR_BUILD(MT, DT)                                                                                  \
-  stencil_build_kernel<MT, DT><<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, d, h, w, out, scales); \
+  stencil_build_kernel<MT, DT><<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, items, d, h, w, out, \
+                                                    scales);                                                    \
   break;
   if (master_dtype == FVR_F32) {
     switch (out_dtype) {

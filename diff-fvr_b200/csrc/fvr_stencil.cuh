@@ -70,6 +70,21 @@ __device__ __forceinline__ void trilerp(const Sample8& v, float tx, float ty, fl
 
 // ---- split load / decode, so a thread can put several samples' loads in flight
 
+// One 256-bit read-only load (sm_100 ld.global.nc.v8): a whole 32-byte stencil
+// entry (16-bit storage) or half of one (f32) per instruction.  `p` must be
+// 32-byte aligned (entries are 32 or 64 bytes, the buffer base is aligned).
+__device__ __forceinline__ void ldg256(const void* p, uint4& a, uint4& b) {
+  asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+               : "l"(p));
+}
+__device__ __forceinline__ void ldg256(const float4* p, float4& a, float4& b) {
+  uint4 ua, ub;
+  ldg256(static_cast<const void*>(p), ua, ub);
+  a = make_float4(__uint_as_float(ua.x), __uint_as_float(ua.y), __uint_as_float(ua.z), __uint_as_float(ua.w));
+  b = make_float4(__uint_as_float(ub.x), __uint_as_float(ub.y), __uint_as_float(ub.z), __uint_as_float(ub.w));
+}
+
 template <int DT>
 struct Raw;
 template <>
@@ -130,8 +145,8 @@ __device__ __forceinline__ void raw_load(const Stencil& s, const Cell& c, Raw<DT
       return;
     }
     const float4* p = static_cast<const float4*>(s.data) + c.e * 4;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) r.q[i] = __ldg(p + i);
+    ldg256(p, r.q[0], r.q[1]);
+    ldg256(p + 2, r.q[2], r.q[3]);
   } else {
     if (c.e < 0) {
       r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
@@ -139,8 +154,7 @@ __device__ __forceinline__ void raw_load(const Stencil& s, const Cell& c, Raw<DT
       return;
     }
     const uint4* p = static_cast<const uint4*>(s.data) + c.e * 2;
-    r.q[0] = __ldg(p);
-    r.q[1] = __ldg(p + 1);
+    ldg256(p, r.q[0], r.q[1]);
     if constexpr (DT == FVR_F16) {
       const int bx = (s.W + 1 + kBrick - 1) / kBrick, by = (s.H + 1 + kBrick - 1) / kBrick;
       r.sc = __ldg(s.scales + (static_cast<int64_t>(c.ez / kBrick) * by + c.ey / kBrick) * bx + c.ex / kBrick);

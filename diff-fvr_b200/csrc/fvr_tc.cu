@@ -78,7 +78,18 @@ enum {
 constexpr int kMomStride = 18;  // mom[v][c][18]: 17 moments + ncc
 constexpr int kMaxViews = 4;
 constexpr int kSnccThreads = 256;
-constexpr int kSnccGroup = 4;  // samples with loads in flight per thread
+
+// Launch variants of the moments kernel (chosen per shape by the caller's
+// autotuner): samples whose loads are in flight per thread, and the resident
+// CTAs per SM the register budget is sized for.
+struct SnccVariant {
+  int group, min_blocks;
+};
+constexpr int kSnccVariants = 5;
+__host__ __device__ constexpr SnccVariant sncc_variant(int v) {
+  return v == 1 ? SnccVariant{2, 4} : v == 2 ? SnccVariant{4, 3} : v == 3 ? SnccVariant{8, 1}
+                : v == 4 ? SnccVariant{2, 3} : SnccVariant{4, 2};
+}
 
 struct SnccArgs {
   Stencil st;
@@ -111,8 +122,8 @@ __device__ __forceinline__ void block_reduce_d(T (&acc)[NV], double* red, double
   }
 }
 
-template <int DT, bool GRAD>
-__global__ void __launch_bounds__(kSnccThreads, 2) tc_sncc_moments_kernel(SnccArgs a) {
+template <int DT, bool GRAD, int GROUP, int MINB>
+__global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(SnccArgs a) {
   constexpr int NM = GRAD ? M_NGRAD : 3;
   __shared__ double red[NM * (kSnccThreads / 32)];
   __shared__ double ax_s[8];
@@ -131,14 +142,14 @@ __global__ void __launch_bounds__(kSnccThreads, 2) tc_sncc_moments_kernel(SnccAr
 #pragma unroll
   for (int m = 0; m < NM; ++m) acc[m] = 0.f;
 
-  for (int base = q_begin; base < q_end; base += kSnccThreads * kSnccGroup) {
-    Raw<DT> raw[kSnccGroup];
-    Cell cell[kSnccGroup];
-    float kus[kSnccGroup], kvs[kSnccGroup], hs[kSnccGroup];
-    float2 Ts[kSnccGroup];
+  for (int base = q_begin; base < q_end; base += kSnccThreads * GROUP) {
+    Raw<DT> raw[GROUP];
+    Cell cell[GROUP];
+    float kus[GROUP], kvs[GROUP], hs[GROUP];
+    float2 Ts[GROUP];
     // issue every load of the group before using any of them
 #pragma unroll
-    for (int g = 0; g < kSnccGroup; ++g) {
+    for (int g = 0; g < GROUP; ++g) {
       const int q = base + g * kSnccThreads + threadIdx.x;
       const bool ok = q < q_end;
       const int i = ok ? q / R : 0, j = ok ? q - i * R : 0;
@@ -156,7 +167,7 @@ __global__ void __launch_bounds__(kSnccThreads, 2) tc_sncc_moments_kernel(SnccAr
       hs[g] = ok ? (a.hp ? __ldg(a.hp + q) : 1.f) : 0.f;
     }
 #pragma unroll
-    for (int g = 0; g < kSnccGroup; ++g) {
+    for (int g = 0; g < GROUP; ++g) {
       Sample8 sm;
       raw_decode<DT>(raw[g], sm);
       Interp o;
@@ -395,22 +406,36 @@ static int stencil_from(int dtype, const void* data, const float* scales, int64_
 
 static double half_extent(int64_t n) { return 0.5 * static_cast<double>(n > 1 ? n - 1 : 1); }
 
-// Samples per CTA: fill about two resident CTAs per SM in one wave.
-static int sncc_tile(int64_t C, int64_t K, int nv) {
+// Samples per CTA: one wave of min_blocks resident CTAs per SM (never more
+// CTAs than slots), whole passes of 256 x group samples.
+static int sncc_tile(int64_t C, int64_t K, int nv, int variant) {
   static int sms = 0;
   if (sms == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
   }
+  const SnccVariant v = sncc_variant(variant);
   const int64_t items = C * nv;
-  int64_t tiles = (2LL * sms + items - 1) / items;
-  const int64_t max_tiles = cdiv64(K, kSnccThreads * kSnccGroup);
+  const int64_t pass = static_cast<int64_t>(kSnccThreads) * v.group;
+  int64_t tiles = (static_cast<int64_t>(v.min_blocks) * sms) / items;
+  const int64_t max_tiles = cdiv64(K, pass);
   if (tiles > max_tiles) tiles = max_tiles;
   if (tiles < 1) tiles = 1;
   int64_t tile = cdiv64(K, tiles);
-  tile = cdiv64(tile, kSnccThreads) * kSnccThreads;
+  tile = cdiv64(tile, pass) * pass;
   return static_cast<int>(tile);
+}
+
+template <int DT, bool GRAD>
+static void launch_sncc(int variant, dim3 grid, cudaStream_t s, const SnccArgs& a) {
+  switch (variant) {
+    case 1: tc_sncc_moments_kernel<DT, GRAD, 2, 4><<<grid, kSnccThreads, 0, s>>>(a); break;
+    case 2: tc_sncc_moments_kernel<DT, GRAD, 4, 3><<<grid, kSnccThreads, 0, s>>>(a); break;
+    case 3: tc_sncc_moments_kernel<DT, GRAD, 8, 1><<<grid, kSnccThreads, 0, s>>>(a); break;
+    case 4: tc_sncc_moments_kernel<DT, GRAD, 2, 3><<<grid, kSnccThreads, 0, s>>>(a); break;
+    default: tc_sncc_moments_kernel<DT, GRAD, 4, 2><<<grid, kSnccThreads, 0, s>>>(a); break;
+  }
 }
 
 }  // namespace fvr
@@ -434,18 +459,21 @@ int64_t fvr_tc_sncc_workspace(int64_t C, int64_t R, int64_t nviews) {
 
 int64_t fvr_tc_sncc_mom_stride(void) { return kMomStride; }
 
+int fvr_tc_sncc_variants(void) { return kSnccVariants; }
+
 int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
                         const float* poses, int64_t C, int nviews, const int* views, const void* const* ftargs,
-                        const float* hp, const float* lin, int64_t R, double kappa, int with_grad, void* workspace,
-                        int64_t ws_bytes, void* stream) {
+                        const float* hp, const float* lin, int64_t R, double kappa, int with_grad, int variant,
+                        void* workspace, int64_t ws_bytes, void* stream) {
   Stencil st;
   int rc = stencil_from(dtype, stencil, scales, D, H, W, &st);
   if (rc) return rc;
   if (!poses || !views || !ftargs || !lin || !workspace || C < 1 || R < 1 || C > 65535) return FVR_ERR_ARG;
   if (nviews < 1 || nviews > kMaxViews || R * R > (int64_t)1 << 30) return FVR_ERR_ARG;
+  if (variant < 0 || variant >= kSnccVariants) return FVR_ERR_ARG;
   if (ws_bytes < fvr_tc_sncc_workspace(C, R, nviews)) return FVR_ERR_WORKSPACE;
   const int64_t K = R * R;
-  const int tile = sncc_tile(C, K, nviews);
+  const int tile = sncc_tile(C, K, nviews, variant);
   SnccArgs a{};
   a.st = st;
   a.poses = poses;
@@ -466,11 +494,11 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
   a.partial = static_cast<double*>(workspace);
   dim3 grid(static_cast<unsigned>(cdiv64(K, tile)), static_cast<unsigned>(C), static_cast<unsigned>(nviews));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-#define FVR_SNCC(DT)                                                    \
-  if (with_grad)                                                        \
-    tc_sncc_moments_kernel<DT, true><<<grid, kSnccThreads, 0, s>>>(a);  \
-  else                                                                  \
-    tc_sncc_moments_kernel<DT, false><<<grid, kSnccThreads, 0, s>>>(a); \
+#define FVR_SNCC(DT)                              \
+  if (with_grad)                                  \
+    launch_sncc<DT, true>(variant, grid, s, a);   \
+  else                                            \
+    launch_sncc<DT, false>(variant, grid, s, a);  \
   break;
   switch (dtype) {
     case FVR_F32: FVR_SNCC(FVR_F32)
@@ -482,11 +510,12 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
   return FVR_OK;
 }
 
-int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews, int with_grad, double* mom,
-                         float* loss, float* ncc_out, void* stream) {
+int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews, int with_grad, int variant,
+                         double* mom, float* loss, float* ncc_out, void* stream) {
   if (!workspace || !mom || !loss || C < 1 || R < 1 || nviews < 1 || nviews > kMaxViews) return FVR_ERR_ARG;
+  if (variant < 0 || variant >= kSnccVariants) return FVR_ERR_ARG;
   const int64_t K = R * R;
-  const int tiles = static_cast<int>(cdiv64(K, sncc_tile(C, K, nviews)));
+  const int tiles = static_cast<int>(cdiv64(K, sncc_tile(C, K, nviews, variant)));
   tc_sncc_finalize_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const double*>(workspace), (int)C, nviews, tiles, with_grad ? M_NGRAD : 3, mom, loss, ncc_out);
   FVR_LAUNCH_CHECK();

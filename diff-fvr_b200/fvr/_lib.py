@@ -37,15 +37,17 @@ SIGNATURES = {
     "fvr_fft2d": (I32, [P, I32, I64, I64, I64, I32, I32, I32, I32, F64, I32, P, I64, I64, I64, I64, P, P, P, P]),
     "fvr_stencil_bytes": (I64, [I64, I64, I64, I32]),
     "fvr_stencil_scale_count": (I64, [I64, I64, I64]),
-    "fvr_stencil_build": (I32, [P, I32, I32, I64, I64, I64, I32, P, P, P, P]),
+    "fvr_stencil_build": (I32, [P, I32, I32, I64, I64, I64, I64, I32, P, P, P, P]),
     "fvr_slice3d_fwd": (I32, [P, I32, I64, I64, I64, I64, P, P, I64, P, P, I64, F32, F32, F32, P, P]),
     "fvr_slice3d_bwd_workspace": (I64, [I64, I64]),
     "fvr_slice3d_bwd": (I32, [P, I32, I64, I64, I64, I64, P, P, P, I64, P, P, I64, F32, F32, F32, P, P, P, I64, P]),
     "fvr_tc_axes": (I32, [P, I64, I32, I64, I64, I64, P, P]),
     "fvr_tc_sncc_workspace": (I64, [I64, I64, I64]),
     "fvr_tc_sncc_mom_stride": (I64, []),
-    "fvr_tc_sncc_moments": (I32, [I32, P, P, I64, I64, I64, P, I64, I32, P, P, P, P, I64, F64, I32, P, I64, P]),
-    "fvr_tc_sncc_finalize": (I32, [P, I64, I64, I32, I32, P, P, P, P]),
+    "fvr_tc_sncc_variants": (I32, []),
+    "fvr_tc_sncc_moments": (I32, [I32, P, P, I64, I64, I64, P, I64, I32, P, P, P, P, I64, F64, I32, I32, P, I64,
+                                  P]),
+    "fvr_tc_sncc_finalize": (I32, [P, I64, I64, I32, I32, I32, P, P, P, P]),
     "fvr_event_record": (I32, [P, P, I32]),
     "fvr_tc_sncc_backward": (I32, [P, I32, P, P, I64, P, I64, I64, I64, I64, F64, P, I32, P]),
     "fvr_tc_slice": (I32, [I32, P, P, I64, I64, I64, P, I64, P, I64, F64, I32, P, P]),
@@ -55,6 +57,22 @@ SIGNATURES = {
     "fvr_cmul_table": (I32, [P, P, I64, I64, P]),
     "fvr_hp_filter": (I32, [P, I64, I64, F64, P]),
     "fvr_linspace": (I32, [P, F32, F32, I64, P]),
+    "fvr_pou_block_sums": (I32, [P, I64, I64, I64, P, P, I64, P, P, I64, P, P, I64, P, P]),
+    "fvr_pou_build_blocks": (I32, [P, I64, I64, I64, P, P, I64, P, P, I64, P, P, I64, P, I64, P, I64, I64, I64, F64,
+                                   P, P]),
+    "fvr_pou_geo_stride": (I64, []),
+    "fvr_pou_pose": (I32, [P, P, I64, P, F64, P, I64, P, P, P]),
+    "fvr_pou_rays_prep": (I32, [P, P, I64, I64, P, P, P, P]),
+    "fvr_pou_rays_bwd_workspace": (I64, [I64, I64]),
+    "fvr_pou_rays_bwd": (I32, [P, P, I64, I64, P, P, P, I64, P]),
+    "fvr_pou_slice": (I32, [I32, P, P, I64, I64, P, I64, P, P, P]),
+    "fvr_pou_slice_adjoint_workspace": (I64, [I64, I64, I64]),
+    "fvr_pou_slice_adjoint": (I32, [I32, P, P, I64, I64, P, I64, P, P, P, I64, P]),
+    "fvr_pou_warp": (I32, [P, I64, I64, I64, P, P, P, I32, I64, P, P, P, I64, I64, F64, F64, P, P]),
+    "fvr_pou_warp_bwd_workspace": (I64, [I64, I64, I64]),
+    "fvr_pou_warp_bwd": (I32, [P, I64, I64, I64, P, P, P, I32, I64, P, P, P, I64, I64, F64, F64, P, P, P, P, P, I64,
+                               P]),
+    "fvr_pou_pose_backward": (I32, [P, I64, P, P, I64, P, P, I64, I64, P, F64, P, P, P]),
     "fvr_cncc_workspace": (I64, [I64, I64]),
     "fvr_cncc_forward": (I32, [P, P, I64, I64, I64, P, P, I64, P, P, P]),
     "fvr_cncc_backward": (I32, [P, P, I64, I64, I64, P, P, P, P, P]),
@@ -99,6 +117,7 @@ KERNELS_PER_CALL = {
     "fvr_slice3d_bwd": 2,
     "fvr_tc_slice_adjoint": 2,
     "fvr_cncc_forward": 2,
+    "fvr_pou_warp_bwd": 2,
 }
 launch_count = [0]
 

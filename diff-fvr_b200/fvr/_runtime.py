@@ -132,24 +132,26 @@ def spectrum3d(vol, pad_shape, convention, *, prec=L.F32_, premult=None, batch_f
 class Stencil:
     """Stencil ("corner-cube") copy of a centred spectrum (see include/fvr_b200.h)."""
 
-    def __init__(self, master, planar, dims, dtype):
+    def __init__(self, master, planar, dims, dtype, items=1):
         dev = L.require_cuda(master)
         D, H, W = (int(s) for s in dims)
         self.dims = (D, H, W)
+        self.items = int(items)
         self.dtype = dtype
         self.code = L.dtype_code(dtype)
-        nbytes = L.query("fvr_stencil_bytes", D, H, W, self.code)
-        if nbytes <= 0:
+        self.item_bytes = L.query("fvr_stencil_bytes", D, H, W, self.code)
+        if self.item_bytes <= 0:
             raise L.FvrError(f"unsupported stencil dtype {dtype}")
-        self.data = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        self.data = torch.empty(self.item_bytes * self.items, dtype=torch.uint8, device=dev)
         self.scales = None
+        self.item_scales = 0
         scratch = None
         if self.code == L.F16_:
-            nsc = L.query("fvr_stencil_scale_count", D, H, W)
-            self.scales = torch.empty(nsc, dtype=torch.float32, device=dev)
-            scratch = torch.empty(nsc, dtype=torch.int32, device=dev)
+            self.item_scales = L.query("fvr_stencil_scale_count", D, H, W)
+            self.scales = torch.empty(self.item_scales * self.items, dtype=torch.float32, device=dev)
+            scratch = torch.empty(self.item_scales * self.items, dtype=torch.int32, device=dev)
         m = master.contiguous()
-        L.call("fvr_stencil_build", L.ptr(m), L.dtype_code(m.dtype), int(planar), D, H, W, self.code,
+        L.call("fvr_stencil_build", L.ptr(m), L.dtype_code(m.dtype), int(planar), self.items, D, H, W, self.code,
                L.ptr(self.data), L.ptr(self.scales), L.ptr(scratch), L.stream_ptr(dev))
 
     def args(self):

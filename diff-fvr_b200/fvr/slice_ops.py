@@ -95,3 +95,60 @@ def triton_slice_available(tensor: torch.Tensor) -> bool:
 
 
 HAS_TRITON = False
+
+
+class _WarpSumFn(torch.autograd.Function):
+    """PoU pinhole warp + obliquity sum (triton_slice.py:498-591)."""
+
+    @staticmethod
+    def forward(ctx, imgs, d_b, cu, cv, rx, ry, ic, inv_ds, c_idx):
+        dev = L.require_cuda(imgs)
+        im = imgs.detach().float().contiguous()
+        B, N, P, _ = (int(x) for x in im.shape)
+        offs = [x.detach().to(dev, torch.float64).contiguous() for x in (d_b, cu, cv)]
+        r = [x.detach().to(dev, torch.float32).reshape(-1).contiguous() for x in (rx, ry, ic)]
+        K = int(r[0].numel())
+        out = torch.empty((N, K), dtype=torch.float32, device=dev)
+        L.call("fvr_pou_warp", L.ptr(im), B, N, P, L.ptr(offs[0]), L.ptr(offs[1]), L.ptr(offs[2]), 1, 1, L.ptr(r[0]),
+               L.ptr(r[1]), L.ptr(r[2]), K, 0, float(inv_ds), float(c_idx), L.ptr(out), L.stream_ptr(dev))
+        ctx.save_for_backward(im, *offs, *r)
+        ctx.meta = (float(inv_ds), float(c_idx), imgs.dtype, d_b.dtype)
+        return out
+
+    @staticmethod
+    def backward(ctx, g_out):
+        im, db, cu, cv, rx, ry, ic = ctx.saved_tensors
+        inv_ds, c_idx, idt, odt = ctx.meta
+        dev = im.device
+        B, N, P, _ = (int(x) for x in im.shape)
+        K = int(rx.numel())
+        g = g_out.detach().to(dev, torch.float32).reshape(N, K).contiguous()
+        gi = torch.zeros_like(im) if ctx.needs_input_grad[0] else None
+        goffs = torch.empty((3, B, N), dtype=torch.float64, device=dev)
+        wsb = L.query("fvr_pou_warp_bwd_workspace", B, N, K)
+        ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        L.call("fvr_pou_warp_bwd", L.ptr(im), B, N, P, L.ptr(db), L.ptr(cu), L.ptr(cv), 1, 1, L.ptr(rx), L.ptr(ry),
+               L.ptr(ic), K, 0, inv_ds, c_idx, L.ptr(g), L.ptr(gi), L.ptr(goffs), None, L.ptr(ws), wsb,
+               L.stream_ptr(dev))
+        return (None if gi is None else gi.to(idt), goffs[0].to(odt), goffs[1].to(odt), goffs[2].to(odt), None, None,
+                None, None, None)
+
+
+def pou_pinhole_warp_sum(imgs, d_b, cu, cv, rx_hw, ry_hw, inv_cos_hw, rx_flat, ry_flat, ic_flat, inv_ds, c_idx,
+                         use_triton: bool = True):
+    """Batched PoU pinhole bilinear warp + obliquity sum ``(N, H, W)``
+    (triton_slice.py:787-808); differentiable in imgs, d_b, cu, cv."""
+    H, W = int(rx_hw.shape[0]), int(rx_hw.shape[1])
+    out = _WarpSumFn.apply(imgs, d_b, cu, cv, rx_flat, ry_flat, ic_flat, inv_ds, c_idx)
+    return out.view(out.shape[0], H, W)
+
+
+def pou_pinhole_warp_sum_torch(imgs, d_b, cu, cv, rx_hw, ry_hw, inv_cos_hw, inv_ds, c_idx):
+    """API-compatible name for triton_slice.py:718-745; runs the CUDA warp."""
+    return pou_pinhole_warp_sum(imgs, d_b, cu, cv, rx_hw, ry_hw, inv_cos_hw, rx_hw.reshape(-1), ry_hw.reshape(-1),
+                                inv_cos_hw.reshape(-1), inv_ds, c_idx)
+
+
+def pou_pinhole_warp_sum_analytical_ref(imgs, d_b, cu, cv, rx_hw, ry_hw, inv_cos_hw, inv_ds, c_idx):
+    """API-compatible name for triton_slice.py:748-784; runs the CUDA warp."""
+    return pou_pinhole_warp_sum_torch(imgs, d_b, cu, cv, rx_hw, ry_hw, inv_cos_hw, inv_ds, c_idx)

@@ -35,3 +35,25 @@ def make_poses(n, seed, rot_deg=10.0, trans_mm=5.0):
     p[:, :3] = rng.uniform(-rot_deg, rot_deg, (n, 3))
     p[:, 3:] = rng.uniform(-trans_mm, trans_mm, (n, 3))
     return p
+
+
+def make_pinhole_mats(n, seed, sad_mm=765.0, rot_deg=10.0, trans_mm=5.0, device=None):
+    """Camera-to-world matrices ``[n, 4, 4]`` for ``PerspectiveSlabFVR.forward_pinhole``:
+    the camera (source at its origin, looking along +z) sits at distance
+    ``sad_mm`` from the isocentre, rotated about it by U(+-rot_deg) per axis
+    (rotation vector), then shifted by U(+-trans_mm) per axis."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    rv = rng.uniform(-np.radians(rot_deg), np.radians(rot_deg), (n, 3))
+    tj = rng.uniform(-trans_mm, trans_mm, (n, 3))
+    mats = np.zeros((n, 4, 4), np.float64)
+    for i in range(n):
+        th = np.linalg.norm(rv[i])
+        k = rv[i] / th if th > 0 else np.zeros(3)
+        Kx = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+        R = np.eye(3) + np.sin(th) * Kx + (1 - np.cos(th)) * (Kx @ Kx)
+        mats[i, :3, :3] = R
+        mats[i, :3, 3] = R @ np.array([0.0, 0.0, -sad_mm]) + tj[i]
+        mats[i, 3, 3] = 1.0
+    return torch.from_numpy(mats.astype(np.float32)).to(device)

@@ -32,7 +32,7 @@ import torch.nn as nn
 
 from . import _lib as L
 from . import _runtime as RT
-from . import profiling
+from . import autotune, profiling
 
 VIEW_AP, VIEW_LATERAL = 0, 1
 
@@ -60,10 +60,18 @@ def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
     fptrs = (ctypes.c_void_p * nv)(*[f.data_ptr() for f in fts])
     kap = RT.kappa(R, eng.spacing[0])
     s = L.stream_ptr(dev)
+    lin = RT.linspace(R, dev)
+
+    def run(variant):
+        L.call("fvr_tc_sncc_moments", *st.args(), L.ptr(p), C, nv, vcodes, fptrs, L.ptr(hp), L.ptr(lin), R, kap,
+               int(with_grad), int(variant), L.ptr(ws), ws_bytes, s)
+
+    variant = autotune.choose("sncc", (st.code, C, R, nv, int(with_grad), st.dims), run,
+                              L.load().fvr_tc_sncc_variants())
     with profiling.section("tc_sncc_moments"):
-        L.call("fvr_tc_sncc_moments", *st.args(), L.ptr(p), C, nv, vcodes, fptrs, L.ptr(hp),
-               L.ptr(RT.linspace(R, dev)), R, kap, int(with_grad), L.ptr(ws), ws_bytes, s)
-    L.call("fvr_tc_sncc_finalize", L.ptr(ws), C, R, nv, int(with_grad), L.ptr(mom), L.ptr(loss), None, s)
+        run(variant)
+    L.call("fvr_tc_sncc_finalize", L.ptr(ws), C, R, nv, int(with_grad), int(variant), L.ptr(mom), L.ptr(loss), None,
+           s)
     return mom, loss
 
 

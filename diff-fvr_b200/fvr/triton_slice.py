@@ -7,6 +7,9 @@ from .slice_ops import *  # noqa: F401,F403
 from .slice_ops import (  # noqa: F401
     HAS_TRITON,
     fourier_slice_3d,
+    pou_pinhole_warp_sum,
+    pou_pinhole_warp_sum_analytical_ref,
+    pou_pinhole_warp_sum_torch,
     fourier_slice_3d_torch,
     trilinear_slice_analytical_ref,
     triton_slice_available,

@@ -79,9 +79,11 @@ int fvr_fft2d(const void* in, int in_real, int64_t batch, int64_t n0, int64_t n1
  * to_precision cast (:90-95). */
 int64_t fvr_stencil_bytes(int64_t D, int64_t H, int64_t W, int dtype);
 int64_t fvr_stencil_scale_count(int64_t D, int64_t H, int64_t W);
-/* scratch_max: fvr_stencil_scale_count() uint32 (f16 only, else NULL) */
-int fvr_stencil_build(const void* master, int master_dtype, int master_planar, int64_t D, int64_t H, int64_t W,
-                      int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream);
+/* `items` spectra back to back (master item stride 2*D*H*W; out item stride
+ * fvr_stencil_bytes(); scales item stride fvr_stencil_scale_count()).
+ * scratch_max: items * fvr_stencil_scale_count() uint32 (f16 only, else NULL). */
+int fvr_stencil_build(const void* master, int master_dtype, int master_planar, int64_t items, int64_t D, int64_t H,
+                      int64_t W, int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream);
 
 /* --------------------------------------- drop-in trilinear slice gather -- */
 /* fourier_slice_3d on the reference layout vol[B][2][D][H][W] (dtype f32 /
@@ -115,18 +117,22 @@ int64_t fvr_tc_sncc_mom_stride(void);
  * slice at fp64 positions, applies the phase ramp kappa*(ku tx + kv ty) and
  * the high-pass table hp (NULL = none), and reduces the NCC moments; with
  * with_grad also the 14 pose-gradient moments.  Per-tile partial sums go to
- * `workspace`.  lin = torch.linspace(-1, 1, R).
+ * `workspace`.  lin = torch.linspace(-1, 1, R).  `variant` in
+ * [0, fvr_tc_sncc_variants()) selects the launch shape (samples in flight per
+ * thread, resident CTAs per SM); results do not depend on it beyond fp64
+ * summation order.
  * Replaces TorchDiffFVREngine._spectral_ncc_core / forward_spectral_ncc,
  * src/fvr/torch_engine.py:269-307 (the gather of :176-234 included). */
+int fvr_tc_sncc_variants(void);
 int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
                         const float* poses, int64_t C, int nviews, const int* views, const void* const* ftargs,
-                        const float* hp, const float* lin, int64_t R, double kappa, int with_grad, void* workspace,
-                        int64_t ws_bytes, void* stream);
-/* Pass 2: tile sums in fp64 -> mom[nviews][C][stride] (kept for the
- * backward); loss[v] = 1 - mean_c ncc (f32), loss[nviews] = sum of the view
- * losses; ncc_out[nviews][C] optional. */
-int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews, int with_grad, double* mom,
-                         float* loss, float* ncc_out, void* stream);
+                        const float* hp, const float* lin, int64_t R, double kappa, int with_grad, int variant,
+                        void* workspace, int64_t ws_bytes, void* stream);
+/* Pass 2 (same variant): tile sums in fp64 -> mom[nviews][C][stride] (kept
+ * for the backward); loss[v] = 1 - mean_c ncc (f32), loss[nviews] = sum of the
+ * view losses; ncc_out[nviews][C] optional. */
+int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews, int with_grad, int variant,
+                         double* mom, float* loss, float* ncc_out, void* stream);
 /* dL/dposes[C][6] from the saved moments and the device scalars
  * g[v * g_stride] = dL/dloss_v (tz column is zero: the reference never reads
  * poses[:, 5]); accumulate != 0 adds into grad_poses.
@@ -157,6 +163,77 @@ int fvr_cmul_table(void* x, const float* table, int64_t per, int64_t n, void* st
 int fvr_hp_filter(float* out, int64_t H, int64_t W, double sigma, void* stream);
 /* torch.linspace(start, end, n) in float32 */
 int fvr_linspace(float* out, float start, float end, int64_t n, void* stream);
+
+/* ------------------------------------------------ PoU-FVR cone beam ---- */
+/* Per-candidate-block windowed mass sum(vol * w0 * w1 * w2) over the block's
+ * support (fp64), k0*k1*k2 blocks in (i0, i1, i2) row-major order.  w_d are the
+ * 1D partition-of-unity windows [k_d][n_d] (float32), sup_d [k_d][2] = (first
+ * index, length) of each window's support.  The energy pruning input of
+ * PerspectiveSlabFVR.__init__, src/fvr/cone_beam_fvr.py:231-245. */
+int fvr_pou_block_sums(const float* vol, int64_t n0, int64_t n1, int64_t n2, const float* w0, const int* sup0,
+                       int64_t k0, const float* w1, const int* sup1, int64_t k1, const float* w2, const int* sup2,
+                       int64_t k2, double* sums, void* stream);
+/* Padded real blocks out[B][P][P][P] for the active candidate indices
+ * blocks[B]: windowed sub-volume centred in an M^3 cube, trilinear resize to
+ * block_res^3 (align_corners=False) times ds_block, times the sinc^2 table
+ * w3[block_res] per axis, zero pad to P^3.  cone_beam_fvr.py:241-283. */
+int fvr_pou_build_blocks(const float* vol, int64_t n0, int64_t n1, int64_t n2, const float* w0, const int* sup0,
+                         int64_t k0, const float* w1, const int* sup1, int64_t k1, const float* w2, const int* sup2,
+                         int64_t k2, const int* blocks, int64_t B, const float* w3, int64_t M, int64_t block_res,
+                         int64_t P, double ds_block, float* out, void* stream);
+/* Per pose: geo[N][18] (fp64) = source, u, v, n (the lattice basis base12 =
+ * src0, u0, v0, n0 moved by mats[N][4][4], or given directly as
+ * vecs[N][12] = (s, u, v, n) when mats is NULL), slice axes flip(u)*vscale,
+ * flip(v)*vscale; offs[B][N][3] (fp64) = (d_b, cu, cv) = (c_b - s).(n, u, v)
+ * for the block centres [B][3].  cone_beam_fvr.py:485-488, 507-521, 676-682. */
+int64_t fvr_pou_geo_stride(void);
+int fvr_pou_pose(const float* mats, const float* vecs, int64_t N, const double* base12, double vscale,
+                 const float* centers, int64_t B, double* geo, double* offs, void* stream);
+/* Explicit rays (cone_beam_fvr.py:451-457): per pose and pixel of
+ * trg[N][K][3], rx = (r.u)/cos, ry = (r.v)/cos, ic = 1/cos, cos = max(r.n, 0.1). */
+int fvr_pou_rays_prep(const float* trg, const double* geo, int64_t N, int64_t K, float* rx, float* ry, float* ic,
+                      void* stream);
+int64_t fvr_pou_rays_bwd_workspace(int64_t N, int64_t K);
+/* Explicit-ray adjoint: gray[N][K][3] = dL/d(rx, ry, ic) -> gtrg[N][K][3] and
+ * per-(pose, tile) partials of dL/d(src, u, v, n) in `workspace`. */
+int fvr_pou_rays_bwd(const float* trg, const double* geo, int64_t N, int64_t K, const float* gray, float* gtrg,
+                     void* workspace, int64_t ws_bytes, void* stream);
+/* Block slices out[B][N][P][P] (complex, ifftshift order for the image IFFT)
+ * from the stacked per-block stencil spectra (B items), at
+ * p = P//2 + freqs[j] u_xyz + freqs[i] v_xyz.  cone_beam_fvr.py:480-501. */
+int fvr_pou_slice(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P, const double* geo,
+                  int64_t N, const float* freqs, void* out, void* stream);
+int64_t fvr_pou_slice_adjoint_workspace(int64_t B, int64_t P, int64_t N);
+/* Slice adjoint for G[B][N][P][P] (complex, natural order): per-(pose, block,
+ * tile) partials of dL/du_xyz, dL/dv_xyz in `workspace` (consumed by
+ * fvr_pou_pose_backward). */
+int fvr_pou_slice_adjoint(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
+                          const double* geo, int64_t N, const float* freqs, const void* G, void* workspace,
+                          int64_t ws_bytes, void* stream);
+/* out[N][K] = ic[q] * sum_b bilinear(imgs[b][n], (d_b rx - cu)/ds + c, (d_b ry - cv)/ds + c),
+ * zero padding; offsets float (offs_f64 = 0) or double, element (b, n) at
+ * index (b*N + n) * ostride; ray tables shared (ray_stride 0) or per pose
+ * (ray_stride K).  Replaces pou_pinhole_warp_sum and
+ * _PouPinholeWarpSumFn.forward, src/fvr/triton_slice.py:341-407, 498-545, 787-808. */
+int fvr_pou_warp(const float* imgs, int64_t B, int64_t N, int64_t P, const void* db, const void* cu, const void* cv,
+                 int offs_f64, int64_t ostride, const float* rx, const float* ry, const float* ic, int64_t K,
+                 int64_t ray_stride, double inv_ds, double c_idx, float* out, void* stream);
+int64_t fvr_pou_warp_bwd_workspace(int64_t B, int64_t N, int64_t K);
+/* Adjoint: grad_imgs[B][N][P][P] += (scatter; NULL to skip; caller zeroes it),
+ * goffs[3][B][N] (fp64) = dL/d(d_b, cu, cv), and with gray != NULL the
+ * per-pixel dL/d(rx, ry, ic) [N][K][3] of the explicit-ray path.
+ * _PouPinholeWarpSumFn.backward, src/fvr/triton_slice.py:409-496, 547-591. */
+int fvr_pou_warp_bwd(const float* imgs, int64_t B, int64_t N, int64_t P, const void* db, const void* cu,
+                     const void* cv, int offs_f64, int64_t ostride, const float* rx, const float* ry, const float* ic,
+                     int64_t K, int64_t ray_stride, double inv_ds, double c_idx, const float* gout, float* grad_imgs,
+                     double* goffs, float* gray, void* workspace, int64_t ws_bytes, void* stream);
+/* d loss / d(src, u, v, n) gvec[N][12] and / or d loss / d mats[N][4][4]
+ * from the slice-adjoint partials (tiles per (pose, block)), the offset
+ * gradients goffs[3][B][N] and the explicit-ray partials (rtiles per pose);
+ * goffs and ray_part may be NULL.  Autograd of cone_beam_fvr.py:423-521, 676-682. */
+int fvr_pou_pose_backward(const double* sl_part, int64_t tiles, const double* goffs, const double* ray_part,
+                          int64_t rtiles, const double* geo, const float* centers, int64_t B, int64_t N,
+                          const double* base12, double vscale, float* gmats, float* gvec, void* stream);
 
 /* ----------------------------------------------------------- timing ---- */
 /* cudaEventRecordWithFlags(event, stream, external ? cudaEventRecordExternal

@@ -368,8 +368,8 @@ def forward_pinhole_grad(model, mats, lattice, w):
     inv_ds, c_idx = 1.0 / model.ds_block, float(P // 2)
     g_imgs, g_db, g_cu, g_cv = warp_sum_adjoint(imgs, d_b, cu, cv, rx, ry, ic, inv_ds, c_idx,
                                                 np.asarray(w, np.float64).reshape(N, -1))
-    # imgs = Re fftshift(ifft2(ifftshift(S)))  ->  G = ifftshift(fft2(fftshift(g))) / P^2
-    G = np.fft.ifftshift(np.fft.fft2(np.fft.fftshift(g_imgs, axes=(-2, -1)), axes=(-2, -1)), axes=(-2, -1)) / (P * P)
+    # imgs = Re fftshift(ifft2(ifftshift(S)))  ->  G = fftshift(fft2(ifftshift(g))) / P^2
+    G = np.fft.fftshift(np.fft.fft2(np.fft.ifftshift(g_imgs, axes=(-2, -1)), axes=(-2, -1)), axes=(-2, -1)) / (P * P)
     vs = float(P) * model.ds_block
     u_xyz, v_xyz = u[:, ::-1] * vs, v[:, ::-1] * vs
     fx, fy = model.FX_flat.reshape(1, -1), model.FY_flat.reshape(1, -1)
