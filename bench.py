@@ -292,9 +292,10 @@ def run_b200(args, torch):
                 "views": 2,
                 "out_res": OUT_RES,
                 "spectrum_storage": "f16 stencil with per-16^3-brick power-of-two scales (32-byte entry of 8 "
-                                    "complex corners); f32 interpolation, fp64 positions and reductions",
-                "step": "CUDA-graph replay: fused gather+NCC moments for both views, fp64 finalize, fp64 pose "
-                        "gradient (3 kernels)",
+                                    "complex corners); f32 interpolation, positions and phases from fp64 "
+                                    "per-row/column tables, fp64 reductions",
+                "step": "CUDA-graph replay of one kernel: gather + NCC/pose moments for both views, with the "
+                        "per-candidate fp64 finalize and pose gradient in the last CTA of each candidate",
                 "l2": "flushed before every timed step (256 MiB write)",
                 "parallelism": f"replicas x{ws}",
             },
@@ -307,7 +308,7 @@ def run_b200(args, torch):
             "f16_batched_over_fp32_single": value / ws / single_value,
             "roofline": {
                 "bound": "hbm",
-                "kernel": "tc_sncc_moments_kernel<f16, grad> (both views, 64 candidates)",
+                "kernel": "tc_sncc_moments_kernel<f16, grad, fused> (both views, 64 candidates)",
                 "achieved": achieved,
                 "peak": peak,
                 "unit": "GB/s",

@@ -1,8 +1,8 @@
 // Batched mixed-radix FFTs in shared memory (Stockham autosort), sm_100a.
 //
 // One CTA transforms `L` lines of length n entirely in shared memory
-// (ping-pong buffers, radix 4/2/3/5 butterflies plus a generic prime radix
-// up to 13).  Multi-dimensional transforms are sequences of line passes; the
+// (ping-pong buffers, radix 4/2/3/5 butterflies plus direct-DFT passes for
+// the other prime factors up to 127).  Multi-dimensional transforms are sequences of line passes; the
 // fftshift / ifftshift permutations, zero-padding of real volumes, sinc^2
 // pre-compensation, 1/n scaling and real-part / ReLU extraction are folded
 // into the first pass's loads and the last pass's stores, so every pass moves
@@ -17,6 +17,8 @@
 namespace fvr {
 
 constexpr int kMaxPass = 24;
+// Largest prime factor of a transform length (direct DFT pass, O(n * p) work).
+constexpr int kMaxPrime = 127;
 
 struct FftPlan {
   int n;
@@ -31,6 +33,14 @@ static bool make_plan(int64_t n, FftPlan* plan) {
   int64_t m = n;
   const int order[] = {4, 2, 3, 5, 7, 11, 13};
   for (int r : order) {
+    while (m % r == 0) {
+      if (plan->npass >= kMaxPass) return false;
+      plan->radix[plan->npass++] = r;
+      m /= r;
+    }
+  }
+  // remaining odd prime factors up to kMaxPrime run as direct DFT passes
+  for (int r = 17; r <= kMaxPrime && m > 1; r += 2) {
     while (m % r == 0) {
       if (plan->npass >= kMaxPass) return false;
       plan->radix[plan->npass++] = r;
@@ -156,6 +166,34 @@ __device__ __forceinline__ void bfly_generic(const Cx<T>* __restrict__ src, Cx<T
       Cx<T> w = tw[((t * m) % R) * nb];
       if (inv) w.y = -w.y;
       Cx<T> p = cmul(v[t], w);
+      acc.x += p.x;
+      acc.y += p.y;
+    }
+    dst[idx + m * Ns] = acc;
+  }
+}
+
+// Prime radix 17..kMaxPrime: direct DFT, inputs re-read from shared memory
+// for every output (no per-thread array of R values).
+template <typename T>
+__device__ __noinline__ void bfly_generic_wide(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst, int j, int Ns,
+                                               int n, int R, const Cx<T>* __restrict__ tw, bool inv) {
+  const int nb = n / R;
+  const int k = j % Ns;
+  const int ts = n / (Ns * R);
+  const int idx = (j / Ns) * Ns * R + k;
+  for (int m = 0; m < R; ++m) {
+    Cx<T> acc = src[j];
+    for (int t = 1; t < R; ++t) {
+      Cx<T> x = src[j + t * nb];
+      if (Ns > 1) {
+        Cx<T> w = tw[k * t * ts];
+        if (inv) w.y = -w.y;
+        x = cmul(x, w);
+      }
+      Cx<T> w = tw[((t * m) % R) * nb];
+      if (inv) w.y = -w.y;
+      const Cx<T> p = cmul(x, w);
       acc.x += p.x;
       acc.y += p.y;
     }
@@ -290,7 +328,12 @@ __global__ void __launch_bounds__(256) fft_lines_kernel(LD ld, bool ld_kc, ST st
         case 2: bfly<T, 2>(s, d, j, Ns, n, tw, binv); break;
         case 3: bfly<T, 3>(s, d, j, Ns, n, tw, binv); break;
         case 5: bfly<T, 5>(s, d, j, Ns, n, tw, binv); break;
-        default: bfly_generic<T>(s, d, j, Ns, n, r, tw, binv); break;
+        default:
+          if (r <= 13)
+            bfly_generic<T>(s, d, j, Ns, n, r, tw, binv);
+          else
+            bfly_generic_wide<T>(s, d, j, Ns, n, r, tw, binv);
+          break;
       }
     }
     __syncthreads();

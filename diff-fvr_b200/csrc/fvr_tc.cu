@@ -2,8 +2,9 @@
 //
 //  * fused zero-IFFT spectral NCC (src/fvr/torch_engine.py:176-234, 269-307):
 //    one pass per (candidate, view) that forms the slice axes from the pose in
-//    FP64, gathers the slice from the stencil spectrum at FP64 positions,
-//    applies the phase ramp and the high-pass filter, and reduces the NCC
+//    FP64, gathers the slice from the stencil spectrum at positions built
+//    from FP64 per-row / per-column tables, applies the phase ramp (table
+//    factors) and the high-pass filter, and reduces the NCC
 //    moments together with the 14 moments the pose gradient needs, so the
 //    adjoint is a per-candidate FP64 epilogue (no slice is stored and none is
 //    recomputed).  Several views share one launch.
@@ -85,10 +86,10 @@ constexpr int kSnccThreads = 256;
 struct SnccVariant {
   int group, min_blocks;
 };
-constexpr int kSnccVariants = 5;
+constexpr int kSnccVariants = 6;
 __host__ __device__ constexpr SnccVariant sncc_variant(int v) {
   return v == 1 ? SnccVariant{2, 4} : v == 2 ? SnccVariant{4, 3} : v == 3 ? SnccVariant{8, 1}
-                : v == 4 ? SnccVariant{2, 3} : SnccVariant{4, 2};
+                : v == 4 ? SnccVariant{2, 3} : v == 5 ? SnccVariant{3, 3} : SnccVariant{4, 2};
 }
 
 struct SnccArgs {
@@ -98,11 +99,74 @@ struct SnccArgs {
   int lateral[kMaxViews];
   const float* hp;   // [R*R] or null
   const float* lin;  // [R]
-  int R, C, tile;    // tile = samples per CTA, multiple of 256
+  int R, C, tile;    // tile = samples per CTA
+  int tab_rows;      // row-table entries per CTA (>= rows a tile touches)
   double kpi;        // kappa / pi
   double sx, sy, sz;
   double* partial;  // [nv][C][tiles][NM]
+  // fused epilogue (value_and_grad launch) only
+  unsigned* counters;  // [C + 1], zero on entry, left zero on exit
+  double* mom;         // [nv][C][kMomStride]
+  float* loss;         // [nv + 1]
+  float* ncc_out;      // [nv][C] or null
+  float* grad;         // [C][6]
+  const float* g;      // dL/dloss_v at g[v * g_stride]; null = all ones
+  int g_stride, accumulate;
+  double kappa;
 };
+
+// dL/dpose of one candidate from its per-view moment records (record of view v
+// at mom + v * view_stride): per axis dL/dp = gc (a A + 2 b B) with
+// a = 1/(s + eps), b = -cross Et / (2 s (s + eps)^2), s = sqrt(Ep Et),
+// gc = -g_v / C; rotations through the Euler vector-Jacobian product, the
+// in-plane translations from the phase moments.
+__device__ __forceinline__ void sncc_pose_grad(const double* mom, int64_t view_stride, const float* p, int nv,
+                                               int lat_bits, const float* g, int g_stride, int C, double sx,
+                                               double sy, double sz, double kappa, float r[6]) {
+  double gang[3] = {0.0, 0.0, 0.0}, gtx = 0.0, gty = 0.0;
+  for (int v = 0; v < nv; ++v) {
+    const double* m = mom + v * view_stride;
+    const double s = sqrt(m[M_EP] * m[M_ET]);
+    const double aa = 1.0 / (s + 1e-8);
+    const double bb = s > 0.0 ? -m[M_CROSS] * m[M_ET] / (2.0 * s * (s + 1e-8) * (s + 1e-8)) : 0.0;
+    const double gc = -(g ? static_cast<double>(g[v * g_stride]) : 1.0) / C;
+    double du[3], dv[3], ga[3];
+    for (int k = 0; k < 3; ++k) {
+      du[k] = gc * (aa * m[M_AU + k] + 2.0 * bb * m[M_BU + k]);
+      dv[k] = gc * (aa * m[M_AV + k] + 2.0 * bb * m[M_BV + k]);
+    }
+    axes_vjp(p, (lat_bits >> v) & 1, sx, sy, sz, du, dv, ga);
+    for (int k = 0; k < 3; ++k) gang[k] += ga[k];
+    gtx += gc * aa * kappa * m[M_PHU];
+    gty += gc * aa * kappa * m[M_PHV];
+  }
+  r[0] = static_cast<float>(gang[0]);
+  r[1] = static_cast<float>(gang[1]);
+  r[2] = static_cast<float>(gang[2]);
+  r[3] = static_cast<float>(gtx);
+  r[4] = static_cast<float>(gty);
+  r[5] = 0.f;
+}
+
+// bit v = lateral flag of view v (constant indices only: no dynamic indexing
+// of the kernel parameter space)
+__device__ __forceinline__ int lateral_bits(const int (&lat)[kMaxViews]) {
+  return (lat[0] & 1) | ((lat[1] & 1) << 1) | ((lat[2] & 1) << 2) | ((lat[3] & 1) << 3);
+}
+
+// Out-of-line form for the fused epilogue (one thread per candidate): keeps
+// its fp64 register demand out of the gather loop's allocation.
+__device__ __noinline__ void sncc_pose_grad_store(const double* mom, const float* p, int nv, int lat_bits,
+                                                  const float* g, int g_stride, int C, double sx, double sy,
+                                                  double sz, double kappa, float* o, int accumulate) {
+  float r[6];
+  sncc_pose_grad(mom, kMomStride, p, nv, lat_bits, g, g_stride, C, sx, sy, sz, kappa, r);
+  for (int k = 0; k < 6; ++k) o[k] = accumulate ? o[k] + r[k] : r[k];
+}
+
+__device__ __forceinline__ double sncc_ncc(const double* m) {
+  return m[M_CROSS] / (sqrt(m[M_EP] * m[M_ET]) + 1e-8);
+}
 
 // CTA sum of per-thread partials; every cross-lane / cross-warp step in fp64
 // (the pose-gradient moments are small residuals of large cancelling sums).
@@ -122,60 +186,271 @@ __device__ __forceinline__ void block_reduce_d(T (&acc)[NV], double* red, double
   }
 }
 
-template <int DT, bool GRAD, int GROUP, int MINB>
+// Per-CTA sample tables.  The slice position s + ku*u + kv*v is split into a
+// row part (s + ku*u, ku = lin[i]) and a column part (kv*v, kv = lin[j]); each
+// is formed in FP64 once per CTA and kept as an integer cell index plus a
+// float fraction in [0, 1], so a sample's position (their sum) is the FP64
+// position to within 2^-24 of a cell with integer adds and one float add per
+// axis.  The phase ramp factorises the same way:
+//   e^{i pi kpi (ku tx + kv ty)} = e^{i pi kpi ku tx} . e^{i pi kpi kv ty},
+// each factor from FP64 sincospi.  Entry n < R is column n; entry R + r is row
+// row0 + r.
+struct AxisTables {
+  int4* idx;    // (floor x, floor y, floor z, -)
+  float4* frac; // (frac x, frac y, frac z, k)
+  float2* ph;   // (cos, sin)
+};
+
+__device__ __forceinline__ AxisTables axis_tables(unsigned char* smem, int n_tab) {
+  AxisTables t;
+  t.idx = reinterpret_cast<int4*>(smem);
+  t.frac = reinterpret_cast<float4*>(smem + 16 * n_tab);
+  t.ph = reinterpret_cast<float2*>(smem + 32 * n_tab);
+  return t;
+}
+
+__device__ __forceinline__ void build_axis_tables(const AxisTables& t, int R, int row0, int n_row,
+                                                  const float* __restrict__ lin, const double* ax, double sx,
+                                                  double sy, double sz, double kpi) {
+  for (int n = threadIdx.x; n < R + n_row; n += blockDim.x) {
+    const bool col = n < R;
+    const float kf = __ldg(lin + (col ? n : row0 + n - R));
+    const double k = kf;
+    const double px = col ? k * ax[3] : fma(k, ax[0], sx);
+    const double py = col ? k * ax[4] : fma(k, ax[1], sy);
+    const double pz = col ? k * ax[5] : fma(k, ax[2], sz);
+    const double fx = floor(px), fy = floor(py), fz = floor(pz);
+    t.idx[n] = make_int4(static_cast<int>(fx), static_cast<int>(fy), static_cast<int>(fz), 0);
+    t.frac[n] = make_float4(static_cast<float>(px - fx), static_cast<float>(py - fy), static_cast<float>(pz - fz), kf);
+    double sn, cs;
+    sincospi(kpi * k * (col ? ax[7] : ax[6]), &sn, &cs);
+    t.ph[n] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
+  }
+}
+
+// Cell of sample (row entry a, column entry b); e = -1 when no corner of the
+// cell is inside (zero-padding partial: -1 <= p < n on every axis).
+struct TabCell {
+  int e;
+  float tx, ty, tz;
+  int ex, ey, ez;
+};
+
+__device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa, int4 ib, float4 fb) {
+  TabCell c;
+  c.tx = fa.x + fb.x;
+  c.ty = fa.y + fb.y;
+  c.tz = fa.z + fb.z;
+  int ix = ia.x + ib.x, iy = ia.y + ib.y, iz = ia.z + ib.z;
+  if (c.tx >= 1.f) { c.tx -= 1.f; ++ix; }
+  if (c.ty >= 1.f) { c.ty -= 1.f; ++iy; }
+  if (c.tz >= 1.f) { c.tz -= 1.f; ++iz; }
+  c.ex = ix + 1;
+  c.ey = iy + 1;
+  c.ez = iz + 1;
+  const bool ok = static_cast<unsigned>(c.ex) <= static_cast<unsigned>(s.W) &&
+                  static_cast<unsigned>(c.ey) <= static_cast<unsigned>(s.H) &&
+                  static_cast<unsigned>(c.ez) <= static_cast<unsigned>(s.D);
+  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + 1) + c.ex : -1;
+  return c;
+}
+
+// Entry load without the f16 brick scale applied (it multiplies the
+// interpolated value and derivatives instead: 8 products, not 16).
+template <int DT>
+__device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw<DT>& r) {
+  if constexpr (DT == FVR_F32) {
+    if (c.e < 0) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      return;
+    }
+    const float4* p = static_cast<const float4*>(s.data) + static_cast<int64_t>(c.e) * 4;
+    ldg256(p, r.q[0], r.q[1]);
+    ldg256(p + 2, r.q[2], r.q[3]);
+  } else {
+    if (c.e < 0) {
+      r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
+      if constexpr (DT == FVR_F16) r.sc = 0.f;
+      return;
+    }
+    ldg256(static_cast<const uint4*>(s.data) + static_cast<int64_t>(c.e) * 2, r.q[0], r.q[1]);
+    if constexpr (DT == FVR_F16) {
+      const int bx = (s.W + kBrick) / kBrick, by = (s.H + kBrick) / kBrick;
+      r.sc = __ldg(s.scales + ((c.ez / kBrick) * by + c.ey / kBrick) * bx + c.ex / kBrick);
+    }
+  }
+}
+
+template <int DT>
+__device__ __forceinline__ void tab_decode(const Raw<DT>& r, Sample8& v) {
+  if constexpr (DT == FVR_F16) {
+    const uint32_t w[8] = {r.q[0].x, r.q[0].y, r.q[0].z, r.q[0].w, r.q[1].x, r.q[1].y, r.q[1].z, r.q[1].w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v.re[i] = h_lo(w[i]);
+      v.im[i] = h_hi(w[i]);
+    }
+  } else {
+    raw_decode<DT>(r, v);
+  }
+}
+
+template <int DT, bool DERIV>
+__device__ __forceinline__ void tab_scale(const Raw<DT>& r, Interp& o) {
+  if constexpr (DT == FVR_F16) {
+    o.sr *= r.sc;
+    o.si *= r.sc;
+    if (DERIV) {
+      o.dxr *= r.sc;
+      o.dxi *= r.sc;
+      o.dyr *= r.sc;
+      o.dyi *= r.sc;
+      o.dzr *= r.sc;
+      o.dzi *= r.sc;
+    }
+  }
+}
+
+__device__ __forceinline__ void sncc_fused_epilogue(const SnccArgs& a, int c) {
+  __shared__ int s_last;
+  __shared__ double s_mom[kMaxViews * kMomStride];
+  const int tiles = gridDim.x, nv = gridDim.z, C = a.C;
+  __threadfence();  // this CTA's partial stores before its ticket
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(a.counters + c, 1u) == static_cast<unsigned>(tiles * nv - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // candidate c is complete: tile sums in fixed order
+  for (int t = threadIdx.x; t < nv * M_NGRAD; t += blockDim.x) {
+    const int v = t / M_NGRAD, m = t - v * M_NGRAD;
+    const double* src = a.partial + (static_cast<int64_t>(v) * C + c) * tiles * M_NGRAD + m;
+    double sum = 0.0;
+    for (int k = 0; k < tiles; ++k) sum += __ldcg(src + k * M_NGRAD);
+    s_mom[v * kMomStride + m] = sum;
+  }
+  __syncthreads();
+  if (threadIdx.x < nv) {
+    const int v = threadIdx.x;
+    const double n = sncc_ncc(s_mom + v * kMomStride);
+    s_mom[v * kMomStride + 17] = n;
+    if (a.ncc_out) a.ncc_out[v * C + c] = static_cast<float>(n);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nv * kMomStride; t += blockDim.x) {
+    const int v = t / kMomStride, m = t - v * kMomStride;
+    a.mom[(static_cast<int64_t>(v) * C + c) * kMomStride + m] = s_mom[t];
+  }
+  if (threadIdx.x == 0) {
+    sncc_pose_grad_store(s_mom, a.poses + 6 * c, nv, lateral_bits(a.lateral), a.g, a.g_stride, C, a.sx, a.sy, a.sz,
+                         a.kappa, a.grad + 6 * c, a.accumulate);
+    a.counters[c] = 0u;  // every ticket of candidate c has been taken
+  }
+  // global ticket: the last candidate forms the losses
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(a.counters + C, 1u) == static_cast<unsigned>(C - 1);
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  __shared__ double s_red[kSnccThreads / 32];
+  double total = 0.0;
+  for (int v = 0; v < nv; ++v) {
+    double sum = 0.0;
+    for (int k = threadIdx.x; k < C; k += blockDim.x)
+      sum += __ldcg(a.mom + (static_cast<int64_t>(v) * C + k) * kMomStride + 17);
+    sum = warp_sum(sum);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += s_red[w];
+      const double l = 1.0 - t / C;
+      a.loss[v] = static_cast<float>(l);
+      total += l;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.loss[nv] = static_cast<float>(total);
+    a.counters[C] = 0u;
+  }
+}
+
+// FUSE: the last CTA to finish a candidate (ticket per candidate) sums its
+// tiles, writes its moments, ncc and pose gradient; the last candidate to
+// finish (global ticket) forms the view losses.  Tickets reset themselves, so
+// the counters stay zero between launches.  No CTA ever waits on another.
+template <int DT, bool GRAD, int GROUP, int MINB, bool FUSE>
 __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(SnccArgs a) {
   constexpr int NM = GRAD ? M_NGRAD : 3;
   __shared__ double red[NM * (kSnccThreads / 32)];
   __shared__ double ax_s[8];
+  extern __shared__ __align__(16) unsigned char tab_smem[];
   const int tile = blockIdx.x, c = blockIdx.y, v = blockIdx.z;
   // select the view's parameters without dynamic indexing of the parameter space
   const int lateral = v == 0 ? a.lateral[0] : v == 1 ? a.lateral[1] : v == 2 ? a.lateral[2] : a.lateral[3];
   const float2* __restrict__ ft = v == 0 ? a.ftarg[0] : v == 1 ? a.ftarg[1] : v == 2 ? a.ftarg[2] : a.ftarg[3];
-  if (threadIdx.x == 0) slice_axes(a.poses + 6 * c, lateral, a.sx, a.sy, a.sz, ax_s);
-  __syncthreads();
-  const double ux = ax_s[0], uy = ax_s[1], uz = ax_s[2], vx = ax_s[3], vy = ax_s[4], vz = ax_s[5];
-  const float tx = static_cast<float>(ax_s[6]), ty = static_cast<float>(ax_s[7]);
   const int R = a.R, K = R * R;
   const int q_begin = tile * a.tile;
   const int q_end = min(q_begin + a.tile, K);
+  const int row0 = q_begin / R;
+  const AxisTables tab = axis_tables(tab_smem, R + a.tab_rows);
+  if (threadIdx.x == 0) slice_axes(a.poses + 6 * c, lateral, a.sx, a.sy, a.sz, ax_s);
+  __syncthreads();
+  build_axis_tables(tab, R, row0, (q_end - 1) / R - row0 + 1, a.lin, ax_s, a.sx, a.sy, a.sz, a.kpi);
+  __syncthreads();
   float acc[NM];  // per-thread partial over ~K*C*nv/(2*SMs*256) samples
 #pragma unroll
   for (int m = 0; m < NM; ++m) acc[m] = 0.f;
 
-  for (int base = q_begin; base < q_end; base += kSnccThreads * GROUP) {
+  // this thread's samples: q = q_begin + threadIdx.x + 256 m, (i, j) = divmod(q, R)
+  const int di = kSnccThreads / R, dj = kSnccThreads - di * R;
+  int q = q_begin + threadIdx.x;
+  int i = q / R, j = q - i * R;
+  while (q < q_end) {
     Raw<DT> raw[GROUP];
-    Cell cell[GROUP];
-    float kus[GROUP], kvs[GROUP], hs[GROUP];
+    int rc[GROUP];  // row entry << 16 | column entry
+    float hs[GROUP];
     float2 Ts[GROUP];
-    // issue every load of the group before using any of them
+    // issue every load of the group before using any of them; only the loads
+    // and the table entries stay live, positions and phases are re-derived
 #pragma unroll
     for (int g = 0; g < GROUP; ++g) {
-      const int q = base + g * kSnccThreads + threadIdx.x;
       const bool ok = q < q_end;
-      const int i = ok ? q / R : 0, j = ok ? q - i * R : 0;
-      kus[g] = __ldg(a.lin + i);
-      kvs[g] = __ldg(a.lin + j);
-      const double ku = kus[g], kv = kvs[g];
-      if (ok) {
-        cell[g] = stencil_cell<false>(a.st, fma(kv, vx, fma(ku, ux, a.sx)), fma(kv, vy, fma(ku, uy, a.sy)),
-                                      fma(kv, vz, fma(ku, uz, a.sz)));
-      } else {
-        cell[g] = Cell{-1, 0.f, 0.f, 0.f, 0, 0, 0};
-      }
-      raw_load<DT>(a.st, cell[g], raw[g]);
+      const int rn = ok ? R + i - row0 : 0, cn = ok ? j : 0;
+      rc[g] = (rn << 16) | cn;
+      TabCell cell = tab_cell(a.st, tab.idx[rn], tab.frac[rn], tab.idx[cn], tab.frac[cn]);
+      if (!ok) cell.e = -1;
+      tab_load<DT>(a.st, cell, raw[g]);
       Ts[g] = ok ? __ldg(ft + q) : make_float2(0.f, 0.f);
       hs[g] = ok ? (a.hp ? __ldg(a.hp + q) : 1.f) : 0.f;
+      q += kSnccThreads;
+      i += di;
+      j += dj;
+      if (j >= R) {
+        j -= R;
+        ++i;
+      }
     }
 #pragma unroll
     for (int g = 0; g < GROUP; ++g) {
+      const int rn = rc[g] >> 16, cn = rc[g] & 0xffff;
+      const float4 fa = tab.frac[rn], fb = tab.frac[cn];
+      const float2 pa = tab.ph[rn], pb = tab.ph[cn];
+      float tx = fa.x + fb.x, ty = fa.y + fb.y, tz = fa.z + fb.z;
+      if (tx >= 1.f) tx -= 1.f;
+      if (ty >= 1.f) ty -= 1.f;
+      if (tz >= 1.f) tz -= 1.f;
       Sample8 sm;
-      raw_decode<DT>(raw[g], sm);
+      tab_decode<DT>(raw[g], sm);
       Interp o;
-      trilerp<GRAD>(sm, cell[g].tx, cell[g].ty, cell[g].tz, o);
-      const float ku = kus[g], kv = kvs[g], h = hs[g];
+      trilerp<GRAD>(sm, tx, ty, tz, o);
+      tab_scale<DT, GRAD>(raw[g], o);
+      const float ku = fa.w, kv = fb.w, h = hs[g];
+      const float cs = pa.x * pb.x - pa.y * pb.y, sn = pa.y * pb.x + pa.x * pb.y;
       const float2 T = Ts[g];
-      float sn, cs;
-      phase_sincos(a.kpi, ku, kv, tx, ty, &sn, &cs);
       const float shr = h * (o.sr * cs - o.si * sn);
       const float shi = h * (o.sr * sn + o.si * cs);
       acc[M_CROSS] = fmaf(shr, T.x, fmaf(shi, T.y, acc[M_CROSS]));
@@ -212,6 +487,7 @@ __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(Snc
   block_reduce_d<NM, float>(acc, red, &tot);
   if (threadIdx.x < NM)
     a.partial[((static_cast<int64_t>(v) * a.C + c) * gridDim.x + tile) * NM + threadIdx.x] = tot;
+  if constexpr (FUSE && GRAD) sncc_fused_epilogue(a, c);
 }
 
 // Tile sums (fp64, fixed order) -> mom[v][c][0..NM), ncc in mom[v][c][17];
@@ -271,27 +547,10 @@ struct SnccGradArgs {
 __global__ void tc_sncc_grad_kernel(SnccGradArgs a) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= a.C) return;
-  const float* p = a.poses + 6 * c;
-  double gang[3] = {0.0, 0.0, 0.0}, gtx = 0.0, gty = 0.0;
-  for (int v = 0; v < a.nv; ++v) {
-    const double* m = a.mom + (static_cast<int64_t>(v) * a.C + c) * kMomStride;
-    const double s = sqrt(m[M_EP] * m[M_ET]);
-    const double aa = 1.0 / (s + 1e-8);
-    const double bb = s > 0.0 ? -m[M_CROSS] * m[M_ET] / (2.0 * s * (s + 1e-8) * (s + 1e-8)) : 0.0;
-    const double gc = -static_cast<double>(a.g[v * a.g_stride]) / a.C;
-    double du[3], dv[3], ga[3];
-    for (int k = 0; k < 3; ++k) {
-      du[k] = gc * (aa * m[M_AU + k] + 2.0 * bb * m[M_BU + k]);
-      dv[k] = gc * (aa * m[M_AV + k] + 2.0 * bb * m[M_BV + k]);
-    }
-    axes_vjp(p, a.lateral[v], a.sx, a.sy, a.sz, du, dv, ga);
-    for (int k = 0; k < 3; ++k) gang[k] += ga[k];
-    gtx += gc * aa * a.kappa * m[M_PHU];
-    gty += gc * aa * a.kappa * m[M_PHV];
-  }
+  float r[6];
+  sncc_pose_grad(a.mom + static_cast<int64_t>(c) * kMomStride, static_cast<int64_t>(a.C) * kMomStride,
+                 a.poses + 6 * c, a.nv, lateral_bits(a.lateral), a.g, a.g_stride, a.C, a.sx, a.sy, a.sz, a.kappa, r);
   float* o = a.grad + 6 * c;
-  const float r[6] = {static_cast<float>(gang[0]), static_cast<float>(gang[1]), static_cast<float>(gang[2]),
-                      static_cast<float>(gtx), static_cast<float>(gty), 0.f};
   for (int k = 0; k < 6; ++k) o[k] = a.accumulate ? o[k] + r[k] : r[k];
 }
 
@@ -407,7 +666,7 @@ static int stencil_from(int dtype, const void* data, const float* scales, int64_
 static double half_extent(int64_t n) { return 0.5 * static_cast<double>(n > 1 ? n - 1 : 1); }
 
 // Samples per CTA: one wave of min_blocks resident CTAs per SM (never more
-// CTAs than slots), whole passes of 256 x group samples.
+// CTAs than slots), at least 256 samples (one per thread) per CTA.
 static int sncc_tile(int64_t C, int64_t K, int nv, int variant) {
   static int sms = 0;
   if (sms == 0) {
@@ -417,25 +676,74 @@ static int sncc_tile(int64_t C, int64_t K, int nv, int variant) {
   }
   const SnccVariant v = sncc_variant(variant);
   const int64_t items = C * nv;
-  const int64_t pass = static_cast<int64_t>(kSnccThreads) * v.group;
   int64_t tiles = (static_cast<int64_t>(v.min_blocks) * sms) / items;
-  const int64_t max_tiles = cdiv64(K, pass);
+  const int64_t max_tiles = cdiv64(K, kSnccThreads);
   if (tiles > max_tiles) tiles = max_tiles;
   if (tiles < 1) tiles = 1;
-  int64_t tile = cdiv64(K, tiles);
-  tile = cdiv64(tile, pass) * pass;
-  return static_cast<int>(tile);
+  return static_cast<int>(cdiv64(K, tiles));
 }
 
-template <int DT, bool GRAD>
-static void launch_sncc(int variant, dim3 grid, cudaStream_t s, const SnccArgs& a) {
+// Row-table entries and dynamic shared memory of one moments CTA.
+static int sncc_tab_rows(int64_t R, int tile) { return static_cast<int>(tile / R + 2); }
+static int64_t sncc_smem(int64_t R, int tile) { return (R + sncc_tab_rows(R, tile)) * 40; }
+constexpr int64_t kSnccMaxSmem = 200 * 1024;
+
+template <int DT, bool GRAD, int GROUP, int MINB, bool FUSE>
+static void launch_sncc_v(dim3 grid, int smem, cudaStream_t s, const SnccArgs& a) {
+  auto k = tc_sncc_moments_kernel<DT, GRAD, GROUP, MINB, FUSE>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  k<<<grid, kSnccThreads, smem, s>>>(a);
+}
+
+template <int DT, bool GRAD, bool FUSE = false>
+static void launch_sncc(int variant, dim3 grid, int smem, cudaStream_t s, const SnccArgs& a) {
   switch (variant) {
-    case 1: tc_sncc_moments_kernel<DT, GRAD, 2, 4><<<grid, kSnccThreads, 0, s>>>(a); break;
-    case 2: tc_sncc_moments_kernel<DT, GRAD, 4, 3><<<grid, kSnccThreads, 0, s>>>(a); break;
-    case 3: tc_sncc_moments_kernel<DT, GRAD, 8, 1><<<grid, kSnccThreads, 0, s>>>(a); break;
-    case 4: tc_sncc_moments_kernel<DT, GRAD, 2, 3><<<grid, kSnccThreads, 0, s>>>(a); break;
-    default: tc_sncc_moments_kernel<DT, GRAD, 4, 2><<<grid, kSnccThreads, 0, s>>>(a); break;
+    case 1: launch_sncc_v<DT, GRAD, 2, 4, FUSE>(grid, smem, s, a); break;
+    case 2: launch_sncc_v<DT, GRAD, 4, 3, FUSE>(grid, smem, s, a); break;
+    case 3: launch_sncc_v<DT, GRAD, 8, 1, FUSE>(grid, smem, s, a); break;
+    case 4: launch_sncc_v<DT, GRAD, 2, 3, FUSE>(grid, smem, s, a); break;
+    case 5: launch_sncc_v<DT, GRAD, 3, 3, FUSE>(grid, smem, s, a); break;
+    default: launch_sncc_v<DT, GRAD, 4, 2, FUSE>(grid, smem, s, a); break;
   }
+}
+
+// Shared argument set-up of the moments launches.
+static int sncc_setup(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
+                      const float* poses, int64_t C, int nviews, const int* views, const void* const* ftargs,
+                      const float* hp, const float* lin, int64_t R, double kappa, int variant, SnccArgs* a,
+                      dim3* grid, int64_t* smem) {
+  Stencil st;
+  int rc = stencil_from(dtype, stencil, scales, D, H, W, &st);
+  if (rc) return rc;
+  if (!poses || !views || !ftargs || !lin || C < 1 || R < 1 || C > 65535) return FVR_ERR_ARG;
+  if (nviews < 1 || nviews > kMaxViews || R * R > (int64_t)1 << 30) return FVR_ERR_ARG;
+  if (variant < 0 || variant >= kSnccVariants) return FVR_ERR_ARG;
+  if ((D + 1) * (H + 1) * (W + 1) > INT32_MAX) return FVR_ERR_UNSUPPORTED;  // 32-bit entry index
+  const int64_t K = R * R;
+  const int tile = sncc_tile(C, K, nviews, variant);
+  *a = SnccArgs{};
+  a->st = st;
+  a->poses = poses;
+  for (int v = 0; v < nviews; ++v) {
+    if (!ftargs[v] || (views[v] != 0 && views[v] != 1)) return FVR_ERR_ARG;
+    a->ftarg[v] = static_cast<const float2*>(ftargs[v]);
+    a->lateral[v] = views[v];
+  }
+  a->hp = hp;
+  a->lin = lin;
+  a->R = (int)R;
+  a->C = (int)C;
+  a->tile = tile;
+  a->tab_rows = sncc_tab_rows(R, tile);
+  *smem = sncc_smem(R, tile);
+  if (*smem > kSnccMaxSmem) return FVR_ERR_UNSUPPORTED;
+  a->kpi = kappa / 3.14159265358979323846;
+  a->kappa = kappa;
+  a->sx = half_extent(W);
+  a->sy = half_extent(H);
+  a->sz = half_extent(D);
+  *grid = dim3(static_cast<unsigned>(cdiv64(K, tile)), static_cast<unsigned>(C), static_cast<unsigned>(nviews));
+  return FVR_OK;
 }
 
 }  // namespace fvr
@@ -465,40 +773,21 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
                         const float* poses, int64_t C, int nviews, const int* views, const void* const* ftargs,
                         const float* hp, const float* lin, int64_t R, double kappa, int with_grad, int variant,
                         void* workspace, int64_t ws_bytes, void* stream) {
-  Stencil st;
-  int rc = stencil_from(dtype, stencil, scales, D, H, W, &st);
+  SnccArgs a;
+  dim3 grid;
+  int64_t smem = 0;
+  int rc = sncc_setup(dtype, stencil, scales, D, H, W, poses, C, nviews, views, ftargs, hp, lin, R, kappa, variant,
+                      &a, &grid, &smem);
   if (rc) return rc;
-  if (!poses || !views || !ftargs || !lin || !workspace || C < 1 || R < 1 || C > 65535) return FVR_ERR_ARG;
-  if (nviews < 1 || nviews > kMaxViews || R * R > (int64_t)1 << 30) return FVR_ERR_ARG;
-  if (variant < 0 || variant >= kSnccVariants) return FVR_ERR_ARG;
+  if (!workspace) return FVR_ERR_ARG;
   if (ws_bytes < fvr_tc_sncc_workspace(C, R, nviews)) return FVR_ERR_WORKSPACE;
-  const int64_t K = R * R;
-  const int tile = sncc_tile(C, K, nviews, variant);
-  SnccArgs a{};
-  a.st = st;
-  a.poses = poses;
-  for (int v = 0; v < nviews; ++v) {
-    if (!ftargs[v] || (views[v] != 0 && views[v] != 1)) return FVR_ERR_ARG;
-    a.ftarg[v] = static_cast<const float2*>(ftargs[v]);
-    a.lateral[v] = views[v];
-  }
-  a.hp = hp;
-  a.lin = lin;
-  a.R = (int)R;
-  a.C = (int)C;
-  a.tile = tile;
-  a.kpi = kappa / 3.14159265358979323846;
-  a.sx = half_extent(W);
-  a.sy = half_extent(H);
-  a.sz = half_extent(D);
   a.partial = static_cast<double*>(workspace);
-  dim3 grid(static_cast<unsigned>(cdiv64(K, tile)), static_cast<unsigned>(C), static_cast<unsigned>(nviews));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-#define FVR_SNCC(DT)                              \
-  if (with_grad)                                  \
-    launch_sncc<DT, true>(variant, grid, s, a);   \
-  else                                            \
-    launch_sncc<DT, false>(variant, grid, s, a);  \
+#define FVR_SNCC(DT)                                         \
+  if (with_grad)                                             \
+    launch_sncc<DT, true>(variant, grid, (int)smem, s, a);   \
+  else                                                       \
+    launch_sncc<DT, false>(variant, grid, (int)smem, s, a);  \
   break;
   switch (dtype) {
     case FVR_F32: FVR_SNCC(FVR_F32)
@@ -506,6 +795,48 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
     case FVR_F16: FVR_SNCC(FVR_F16)
   }
 #undef FVR_SNCC
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int64_t fvr_tc_sncc_fused_workspace(int64_t C, int64_t R, int64_t nviews) {
+  if (C < 1 || R < 1 || nviews < 1) return 0;
+  return fvr_tc_sncc_workspace(C, R, nviews) + nviews * C * kMomStride * (int64_t)sizeof(double) +
+         cdiv64((C + 1) * (int64_t)sizeof(unsigned), 256) * 256;
+}
+
+int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
+                               const float* poses, int64_t C, int nviews, const int* views,
+                               const void* const* ftargs, const float* hp, const float* lin, int64_t R,
+                               double kappa, int variant, const float* g, int64_t g_stride, void* workspace,
+                               int64_t ws_bytes, float* loss, float* ncc_out, float* grad_poses, int accumulate,
+                               void* stream) {
+  SnccArgs a;
+  dim3 grid;
+  int64_t smem = 0;
+  int rc = sncc_setup(dtype, stencil, scales, D, H, W, poses, C, nviews, views, ftargs, hp, lin, R, kappa, variant,
+                      &a, &grid, &smem);
+  if (rc) return rc;
+  if (!workspace || !loss || !grad_poses) return FVR_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return FVR_ERR_ARG;
+  if (ws_bytes < fvr_tc_sncc_fused_workspace(C, R, nviews)) return FVR_ERR_WORKSPACE;
+  char* ws = static_cast<char*>(workspace);
+  a.partial = reinterpret_cast<double*>(ws);
+  a.mom = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews));
+  a.counters = reinterpret_cast<unsigned*>(ws + fvr_tc_sncc_workspace(C, R, nviews) +
+                                           nviews * C * kMomStride * (int64_t)sizeof(double));
+  a.loss = loss;
+  a.ncc_out = ncc_out;
+  a.grad = grad_poses;
+  a.g = g;
+  a.g_stride = (int)g_stride;
+  a.accumulate = accumulate;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (dtype) {
+    case FVR_F32: launch_sncc<FVR_F32, true, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_BF16: launch_sncc<FVR_BF16, true, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_F16: launch_sncc<FVR_F16, true, true>(variant, grid, (int)smem, s, a); break;
+  }
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }

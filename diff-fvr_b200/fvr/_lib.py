@@ -48,6 +48,13 @@ SIGNATURES = {
     "fvr_tc_sncc_moments": (I32, [I32, P, P, I64, I64, I64, P, I64, I32, P, P, P, P, I64, F64, I32, I32, P, I64,
                                   P]),
     "fvr_tc_sncc_finalize": (I32, [P, I64, I64, I32, I32, I32, P, P, P, P]),
+    "fvr_tc_sncc_fused_workspace": (I64, [I64, I64, I64]),
+    "fvr_edge_ncc_workspace": (I64, [I64, I64, I64, I64, I64]),
+    "fvr_edge_ncc_stats_count": (I64, []),
+    "fvr_edge_ncc_forward": (I32, [P, P, I64, I64, I64, I64, I64, I64, F32, I32, P, I64, P, P, P]),
+    "fvr_edge_ncc_backward": (I32, [P, P, I64, I64, I64, I64, I64, I64, F32, I32, P, P, I64, I32, P, P]),
+    "fvr_tc_sncc_value_and_grad": (I32, [I32, P, P, I64, I64, I64, P, I64, I32, P, P, P, P, I64, F64, I32, P, I64, P,
+                                         I64, P, P, P, I32, P]),
     "fvr_event_record": (I32, [P, P, I32]),
     "fvr_tc_sncc_backward": (I32, [P, I32, P, P, I64, P, I64, I64, I64, I64, F64, P, I32, P]),
     "fvr_tc_slice": (I32, [I32, P, P, I64, I64, I64, P, I64, P, I64, F64, I32, P, P]),
@@ -73,6 +80,12 @@ SIGNATURES = {
     "fvr_pou_warp_bwd": (I32, [P, I64, I64, I64, P, P, P, I32, I64, P, P, P, I64, I64, F64, F64, P, P, P, P, P, I64,
                                P]),
     "fvr_pou_pose_backward": (I32, [P, I64, P, P, I64, P, P, I64, I64, P, F64, P, P, P]),
+    "fvr_np_item_bytes": (I64, []),
+    "fvr_np_slices": (I32, [P, I64, I64, I64, P, I64, I64, P, P]),
+    "fvr_np_ncc_workspace": (I64, [I64]),
+    "fvr_np_ncc_moments": (I32, [P, I64, I64, I64, P, I64, P, P, I64, P, P]),
+    "fvr_np_pair_workspace": (I64, []),
+    "fvr_np_pair_moments": (I32, [P, P, I64, I64, P, I64, P, P]),
     "fvr_cncc_workspace": (I64, [I64, I64]),
     "fvr_cncc_forward": (I32, [P, P, I64, I64, I64, P, P, I64, P, P, P]),
     "fvr_cncc_backward": (I32, [P, P, I64, I64, I64, P, P, P, P, P]),
@@ -118,6 +131,9 @@ KERNELS_PER_CALL = {
     "fvr_tc_slice_adjoint": 2,
     "fvr_cncc_forward": 2,
     "fvr_pou_warp_bwd": 2,
+    "fvr_np_ncc_moments": 2,
+    "fvr_np_pair_moments": 2,
+    "fvr_edge_ncc_forward": 2,
 }
 launch_count = [0]
 

@@ -20,13 +20,10 @@ from typing import Dict, Optional, Tuple, Union
 import numpy as np
 import torch
 import torch.nn as nn
-import torch.nn.functional as F
 
 from . import _lib as L
 from . import _runtime as RT
 from . import profiling
-
-_SOBEL_CACHE: Dict[Tuple[str, torch.dtype], Tuple[torch.Tensor, torch.Tensor]] = {}
 
 SLAB_PRESETS: Dict[str, Dict[str, object]] = {
     "fast_coarse": {"grid_blocks": (2, 2, 2), "block_res": 64, "dtype": torch.bfloat16},
@@ -81,49 +78,64 @@ def sample_isocenter_parity_offsets(vox_spacing) -> torch.Tensor:
     return grid * sp.unsqueeze(0)
 
 
-def _get_sobel_kernels(device, dtype):
-    key = (str(device), dtype)
-    cached = _SOBEL_CACHE.get(key)
-    if cached is None:
-        kx = torch.tensor([[-1.0, 0.0, 1.0], [-2.0, 0.0, 2.0], [-1.0, 0.0, 1.0]], dtype=dtype,
-                          device=device).view(1, 1, 3, 3)
-        ky = torch.tensor([[-1.0, -2.0, -1.0], [0.0, 0.0, 0.0], [1.0, 2.0, 1.0]], dtype=dtype,
-                          device=device).view(1, 1, 3, 3)
-        cached = (kx, ky)
-        _SOBEL_CACHE[key] = cached
-    return cached
+class _EdgeNCCFn(torch.autograd.Function):
+    """Edge-dominant gradient NCC on ``libfvr_b200.so``: one tiled Sobel +
+    moment pass and a finalize forward; backward applies the transposed Sobel
+    and box filters to the closed-form NCC gradient fields."""
+
+    @staticmethod
+    def forward(ctx, pred, target, crop, weight, mean):
+        dev = L.require_cuda(pred)
+        a = pred.detach().to(torch.float32).contiguous()
+        b = target.detach().to(device=dev, dtype=torch.float32).contiguous()
+        if a.dim() != 4 or b.dim() != 4 or b.shape[1:] != a.shape[1:] or b.shape[0] not in (1, a.shape[0]):
+            raise ValueError(f"edge_dominant_ncc expects [B, C, H, W] inputs (target batch 1 or B), got "
+                             f"{tuple(a.shape)} and {tuple(b.shape)}")
+        B, C, H, W = (int(x) for x in a.shape)
+        Bt = int(b.shape[0])
+        ws_bytes = int(L.query("fvr_edge_ncc_workspace", B, C, H, W, crop))
+        ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=dev)
+        stats = torch.empty((B * C, int(L.query("fvr_edge_ncc_stats_count"))), dtype=torch.float64, device=dev)
+        out = torch.empty(1 if mean else B, dtype=torch.float32, device=dev)
+        L.call("fvr_edge_ncc_forward", L.ptr(a), L.ptr(b), B, Bt, C, H, W, int(crop), float(weight), int(mean),
+               L.ptr(ws), ws_bytes, L.ptr(stats), L.ptr(out), L.stream_ptr(dev))
+        ctx.save_for_backward(a, b, stats)
+        ctx.meta = (B, Bt, C, H, W, int(crop), float(weight), int(mean), pred.dtype, target.dtype)
+        return out[0] if mean else out
+
+    @staticmethod
+    def backward(ctx, g):
+        a, b, stats = ctx.saved_tensors
+        B, Bt, C, H, W, crop, weight, mean, pdt, tdt = ctx.meta
+        dev = a.device
+        g = g.detach().to(device=dev, dtype=torch.float32).contiguous().reshape(-1)
+        g_stride = 0 if mean else 1
+        s = L.stream_ptr(dev)
+        ga = gb = None
+        if ctx.needs_input_grad[0]:
+            ga = torch.empty_like(a)
+            L.call("fvr_edge_ncc_backward", L.ptr(a), L.ptr(b), B, Bt, C, H, W, crop, weight, mean, L.ptr(stats),
+                   L.ptr(g), g_stride, 0, L.ptr(ga), s)
+            ga = ga.to(pdt)
+        if ctx.needs_input_grad[1]:
+            gb = torch.empty_like(a)
+            L.call("fvr_edge_ncc_backward", L.ptr(a), L.ptr(b), B, Bt, C, H, W, crop, weight, mean, L.ptr(stats),
+                   L.ptr(g), g_stride, 1, L.ptr(gb), s)
+            gb = (gb.sum(0, keepdim=True) if Bt == 1 else gb).to(tdt)
+        return ga, gb, None, None, None
 
 
 def edge_dominant_ncc(pred, target, border_crop=None, multiscale_weight=0.25, reduction="mean"):
-    """Sobel gradient NCC on the cropped interior plus a 3x3-blurred scale
-    (cone_beam_fvr.py:71-112); tensor ops on the inputs' device."""
-    H = pred.shape[-1]
-    crop = max(4, H // 8) if border_crop is None else int(border_crop)
-
-    def _grad_ncc(a, b):
-        kx, ky = _get_sobel_kernels(a.device, a.dtype)
-        sl = slice(crop, -crop if crop > 0 else None)
-        ax = F.conv2d(a, kx, padding=1)[..., sl, sl]
-        ay = F.conv2d(a, ky, padding=1)[..., sl, sl]
-        bx = F.conv2d(b, kx, padding=1)[..., sl, sl]
-        by = F.conv2d(b, ky, padding=1)[..., sl, sl]
-
-        def _ncc(u, v):
-            u0 = u - u.mean(dim=(-2, -1), keepdim=True)
-            v0 = v - v.mean(dim=(-2, -1), keepdim=True)
-            num = (u0 * v0).sum(dim=(-2, -1))
-            den = (u0.square().sum(dim=(-2, -1)) * v0.square().sum(dim=(-2, -1))).clamp(min=1e-12).sqrt()
-            val = (num / den).mean(dim=1)
-            return val.mean() if reduction == "mean" else val
-
-        return 0.5 * (_ncc(ax, bx) + _ncc(ay, by))
-
-    g_fine = _grad_ncc(pred, target)
-    if multiscale_weight <= 0.0 or H < 96:
-        return g_fine
-    p_blur = F.avg_pool2d(pred, kernel_size=3, stride=1, padding=1)
-    t_blur = F.avg_pool2d(target, kernel_size=3, stride=1, padding=1)
-    return (1.0 - multiscale_weight) * g_fine + multiscale_weight * _grad_ncc(p_blur, t_blur)
+    """Edge-dominant gradient NCC of ``pred`` [B, C, H, W] against ``target``
+    ([B or 1, C, H, W]): Sobel-x / Sobel-y NCC on the interior after a border
+    crop of ``max(4, W // 8)`` pixels (W the last dim), averaged over
+    directions and channels, plus ``multiscale_weight`` x the same on 3x3
+    box-blurred images when the last dim is at least 96
+    (cone_beam_fvr.py:71-112).  ``reduction`` 'mean' gives a scalar, anything
+    else the per-item values [B]."""
+    W = int(pred.shape[-1])
+    crop = max(4, W // 8) if border_crop is None else int(border_crop)
+    return _EdgeNCCFn.apply(pred, target, crop, float(multiscale_weight), reduction == "mean")
 
 
 _LATTICE_CACHE: Dict[Tuple, Tuple] = {}

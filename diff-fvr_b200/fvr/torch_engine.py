@@ -75,6 +75,44 @@ def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
     return mom, loss
 
 
+def _sncc_fused(eng, p, views, ftargs, hp, R, out=None):
+    """One launch: moments, per-candidate finalize and pose gradient, view losses.
+    Returns (loss [nv + 1] f32, grad [C, 6] f32).  The workspace (with its
+    self-resetting ticket region, zeroed once here) is cached per shape on the
+    engine, so captured graphs keep a stable pointer; launches sharing it are
+    ordered on the engine's stream."""
+    dev = eng._dev
+    C = int(p.shape[0])
+    nv = len(views)
+    st = eng._stencil
+    ws_bytes = int(L.query("fvr_tc_sncc_fused_workspace", C, R, nv))
+    key = (C, R, nv, dev)
+    ws = eng._fused_ws.get(key)
+    if ws is None:
+        ws = torch.zeros(ws_bytes, dtype=torch.uint8, device=dev)
+        eng._fused_ws[key] = ws
+    loss = torch.empty(nv + 1, dtype=torch.float32, device=dev)
+    grad = torch.empty((C, 6), dtype=torch.float32, device=dev) if out is None else out
+    fts = [f.detach().to(device=dev, dtype=torch.complex64).contiguous() for f in ftargs]
+    for f in fts:
+        if f.numel() != R * R:
+            raise L.FvrError(f"target spectrum has {f.numel()} elements, expected {R}x{R}")
+    vcodes = (ctypes.c_int * nv)(*views)
+    fptrs = (ctypes.c_void_p * nv)(*[f.data_ptr() for f in fts])
+    kap = RT.kappa(R, eng.spacing[0])
+    s = L.stream_ptr(dev)
+    lin = RT.linspace(R, dev)
+
+    def run(variant):
+        L.call("fvr_tc_sncc_value_and_grad", *st.args(), L.ptr(p), C, nv, vcodes, fptrs, L.ptr(hp), L.ptr(lin), R, kap,
+               int(variant), None, 0, L.ptr(ws), ws_bytes, L.ptr(loss), None, L.ptr(grad), 0, s)
+
+    variant = autotune.choose("sncc_fused", (st.code, C, R, nv, st.dims), run, L.load().fvr_tc_sncc_variants())
+    with profiling.section("tc_sncc_moments"):
+        run(variant)
+    return loss, grad
+
+
 def _sncc_backward(eng, p, views, mom, g, g_stride, R, out=None):
     dev = p.device
     C = int(p.shape[0])
@@ -273,6 +311,7 @@ class TorchDiffFVREngine(nn.Module):
         del spec
         self.register_buffer("f_vol_5d", planar.to(dtype=dtype))
         self._stencil = RT.Stencil(self.f_vol_5d[0], True, self.pad_shape, self._stencil_dtype(dtype))
+        self._fused_ws = {}  # (C, R, views, device) -> workspace of the single-launch value_and_grad
 
     @staticmethod
     def _stencil_dtype(dtype):
@@ -354,15 +393,15 @@ class TorchDiffFVREngine(nn.Module):
 
     def spectral_ncc_value_and_grad(self, poses, f_targs, views=("ap", "lateral"), high_pass=True,
                                     cutoff_sigma=4.0, out_grad=None):
-        """``(sum_v loss_v, dloss/dposes [C, 6])`` without autograd: one fused gather pass
-        for every candidate and view, an fp64 finalize and an fp64 pose-gradient epilogue
-        (three kernel launches; capturable in a CUDA graph)."""
+        """``(sum_v loss_v, dloss/dposes [C, 6])`` without autograd: one kernel launch
+        gathers every candidate and view, reduces the NCC and pose moments and, in the
+        last CTA of each candidate, forms its fp64 pose gradient (capturable in a CUDA
+        graph).  Launches through one engine must stay on one stream."""
         p = self._prep_poses(poses).detach().to(torch.float32).contiguous()
         R = int(f_targs[0].shape[-1])
         hp = RT.hp_filter(R, R, cutoff_sigma, self._dev) if high_pass else None
         codes = tuple(_view_code(v) for v in views)
-        mom, loss = _sncc_forward(self, p, codes, f_targs, hp, R, True)
-        grad = _sncc_backward(self, p, codes, mom, RT.ones(self._dev), 0, R, out=out_grad)
+        loss, grad = _sncc_fused(self, p, codes, f_targs, hp, R, out=out_grad)
         return loss[len(codes)], grad
 
     def spectral_ncc_loss(self, pred_drr: torch.Tensor, target_drr: torch.Tensor, high_pass: bool = True,

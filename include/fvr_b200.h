@@ -29,7 +29,7 @@ typedef enum {
   FVR_OK = 0,
   FVR_ERR_ARG = 1,         /* null pointer, bad size, stride or alignment   */
   FVR_ERR_DTYPE = 2,       /* unsupported storage dtype for this entry      */
-  FVR_ERR_UNSUPPORTED = 3, /* e.g. FFT length with a prime factor above 13  */
+  FVR_ERR_UNSUPPORTED = 3, /* e.g. FFT length with a prime factor above 127 */
   FVR_ERR_WORKSPACE = 4,   /* caller workspace smaller than the query says  */
   FVR_ERR_CUDA = 5,        /* launch or driver error (cudaGetLastError)     */
   FVR_ERR_TIMEOUT = 6      /* a bounded device-side wait gave up            */
@@ -46,7 +46,7 @@ int fvr_device_supported(int device);
 /* Replaces torch.fft.fftn/ifft2/fft2 + fftshift/ifftshift at
  * src/fvr/torch_engine.py:80-81, 238-239, 263, 322-323,
  * src/fvr/cone_beam_fvr.py:291-294, 502-505 and scipy.fft at
- * src/fvr/diff_fvr.py:54, 168.  Lengths: 2^a 3^b 5^c 7^d 11^e 13^f <= 16384. */
+ * src/fvr/diff_fvr.py:54, 168.  Lengths <= 16384 whose prime factors are all <= 127. */
 int fvr_fft_supported(int64_t n);
 /* tw_out: n complex (prec FVR_F32: float2, FVR_F64: double2) = exp(-2 pi i m/n) */
 int fvr_fft_twiddles(int64_t n, int prec, void* tw_out, void* stream);
@@ -114,7 +114,9 @@ int64_t fvr_tc_sncc_mom_stride(void);
  * nviews (<= 4) views (views[v] = 0 'ap' / 1 'lateral', ftargs[v] the
  * complex [R][R] target spectrum of that view, host arrays of device
  * pointers) one pass forms the slice axes from the pose in fp64, gathers the
- * slice at fp64 positions, applies the phase ramp kappa*(ku tx + kv ty) and
+ * slice at positions assembled from fp64 per-row and per-column parts
+ * (within 2^-24 of a cell of the fp64 position), applies the phase ramp
+ * kappa*(ku tx + kv ty) (per-row x per-column factors from fp64 sincospi) and
  * the high-pass table hp (NULL = none), and reduces the NCC moments; with
  * with_grad also the 14 pose-gradient moments.  Per-tile partial sums go to
  * `workspace`.  lin = torch.linspace(-1, 1, R).  `variant` in
@@ -140,6 +142,24 @@ int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews
 int fvr_tc_sncc_backward(const double* mom, int nviews, const int* views, const float* g, int64_t g_stride,
                          const float* poses, int64_t C, int64_t D, int64_t H, int64_t W, double kappa,
                          float* grad_poses, int accumulate, void* stream);
+/* Single-launch loss + pose gradient (moments, finalize and backward fused):
+ * the last CTA to finish a candidate writes that candidate's fp64 moments,
+ * ncc_out[v][c] (optional) and grad_poses[c][6] (g = dL/dloss_v at
+ * g[v * g_stride], NULL = all ones; accumulate != 0 adds), and the last
+ * candidate writes loss[nviews + 1] as fvr_tc_sncc_finalize does.
+ * `workspace` (>= fvr_tc_sncc_fused_workspace bytes, 256-byte aligned) ends
+ * in a ticket region that must be zero before the first call (zero the
+ * whole workspace once after allocating it); every completed call leaves it
+ * zero.  Calls sharing one workspace must be stream-ordered.
+ * Replaces the forward + autograd backward of TorchDiffFVREngine.
+ * forward_spectral_ncc over several views, src/fvr/torch_engine.py:269-307. */
+int64_t fvr_tc_sncc_fused_workspace(int64_t C, int64_t R, int64_t nviews);
+int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
+                               const float* poses, int64_t C, int nviews, const int* views,
+                               const void* const* ftargs, const float* hp, const float* lin, int64_t R,
+                               double kappa, int variant, const float* g, int64_t g_stride, void* workspace,
+                               int64_t ws_bytes, float* loss, float* ncc_out, float* grad_poses, int accumulate,
+                               void* stream);
 /* Modulated slice S*exp(i phase) -> out[C][R][R] complex from fp64 axes;
  * shift != 0 writes it in ifftshift order (input of the image IFFT).
  * Replaces TorchDiffFVREngine._extract_slice_spectrum, torch_engine.py:176-234. */
@@ -235,6 +255,34 @@ int fvr_pou_pose_backward(const double* sl_part, int64_t tiles, const double* go
                           int64_t rtiles, const double* geo, const float* centers, int64_t B, int64_t N,
                           const double* base12, double vscale, float* gmats, float* gvec, void* stream);
 
+/* ----------------------------------------------- NumPy-convention path -- */
+/* Items are packed host-side as the struct
+ *   { double yaw, pitch, roll, tx, ty; int view, sh, sw, pad; int64 off; }
+ * (fvr_np_item_bytes() bytes; view 0 lateral, 1 ap, 2 axial; sh x sw slice
+ * rows x columns; off = element offset of the item's slice / target).  The
+ * spectrum f3d[D][H][W] is complex fp64 (fftshift(fftn(ifftshift(...)))). */
+int64_t fvr_np_item_bytes(void);
+/* Phase-ramped frequency slices (complex fp64) with map_coordinates
+ * (order 1, mode 'constant') sampling and the basis rz(yaw).ry(roll).rx(pitch)
+ * on (Z, Y, X).  Replaces DifferentiableFourierVolumeRenderer._euler_to_basis /
+ * extract_frequency_slice, src/fvr/diff_fvr.py:56-150; max_n >= sh*sw of every item. */
+int fvr_np_slices(const void* f3d, int64_t D, int64_t H, int64_t W, const void* items, int64_t n_items,
+                  int64_t max_n, void* out, void* stream);
+int64_t fvr_np_ncc_workspace(int64_t n_items);
+/* Per item, against targets (complex fp64, item's offset): mom[item][5] =
+ * (Re sum S conj T, sum |S|^2, sum |T|^2, sum u Im(S conj T), sum v Im(S conj T))
+ * in fp64 -> spectral NCC and its closed-form translation gradient
+ * (diff_fvr.py:184-195, gradients.py:27-74). */
+int fvr_np_ncc_moments(const void* f3d, int64_t D, int64_t H, int64_t W, const void* items, int64_t n_items,
+                       const void* targets, void* workspace, int64_t ws_bytes, double* mom, void* stream);
+int64_t fvr_np_pair_workspace(void);
+/* mom[5] of two complex fp64 [sh][sw] arrays, with u = j - sw/2, v = i - sh/2:
+ * (Re sum a conj b, sum |a|^2, sum |b|^2, sum u Im(a conj b), sum v Im(a conj b))
+ * (compute_spectral_ncc, diff_fvr.py:184-195; closed-form translation
+ * gradient, gradients.py:27-74). */
+int fvr_np_pair_moments(const void* a, const void* b, int64_t sh, int64_t sw, void* workspace, int64_t ws_bytes,
+                        double* mom, void* stream);
+
 /* ----------------------------------------------------------- timing ---- */
 /* cudaEventRecordWithFlags(event, stream, external ? cudaEventRecordExternal
  * : 0): lets a caller time one kernel inside a captured CUDA graph (no
@@ -252,6 +300,27 @@ int fvr_cncc_forward(const void* Fp, const void* Ft, int64_t B, int64_t Bt, int6
 /* X[B][n] = dL/dFp (complex) for the device scalar g = dL/dloss. */
 int fvr_cncc_backward(const void* Fp, const void* Ft, int64_t B, int64_t Bt, int64_t n, const float* hp,
                       const double* mom, const float* g, void* X, void* stream);
+
+/* ------------------------------------------ edge-dominant gradient NCC -- */
+/* pred a[B][C][H][W], target b[Bt][C][H][W] (Bt = 1 broadcast, or B), f32.
+ * Sobel-x / Sobel-y responses (zero padding) on the interior [crop, H-crop) x
+ * [crop, W-crop), NCC per direction (denominator sqrt(max(Suu Svv, 1e-12))),
+ * 0.5 (x + y) averaged over channels; when ms_weight > 0 and W >= 96 mixed
+ * (1 - w) fine + w (same on 3x3 box-blurred images, zero padding, divisor 9).
+ * out[0] = batch mean (reduction_mean) or out[B].  stats[B*C][20] (fp64
+ * moments) is kept for the backward.
+ * Replaces edge_dominant_ncc, src/fvr/cone_beam_fvr.py:71-112. */
+int64_t fvr_edge_ncc_workspace(int64_t B, int64_t C, int64_t H, int64_t W, int64_t crop);
+int64_t fvr_edge_ncc_stats_count(void);
+int fvr_edge_ncc_forward(const float* a, const float* b, int64_t B, int64_t Bt, int64_t C, int64_t H, int64_t W,
+                         int64_t crop, float ms_weight, int reduction_mean, void* workspace, int64_t ws_bytes,
+                         double* stats, float* out, void* stream);
+/* d out / d a (wrt_b = 0) or d out / d b per batch item (wrt_b = 1; the
+ * caller sums over the batch for a broadcast target) into grad[B][C][H][W],
+ * scaled by the upstream g[b * g_stride] (g_stride 0 for the mean). */
+int fvr_edge_ncc_backward(const float* a, const float* b, int64_t B, int64_t Bt, int64_t C, int64_t H, int64_t W,
+                          int64_t crop, float ms_weight, int reduction_mean, const double* stats, const float* g,
+                          int64_t g_stride, int wrt_b, float* grad, void* stream);
 
 #ifdef __cplusplus
 }

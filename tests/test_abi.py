@@ -47,7 +47,8 @@ def test_status_strings_and_queries(lib):
     assert L.load().fvr_status_string(0).decode() == "ok"
     assert "workspace" in L.load().fvr_status_string(4).decode()
     assert L.load().fvr_fft_supported(192) == 1
-    assert L.load().fvr_fft_supported(17) == 0
+    assert L.load().fvr_fft_supported(17) == 1
+    assert L.load().fvr_fft_supported(131) == 0
     assert L.query("fvr_stencil_bytes", 3, 3, 3, 0) == 4 * 4 * 4 * 64
     assert L.query("fvr_stencil_bytes", 3, 3, 3, 1) == 4 * 4 * 4 * 32
 

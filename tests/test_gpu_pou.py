@@ -275,3 +275,78 @@ def test_full_geometry_subset_vs_oracle():
     assert rel_l2(out.detach().cpu().numpy(), ref) < 1e-5
     gref = opou.forward_pinhole_grad(om, mats.numpy(), olat, w)
     assert rel_l2(m.grad.cpu().numpy(), gref) < 1e-4
+
+
+# ----------------------------------------------------- edge-dominant NCC (a17)
+
+
+def _edge_torch64(pred, target, crop, w):
+    """Plain PyTorch float64 statement of the edge-dominant NCC per item [B]
+    (test reference for the CUDA kernel's values and autograd gradients)."""
+    import torch.nn.functional as F
+
+    kx = torch.tensor([[-1.0, 0, 1], [-2, 0, 2], [-1, 0, 1]], dtype=torch.float64, device=pred.device)
+    kx = kx.view(1, 1, 3, 3).repeat(pred.shape[1], 1, 1, 1)
+    ky = kx.transpose(-1, -2).contiguous()
+    C = pred.shape[1]
+
+    def resp(x, k):
+        r = F.conv2d(x, k, padding=1, groups=C)
+        return r[..., crop:r.shape[-2] - crop, crop:r.shape[-1] - crop]
+
+    def ncc(u, v):
+        u0 = u - u.mean((-2, -1), keepdim=True)
+        v0 = v - v.mean((-2, -1), keepdim=True)
+        den = ((u0 * u0).sum((-2, -1)) * (v0 * v0).sum((-2, -1))).clamp(min=1e-12).sqrt()
+        return ((u0 * v0).sum((-2, -1)) / den).mean(1)
+
+    def scale(a, b):
+        return 0.5 * (ncc(resp(a, kx), resp(b, kx)) + ncc(resp(a, ky), resp(b, ky)))
+
+    val = scale(pred, target.expand_as(pred))
+    if w > 0 and pred.shape[-1] >= 96:
+        box = lambda x: F.avg_pool2d(x, 3, stride=1, padding=1)  # noqa: E731
+        val = (1 - w) * val + w * scale(box(pred), box(target.expand_as(pred)))
+    return val
+
+
+@pytest.mark.parametrize("H", [48, 96])
+def test_edge_dominant_ncc_golden(golden, H):
+    from fvr.cone_beam_fvr import edge_dominant_ncc
+
+    g = golden("pou")
+    a = _t(g[f"edge_{H}_a"]).requires_grad_(True)
+    b = _t(g[f"edge_{H}_b"])
+    val = edge_dominant_ncc(a, b, reduction="none")
+    val.sum().backward()
+    assert rel_l2(val.detach().cpu().numpy(), g[f"edge_{H}_val"]) < 1e-5
+    assert rel_l2(a.grad.cpu().numpy(), g[f"edge_{H}_grad"]) < 1e-4
+    ref = opou.edge_dominant_ncc(g[f"edge_{H}_a"], g[f"edge_{H}_b"], reduction="none")
+    assert np.allclose(val.detach().cpu().numpy(), ref, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("B,Bt,C,H,W,crop,w,mean", [
+    (3, 1, 1, 64, 112, None, 0.25, True),     # broadcast target, rectangular, blurred scale on
+    (2, 2, 2, 100, 96, 0, 0.4, False),        # no crop: zero-padded borders enter the moments
+    (4, 4, 1, 130, 70, 7, 0.25, False),       # last dim < 96: fine scale only
+    (1, 1, 1, 256, 256, None, 0.25, True),    # detector size of the PoU workload
+])
+def test_edge_dominant_ncc_vs_torch64(B, Bt, C, H, W, crop, w, mean):
+    from fvr.cone_beam_fvr import edge_dominant_ncc
+
+    rng = np.random.default_rng(B * 100 + H)
+    pa = rng.standard_normal((B, C, H, W)).cumsum(-1).cumsum(-2)
+    pb = pa[:Bt] + 0.3 * rng.standard_normal((Bt, C, H, W)).cumsum(-2)
+    a = _t(pa).requires_grad_(True)
+    b = _t(pb).requires_grad_(True)
+    val = edge_dominant_ncc(a, b, border_crop=crop, multiscale_weight=w, reduction="mean" if mean else "none")
+    (val * torch.arange(1, val.numel() + 1, device=DEV, dtype=torch.float32).reshape(val.shape)).sum().backward()
+    a64 = torch.tensor(pa, dtype=torch.float64, device=DEV, requires_grad=True)
+    b64 = torch.tensor(pb, dtype=torch.float64, device=DEV, requires_grad=True)
+    c = max(4, W // 8) if crop is None else crop
+    ref = _edge_torch64(a64, b64, c, w)
+    ref = ref.mean() if mean else ref
+    (ref * torch.arange(1, ref.numel() + 1, device=DEV, dtype=torch.float64).reshape(ref.shape)).sum().backward()
+    assert rel_l2(val.detach().double().cpu().numpy(), ref.detach().cpu().numpy()) < 1e-6
+    assert rel_l2(a.grad.double().cpu().numpy(), a64.grad.cpu().numpy()) < 1e-4
+    assert rel_l2(b.grad.double().cpu().numpy(), b64.grad.cpu().numpy()) < 1e-4

@@ -45,7 +45,7 @@ def test_spectrum3d_torch_and_numpy_conventions(shape):
     assert rel_l2(got2, ref2) < 1e-13
 
 
-@pytest.mark.parametrize("n0,n1", [(16, 16), (20, 24), (48, 45), (96, 192), (128, 128), (26, 14)])
+@pytest.mark.parametrize("n0,n1", [(16, 16), (20, 24), (48, 45), (96, 192), (128, 128), (26, 14), (34, 17), (127, 254), (38, 6)])
 def test_fft2d_shifts_scales_and_real_outputs(n0, n1):
     from fvr import _runtime as RT
 
@@ -361,3 +361,28 @@ def test_cpu_inputs_are_moved_and_outputs_finite(big):
     (eng(pose, view="ap", out_res=64) ** 2).sum().backward()
     assert pose.grad.shape == (1, 6) and bool(torch.all(torch.isfinite(pose.grad)))
     assert not bool(torch.all(pose.grad == 0))
+
+
+def test_fused_value_and_grad_every_variant_repeatable(big, monkeypatch):
+    """The single-launch value_and_grad (per-candidate and global tickets) agrees
+    with the autograd path for every launch variant, is bitwise repeatable, and
+    leaves its ticket region zero."""
+    import fvr._lib as L
+
+    _, eng, _ = big
+    poses = _t(tc.make_poses(24, 8))
+    tp = _t(tc.make_poses(1, 9))
+    fa = eng.prepare_spectral_target(eng(tp, view="ap", out_res=128))
+    fl = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=128))
+    p1 = poses.clone().requires_grad_(True)
+    l1 = eng.forward_spectral_ncc(p1, fa, view="ap") + eng.forward_spectral_ncc(p1, fl, view="lateral")
+    l1.backward()
+    for variant in range(L.load().fvr_tc_sncc_variants()):
+        monkeypatch.setenv("FVR_SNCC_FUSED_VARIANT", str(variant))
+        la, ga = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
+        lb, gb = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
+        assert torch.equal(la, lb) and torch.equal(ga, gb), variant
+        assert abs(float(la) - float(l1)) < 1e-6, variant
+        assert torch.allclose(ga, p1.grad, rtol=1e-5, atol=1e-9), variant
+        ws = eng._fused_ws[(24, 128, 2, poses.device)]
+        assert int(ws[-256:].count_nonzero()) == 0

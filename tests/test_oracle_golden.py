@@ -247,3 +247,28 @@ def test_warp_sum_and_adjoint(golden):
     assert rel_l2(gdb, g["warp_g_db"]) < 1e-5
     assert rel_l2(gcu, g["warp_g_cu"]) < 1e-5
     assert rel_l2(gcv, g["warp_g_cv"]) < 1e-5
+
+
+# ---------------------------------------------------------- NumPy convention
+
+
+def test_numpy_convention_oracle(golden):
+    from oracle import numpy_convention as nc
+
+    g = golden("numpy_renderer")
+    f3d = nc.spectrum(g["vol"], 2.0)
+    assert rel_l2(f3d, g["f_3d"]) < 1e-13
+    assert rel_l2(nc.spectrum(g["vol"], 2.0, premult=False), g["f_3d_nopremult"]) < 1e-13
+    pose = g["pose5"]
+    for view in ("ap", "lateral", "axial"):
+        assert rel_l2(nc.extract_frequency_slice(f3d, *pose, view=view), g[f"slice_{view}"]) < 1e-12
+        assert rel_l2(nc.render_drr(f3d, g["vol"].shape, *pose, view=view), g[f"drr_{view}"]) < 1e-12
+        assert rel_l2(nc.render_drr(f3d, g["vol"].shape, *pose, view=view, crop_to_roi=False),
+                      g[f"drr_nocrop_{view}"]) < 1e-12
+    t_ap = nc.extract_frequency_slice(f3d, view="ap")
+    t_lat = nc.extract_frequency_slice(f3d, view="lateral")
+    assert abs(nc.spectral_ncc(g["slice_ap"], t_ap) - float(g["ncc_ap"])) < 1e-13
+    loss, grad = nc.biplanar_loss_and_gradients(f3d, g["bip_pose"], t_ap, t_lat)
+    assert abs(loss - float(g["bip_loss"])) < 1e-12
+    assert np.allclose(grad, g["bip_grad"], rtol=1e-9, atol=1e-12)
+    assert np.allclose(nc.ncc_and_grad_translation(g["slice_lateral"], t_lat), g["tgrad"], rtol=1e-10, atol=1e-13)
