@@ -12,6 +12,8 @@
 //    ifftshift order for the 2D IFFT, and the per-sample slice adjoint.
 //  * FP64 pose maps: Euler (yaw Z, pitch Y, roll X) -> slice axes and the
 //    Euler vector-Jacobian product (torch_engine.py:139-211).
+#include <mutex>
+
 #include "fvr_pose.cuh"
 #include "fvr_stencil.cuh"
 
@@ -746,6 +748,67 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
   return FVR_OK;
 }
 
+// ----------------------------------------------------------------------------
+// Scratch of the allocation-free value-and-gradient entry point.
+//
+// fvr_tc_sncc_value_and_grad_static computes exactly what
+// fvr_tc_sncc_value_and_grad computes, with its workspace in this fixed
+// file-scope device array instead of caller memory.  It serves callers that
+// cannot allocate device memory where they call: a host program that links
+// only this C ABI and owns no device allocator, or a loop that must not enter
+// an allocator between steps (cudaMalloc / cudaFree may synchronise the
+// device).
+//
+// Size (about 354 KB per device): kStaticRecords partial-moment records of
+// 17 doubles, kStaticItems (candidate, view) moment records of 18 doubles and
+// kStaticItems + 1 ticket counters.  Calls needing more -- more than 512
+// (candidate, view) pairs, or more than 2048 (candidate, view, tile) partial
+// records for the launch variant -- are refused with FVR_ERR_WORKSPACE before
+// anything is launched.
+//
+// Start state: the ticket counters must be zero before a launch; the static
+// initialiser zeroes them and every completed launch leaves them zero.  The
+// partial and moment records are fully written by every launch, so nothing
+// else needs to start at zero.
+//
+// Set-up: the first call on each device, made with that device current,
+// resolves the array's device address with cudaGetSymbolAddress and caches
+// it; make that first call before any stream capture begins.
+//
+// Races: one array per device is shared by every caller in the process.
+// Calls on the same device must be ordered (one stream, or explicit
+// synchronisation); two calls that overlap in time corrupt each other's
+// scratch and tickets.
+// ----------------------------------------------------------------------------
+constexpr int64_t kStaticItems = 512;
+constexpr int64_t kStaticRecords = 2048;
+constexpr int64_t kStaticPartialDoubles = kStaticRecords * M_NGRAD;
+constexpr int64_t kStaticMomDoubles = kStaticItems * kMomStride;
+constexpr int64_t kStaticTicketDoubles = (kStaticItems + 1 + 1) / 2;  // unsigned counters, two per double
+constexpr int64_t kStaticDoubles = kStaticPartialDoubles + kStaticMomDoubles + kStaticTicketDoubles;
+constexpr int kStaticMaxDevices = 64;
+
+static __device__ __align__(256) double g_sncc_static_scratch[kStaticDoubles];
+
+static std::mutex g_static_mu;
+static double* g_static_ptr[kStaticMaxDevices] = {};
+
+// Device address of this device's scratch array (resolved once per device).
+static int static_scratch(double** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return FVR_ERR_CUDA;
+  if (dev < 0 || dev >= kStaticMaxDevices) return FVR_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&p, g_sncc_static_scratch);
+    if (rc != cudaSuccess || !p) return FVR_ERR_CUDA;
+    g_static_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_static_ptr[dev];
+  return FVR_OK;
+}
+
 }  // namespace fvr
 
 using namespace fvr;
@@ -932,6 +995,42 @@ int fvr_tc_slice_adjoint(int dtype, const void* stencil, const float* scales, in
   tc_adjoint_grad_kernel<<<static_cast<unsigned>(cdiv64(C, 128)), 128, 0, s>>>(
       part, tiles, poses, (int)C, view, half_extent(W), half_extent(H), half_extent(D), kappa, grad_poses,
       accumulate);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H,
+                                      int64_t W, const float* poses, int64_t C, int nviews, const int* views,
+                                      const void* const* ftargs, const float* hp, const float* lin, int64_t R,
+                                      double kappa, int variant, const float* g, int64_t g_stride, float* loss,
+                                      float* ncc_out, float* grad_poses, int accumulate, void* stream) {
+  SnccArgs a;
+  dim3 grid;
+  int64_t smem = 0;
+  int rc = sncc_setup(dtype, stencil, scales, D, H, W, poses, C, nviews, views, ftargs, hp, lin, R, kappa, variant,
+                      &a, &grid, &smem);
+  if (rc) return rc;
+  if (!loss || !grad_poses) return FVR_ERR_ARG;
+  const int64_t items = C * nviews;
+  if (items > kStaticItems || items * static_cast<int64_t>(grid.x) > kStaticRecords) return FVR_ERR_WORKSPACE;
+  double* scratch = nullptr;
+  rc = static_scratch(&scratch);
+  if (rc) return rc;
+  a.partial = scratch;
+  a.mom = scratch + kStaticPartialDoubles;
+  a.counters = reinterpret_cast<unsigned*>(scratch + kStaticPartialDoubles + kStaticMomDoubles);
+  a.loss = loss;
+  a.ncc_out = ncc_out;
+  a.grad = grad_poses;
+  a.g = g;
+  a.g_stride = (int)g_stride;
+  a.accumulate = accumulate;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (dtype) {
+    case FVR_F32: launch_sncc<FVR_F32, true, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_BF16: launch_sncc<FVR_BF16, true, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_F16: launch_sncc<FVR_F16, true, true>(variant, grid, (int)smem, s, a); break;
+  }
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }

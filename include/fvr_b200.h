@@ -160,6 +160,26 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
                                double kappa, int variant, const float* g, int64_t g_stride, void* workspace,
                                int64_t ws_bytes, float* loss, float* ncc_out, float* grad_poses, int accumulate,
                                void* stream);
+/* Allocation-free form of fvr_tc_sncc_value_and_grad (no counterpart in the
+ * reference): same arguments and results, but the workspace is a fixed
+ * per-device scratch array inside the library (about 354 KB), so the call
+ * allocates nothing.  For callers that cannot allocate device memory where
+ * they call (a host linking only this C ABI, with no device allocator; a
+ * loop that must not enter an allocator between steps).
+ * Limits: C * nviews <= 512 and C * nviews * tiles <= 2048 partial records
+ * (tiles per (candidate, view) as the launch variant sizes them); larger
+ * calls return FVR_ERR_WORKSPACE without launching.
+ * The first call on a device (that device current) resolves the scratch
+ * address once; make it before any stream capture begins.  Nothing has to be
+ * zeroed by the caller: the scratch's ticket counters start at zero and each
+ * completed call leaves them zero.  All callers in the process share one
+ * scratch per device, so calls on one device must not overlap in time (use
+ * one stream or synchronise between them). */
+int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H,
+                                      int64_t W, const float* poses, int64_t C, int nviews, const int* views,
+                                      const void* const* ftargs, const float* hp, const float* lin, int64_t R,
+                                      double kappa, int variant, const float* g, int64_t g_stride, float* loss,
+                                      float* ncc_out, float* grad_poses, int accumulate, void* stream);
 /* Modulated slice S*exp(i phase) -> out[C][R][R] complex from fp64 axes;
  * shift != 0 writes it in ifftshift order (input of the image IFFT).
  * Replaces TorchDiffFVREngine._extract_slice_spectrum, torch_engine.py:176-234. */
