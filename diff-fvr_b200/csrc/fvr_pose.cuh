@@ -62,6 +62,20 @@ __device__ __forceinline__ Mat3 euler_R(double yaw, double pitch, double roll) {
   return mat_mul(rot_z(cz, sz), mat_mul(rot_y(cy, sy), rot_x(cx, sx)));
 }
 
+// R and dR/d(yaw, pitch, roll) (per radian) from one set of sines / cosines.
+__device__ __forceinline__ void euler_R_jac(double yaw, double pitch, double roll, Mat3* R, Mat3 dR[3]) {
+  double sz, cz, sy, cy, sx, cx;
+  sincos_deg(yaw, &sz, &cz);
+  sincos_deg(pitch, &sy, &cy);
+  sincos_deg(roll, &sx, &cx);
+  const Mat3 Z = rot_z(cz, sz), Y = rot_y(cy, sy), X = rot_x(cx, sx);
+  const Mat3 YX = mat_mul(Y, X);
+  *R = mat_mul(Z, YX);
+  dR[0] = mat_mul(drot_z(cz, sz), YX);
+  dR[1] = mat_mul(Z, mat_mul(drot_y(cy, sy), X));
+  dR[2] = mat_mul(Z, mat_mul(Y, drot_x(cx, sx)));
+}
+
 // d<G, R>/d(yaw, pitch, roll), per degree.
 __device__ __forceinline__ void euler_vjp(double yaw, double pitch, double roll, const Mat3& G, double out[3]) {
   double sz, cz, sy, cy, sx, cx;

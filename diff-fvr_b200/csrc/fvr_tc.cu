@@ -38,6 +38,34 @@ __device__ __forceinline__ void slice_axes(const float* p, int lateral, double s
   ax[7] = p[4];
 }
 
+// Slice axes (as slice_axes) and their Jacobian with respect to the pose
+// angles: jac[k][r][i] = d(R_total[r][i]) / d(angle k) per degree, k = yaw,
+// pitch, roll, rows r = 0 (u) and 1 (v), R_total = R (. Rz(90) for lateral).
+__device__ __forceinline__ void slice_axes_jac(const float* p, int lateral, double sx, double sy, double sz,
+                                               double* ax, double* jac) {
+  Mat3 R, dR[3];
+  euler_R_jac(p[0], p[1], p[2], &R, dR);
+  if (lateral) {
+    R = mat_mul(R, lateral_rot());
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dR[k] = mat_mul(dR[k], lateral_rot());
+  }
+  ax[0] = R.m[0][0] * sx;
+  ax[1] = R.m[0][1] * sy;
+  ax[2] = R.m[0][2] * sz;
+  ax[3] = R.m[1][0] * sx;
+  ax[4] = R.m[1][1] * sy;
+  ax[5] = R.m[1][2] * sz;
+  ax[6] = p[3];
+  ax[7] = p[4];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) jac[(k * 2 + r) * 3 + i] = dR[k].m[r][i] * kDeg;
+}
+
 __global__ void tc_axes_kernel(const float* __restrict__ poses, int C, int lateral, double sx, double sy, double sz,
                                double* __restrict__ axes) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -109,6 +137,7 @@ struct SnccArgs {
   // fused epilogue (value_and_grad launch) only
   unsigned* counters;  // [C + 1], zero on entry, left zero on exit
   double* mom;         // [nv][C][kMomStride]
+  double* jac;         // [nv][C][18]: slice-axes Jacobian per (view, candidate)
   float* loss;         // [nv + 1]
   float* ncc_out;      // [nv][C] or null
   float* grad;         // [C][6]
@@ -156,29 +185,22 @@ __device__ __forceinline__ int lateral_bits(const int (&lat)[kMaxViews]) {
   return (lat[0] & 1) | ((lat[1] & 1) << 1) | ((lat[2] & 1) << 2) | ((lat[3] & 1) << 3);
 }
 
-// Out-of-line form for the fused epilogue (one thread per candidate): keeps
-// its fp64 register demand out of the gather loop's allocation.
-__device__ __noinline__ void sncc_pose_grad_store(const double* mom, const float* p, int nv, int lat_bits,
-                                                  const float* g, int g_stride, int C, double sx, double sy,
-                                                  double sz, double kappa, float* o, int accumulate) {
-  float r[6];
-  sncc_pose_grad(mom, kMomStride, p, nv, lat_bits, g, g_stride, C, sx, sy, sz, kappa, r);
-  for (int k = 0; k < 6; ++k) o[k] = accumulate ? o[k] + r[k] : r[k];
-}
-
 __device__ __forceinline__ double sncc_ncc(const double* m) {
   return m[M_CROSS] / (sqrt(m[M_EP] * m[M_ET]) + 1e-8);
 }
 
-// CTA sum of per-thread partials; every cross-lane / cross-warp step in fp64
-// (the pose-gradient moments are small residuals of large cancelling sums).
+// CTA sum of per-thread partials; cross-lane in T, cross-warp in fp64 (the
+// pose-gradient moments are small residuals of large cancelling sums: each
+// lane holds a short run of samples, the long sums are fp64).
 template <int NV, typename T>
 __device__ __forceinline__ void block_reduce_d(T (&acc)[NV], double* red, double* out_m) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int m = 0; m < NV; ++m) {
-    const double v = warp_sum(static_cast<double>(acc[m]));
-    if (lane == 0) red[m * nw + wid] = v;
+    T t = acc[m];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) red[m * nw + wid] = static_cast<double>(t);
   }
   __syncthreads();
   if (threadIdx.x < NV) {
@@ -298,81 +320,107 @@ __device__ __forceinline__ void tab_decode(const Raw<DT>& r, Sample8& v) {
   }
 }
 
-template <int DT, bool DERIV>
-__device__ __forceinline__ void tab_scale(const Raw<DT>& r, Interp& o) {
-  if constexpr (DT == FVR_F16) {
-    o.sr *= r.sc;
-    o.si *= r.sc;
-    if (DERIV) {
-      o.dxr *= r.sc;
-      o.dxi *= r.sc;
-      o.dyr *= r.sc;
-      o.dyi *= r.sc;
-      o.dzr *= r.sc;
-      o.dzi *= r.sc;
-    }
-  }
+template <int DT>
+__device__ __forceinline__ float raw_scale(const Raw<DT>& r) {
+  if constexpr (DT == FVR_F16)
+    return r.sc;
+  else
+    return 1.f;
 }
 
+// Ticket protocol (as a grid barrier does it): the CTA barrier orders every
+// thread's stores before thread 0, whose fence publishes them at device scope
+// before it takes a ticket; the thread that takes a last ticket fences again
+// before its CTA reads the other CTAs' records (through L2).  The candidate
+// epilogue needs one round of loads (tile sums and the stored axes
+// Jacobians) and fp64 arithmetic in one thread; the losses one more round.
 __device__ __forceinline__ void sncc_fused_epilogue(const SnccArgs& a, int c) {
   __shared__ int s_last;
-  __shared__ double s_mom[kMaxViews * kMomStride];
+  __shared__ double s_mom[kMaxViews][kMomStride];
+  __shared__ double s_jac[kMaxViews][18];
   const int tiles = gridDim.x, nv = gridDim.z, C = a.C;
-  __threadfence();  // this CTA's partial stores before its ticket
   __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(a.counters + c, 1u) == static_cast<unsigned>(tiles * nv - 1);
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  // candidate c is complete: tile sums in fixed order
-  for (int t = threadIdx.x; t < nv * M_NGRAD; t += blockDim.x) {
-    const int v = t / M_NGRAD, m = t - v * M_NGRAD;
-    const double* src = a.partial + (static_cast<int64_t>(v) * C + c) * tiles * M_NGRAD + m;
-    double sum = 0.0;
-    for (int k = 0; k < tiles; ++k) sum += __ldcg(src + k * M_NGRAD);
-    s_mom[v * kMomStride + m] = sum;
-  }
-  __syncthreads();
-  if (threadIdx.x < nv) {
-    const int v = threadIdx.x;
-    const double n = sncc_ncc(s_mom + v * kMomStride);
-    s_mom[v * kMomStride + 17] = n;
-    if (a.ncc_out) a.ncc_out[v * C + c] = static_cast<float>(n);
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < nv * kMomStride; t += blockDim.x) {
-    const int v = t / kMomStride, m = t - v * kMomStride;
-    a.mom[(static_cast<int64_t>(v) * C + c) * kMomStride + m] = s_mom[t];
-  }
   if (threadIdx.x == 0) {
-    sncc_pose_grad_store(s_mom, a.poses + 6 * c, nv, lateral_bits(a.lateral), a.g, a.g_stride, C, a.sx, a.sy, a.sz,
-                         a.kappa, a.grad + 6 * c, a.accumulate);
-    a.counters[c] = 0u;  // every ticket of candidate c has been taken
+    __threadfence();
+    const bool last = atomicAdd(a.counters + c, 1u) == static_cast<unsigned>(tiles * nv - 1);
+    if (last) __threadfence();
+    s_last = last;
   }
-  // global ticket: the last candidate forms the losses
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(a.counters + C, 1u) == static_cast<unsigned>(C - 1);
   __syncthreads();
   if (!s_last) return;
-  __threadfence();
-  __shared__ double s_red[kSnccThreads / 32];
+  // candidate c is complete: tile sums (fixed order) and Jacobians in one round
+  for (int t = threadIdx.x; t < nv * (M_NGRAD + 18); t += blockDim.x) {
+    if (t < nv * M_NGRAD) {
+      const int v = t / M_NGRAD, m = t - v * M_NGRAD;
+      const double* src = a.partial + (static_cast<int64_t>(v) * C + c) * tiles * M_NGRAD + m;
+      double sum = 0.0;
+      for (int k0 = 0; k0 < tiles; k0 += 4) {  // four independent loads in flight
+        double x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = k0 + u < tiles ? __ldcg(src + (k0 + u) * M_NGRAD) : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) sum += x[u];
+      }
+      s_mom[v][m] = sum;
+    } else {
+      const int k = t - nv * M_NGRAD, v = k / 18;
+      s_jac[v][k - v * 18] = __ldcg(a.jac + (static_cast<int64_t>(v) * C + c) * 18 + (k - v * 18));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // ncc per view and dL/dpose: per axis gc (a A + 2 b B) through the Jacobian
+    double ga[3] = {0.0, 0.0, 0.0}, gtx = 0.0, gty = 0.0;
+    const double s3[3] = {a.sx, a.sy, a.sz};
+    for (int v = 0; v < nv; ++v) {
+      double* m = s_mom[v];
+      const double sq = sqrt(m[M_EP] * m[M_ET]);
+      const double inv = 1.0 / (sq + 1e-8);
+      m[17] = m[M_CROSS] * inv;
+      const double bb = sq > 0.0 ? -0.5 * m[M_CROSS] * m[M_ET] * inv * inv / sq : 0.0;
+      const double gc = -(a.g ? static_cast<double>(a.g[v * a.g_stride]) : 1.0) / C;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double du = gc * (inv * m[M_AU + i] + 2.0 * bb * m[M_BU + i]) * s3[i];
+        const double dv = gc * (inv * m[M_AV + i] + 2.0 * bb * m[M_BV + i]) * s3[i];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ga[k] += du * s_jac[v][(k * 2 + 0) * 3 + i] + dv * s_jac[v][(k * 2 + 1) * 3 + i];
+      }
+      gtx += gc * inv * a.kappa * m[M_PHU];
+      gty += gc * inv * a.kappa * m[M_PHV];
+      if (a.ncc_out) a.ncc_out[v * C + c] = static_cast<float>(m[17]);
+      double* out = a.mom + (static_cast<int64_t>(v) * C + c) * kMomStride;
+      for (int k = 0; k < kMomStride; ++k) out[k] = m[k];
+    }
+    float* o = a.grad + 6 * c;
+    const float r[6] = {static_cast<float>(ga[0]), static_cast<float>(ga[1]), static_cast<float>(ga[2]),
+                        static_cast<float>(gtx), static_cast<float>(gty), 0.f};
+    for (int k = 0; k < 6; ++k) o[k] = a.accumulate ? o[k] + r[k] : r[k];
+    a.counters[c] = 0u;  // every ticket of candidate c has been taken
+    // global ticket: the CTA that completes the last candidate forms the losses
+    __threadfence();
+    const bool last = atomicAdd(a.counters + C, 1u) == static_cast<unsigned>(C - 1);
+    if (last) __threadfence();
+    s_last = last;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x >= 32) return;
+  // one warp: loss[v] = 1 - mean_c ncc (fixed lane order), loss[nv] = their sum;
+  // every view's loads are issued before any sum
+  double part[kMaxViews] = {0.0, 0.0, 0.0, 0.0};
+  for (int k = threadIdx.x; k < C; k += 32) {
+#pragma unroll
+    for (int v = 0; v < kMaxViews; ++v)
+      if (v < nv) part[v] += __ldcg(a.mom + (static_cast<int64_t>(v) * C + k) * kMomStride + 17);
+  }
   double total = 0.0;
-  for (int v = 0; v < nv; ++v) {
-    double sum = 0.0;
-    for (int k = threadIdx.x; k < C; k += blockDim.x)
-      sum += __ldcg(a.mom + (static_cast<int64_t>(v) * C + k) * kMomStride + 17);
-    sum = warp_sum(sum);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += s_red[w];
-      const double l = 1.0 - t / C;
-      a.loss[v] = static_cast<float>(l);
+#pragma unroll
+  for (int v = 0; v < kMaxViews; ++v) {
+    if (v < nv) {
+      const double l = 1.0 - warp_sum(part[v]) / C;
+      if (threadIdx.x == 0) a.loss[v] = static_cast<float>(l);
       total += l;
     }
-    __syncthreads();
   }
   if (threadIdx.x == 0) {
     a.loss[nv] = static_cast<float>(total);
@@ -399,7 +447,16 @@ __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(Snc
   const int q_end = min(q_begin + a.tile, K);
   const int row0 = q_begin / R;
   const AxisTables tab = axis_tables(tab_smem, R + a.tab_rows);
-  if (threadIdx.x == 0) slice_axes(a.poses + 6 * c, lateral, a.sx, a.sy, a.sz, ax_s);
+  if (threadIdx.x == 0) {
+    if (FUSE && GRAD) {
+      double jac[18];
+      slice_axes_jac(a.poses + 6 * c, lateral, a.sx, a.sy, a.sz, ax_s, jac);
+      if (tile == 0)  // one CTA per (view, candidate) stores the axes Jacobian for the epilogue
+        for (int k = 0; k < 18; ++k) a.jac[(static_cast<int64_t>(v) * a.C + c) * 18 + k] = jac[k];
+    } else {
+      slice_axes(a.poses + 6 * c, lateral, a.sx, a.sy, a.sz, ax_s);
+    }
+  }
   __syncthreads();
   build_axis_tables(tab, R, row0, (q_end - 1) / R - row0 + 1, a.lin, ax_s, a.sx, a.sy, a.sz, a.kpi);
   __syncthreads();
@@ -449,8 +506,9 @@ __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(Snc
       tab_decode<DT>(raw[g], sm);
       Interp o;
       trilerp<GRAD>(sm, tx, ty, tz, o);
-      tab_scale<DT, GRAD>(raw[g], o);
-      const float ku = fa.w, kv = fb.w, h = hs[g];
+      // f16: the brick scale rides on the high-pass weight (every moment is
+      // linear in h S or quadratic in it) instead of rescaling 8 values
+      const float ku = fa.w, kv = fb.w, h = DT == FVR_F16 ? hs[g] * raw_scale(raw[g]) : hs[g];
       const float cs = pa.x * pb.x - pa.y * pb.y, sn = pa.y * pb.x + pa.x * pb.y;
       const float2 T = Ts[g];
       const float shr = h * (o.sr * cs - o.si * sn);
@@ -759,17 +817,17 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
 // an allocator between steps (cudaMalloc / cudaFree may synchronise the
 // device).
 //
-// Size (about 354 KB per device): kStaticRecords partial-moment records of
-// 17 doubles, kStaticItems (candidate, view) moment records of 18 doubles and
-// kStaticItems + 1 ticket counters.  Calls needing more -- more than 512
-// (candidate, view) pairs, or more than 2048 (candidate, view, tile) partial
-// records for the launch variant -- are refused with FVR_ERR_WORKSPACE before
-// anything is launched.
+// Size (about 428 KB per device): kStaticRecords partial-moment records of
+// 17 doubles, kStaticItems (candidate, view) moment records and axes
+// Jacobians of 18 doubles each, and kStaticItems + 1 ticket counters.  Calls
+// needing more -- more than 512 (candidate, view) pairs, or more than 2048
+// (candidate, view, tile) partial records for the launch variant -- are
+// refused with FVR_ERR_WORKSPACE before anything is launched.
 //
 // Start state: the ticket counters must be zero before a launch; the static
 // initialiser zeroes them and every completed launch leaves them zero.  The
-// partial and moment records are fully written by every launch, so nothing
-// else needs to start at zero.
+// partial, moment and Jacobian records are written by every launch before
+// they are read, so nothing else needs to start at zero.
 //
 // Set-up: the first call on each device, made with that device current,
 // resolves the array's device address with cudaGetSymbolAddress and caches
@@ -784,8 +842,10 @@ constexpr int64_t kStaticItems = 512;
 constexpr int64_t kStaticRecords = 2048;
 constexpr int64_t kStaticPartialDoubles = kStaticRecords * M_NGRAD;
 constexpr int64_t kStaticMomDoubles = kStaticItems * kMomStride;
+constexpr int64_t kStaticJacDoubles = kStaticItems * 18;
 constexpr int64_t kStaticTicketDoubles = (kStaticItems + 1 + 1) / 2;  // unsigned counters, two per double
-constexpr int64_t kStaticDoubles = kStaticPartialDoubles + kStaticMomDoubles + kStaticTicketDoubles;
+constexpr int64_t kStaticDoubles = kStaticPartialDoubles + kStaticMomDoubles + kStaticJacDoubles +
+                                   kStaticTicketDoubles;
 constexpr int kStaticMaxDevices = 64;
 
 static __device__ __align__(256) double g_sncc_static_scratch[kStaticDoubles];
@@ -862,9 +922,11 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
   return FVR_OK;
 }
 
+// Fused workspace: partial records | moments [nv][C][18] | axes Jacobians
+// [nv][C][18] | tickets [C + 1] (the last region must start zeroed).
 int64_t fvr_tc_sncc_fused_workspace(int64_t C, int64_t R, int64_t nviews) {
   if (C < 1 || R < 1 || nviews < 1) return 0;
-  return fvr_tc_sncc_workspace(C, R, nviews) + nviews * C * kMomStride * (int64_t)sizeof(double) +
+  return fvr_tc_sncc_workspace(C, R, nviews) + 2 * nviews * C * kMomStride * (int64_t)sizeof(double) +
          cdiv64((C + 1) * (int64_t)sizeof(unsigned), 256) * 256;
 }
 
@@ -885,9 +947,10 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
   if (ws_bytes < fvr_tc_sncc_fused_workspace(C, R, nviews)) return FVR_ERR_WORKSPACE;
   char* ws = static_cast<char*>(workspace);
   a.partial = reinterpret_cast<double*>(ws);
+  const int64_t mom_bytes = nviews * C * kMomStride * (int64_t)sizeof(double);
   a.mom = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews));
-  a.counters = reinterpret_cast<unsigned*>(ws + fvr_tc_sncc_workspace(C, R, nviews) +
-                                           nviews * C * kMomStride * (int64_t)sizeof(double));
+  a.jac = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews) + mom_bytes);
+  a.counters = reinterpret_cast<unsigned*>(ws + fvr_tc_sncc_workspace(C, R, nviews) + 2 * mom_bytes);
   a.loss = loss;
   a.ncc_out = ncc_out;
   a.grad = grad_poses;
@@ -1018,7 +1081,8 @@ int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const floa
   if (rc) return rc;
   a.partial = scratch;
   a.mom = scratch + kStaticPartialDoubles;
-  a.counters = reinterpret_cast<unsigned*>(scratch + kStaticPartialDoubles + kStaticMomDoubles);
+  a.jac = scratch + kStaticPartialDoubles + kStaticMomDoubles;
+  a.counters = reinterpret_cast<unsigned*>(scratch + kStaticPartialDoubles + kStaticMomDoubles + kStaticJacDoubles);
   a.loss = loss;
   a.ncc_out = ncc_out;
   a.grad = grad_poses;
