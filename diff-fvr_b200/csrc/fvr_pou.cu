@@ -15,6 +15,7 @@
 // and the adjoint chain warp -> IFFT -> slice -> pose.
 #include "fvr_pose.cuh"
 #include "fvr_stencil.cuh"
+#include "fvr_wfft.cuh"
 
 namespace fvr {
 
@@ -278,6 +279,211 @@ __global__ void __launch_bounds__(256) pou_slice_adjoint_kernel(PouSliceArgs a, 
     partial[((static_cast<int64_t>(n) * gridDim.z + b) * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = s;
   }
 }
+// ----------------------------------------------------------------------------
+// fused block image: slice + 2D inverse FFT in shared memory (forward), and
+// 2D FFT + slice adjoint (backward), one CTA per (pose, block), P = 32 M.
+// ----------------------------------------------------------------------------
+constexpr int kPouImgThreads = 512;
+
+// Row / column split-position tables of one (pose, block) image: entry j < P
+// is the column part fx_j u, entry P + i the row part c + fy_i v (fp64, split
+// into integer cell and float fraction; .w = the frequency).
+__device__ __forceinline__ void pou_image_tables(const AxisTables& t, const PouSliceArgs& a, const double* g) {
+  for (int e = threadIdx.x; e < 2 * a.P; e += blockDim.x) {
+    const bool col = e < a.P;
+    const float kf = __ldg(a.freqs + (col ? e : e - a.P));
+    const double k = kf;
+    const double px = col ? k * g[12] : fma(k, g[15], a.c);
+    const double py = col ? k * g[13] : fma(k, g[16], a.c);
+    const double pz = col ? k * g[14] : fma(k, g[17], a.c);
+    const double fx = floor(px), fy = floor(py), fz = floor(pz);
+    t.idx[e] = make_int4(static_cast<int>(fx), static_cast<int>(fy), static_cast<int>(fz), 0);
+    t.frac[e] = make_float4(static_cast<float>(px - fx), static_cast<float>(py - fy), static_cast<float>(pz - fz), kf);
+  }
+}
+
+template <int DT, bool DERIV>
+__device__ __forceinline__ void pou_table_sample(const Stencil& st, const Raw<DT>& raw, const float4& fa,
+                                                 const float4& fb, Interp& o) {
+  float tx = fa.x + fb.x, ty = fa.y + fb.y, tz = fa.z + fb.z;
+  if (tx >= 1.f) tx -= 1.f;
+  if (ty >= 1.f) ty -= 1.f;
+  if (tz >= 1.f) tz -= 1.f;
+  Sample8 sm;
+  tab_decode<DT>(raw, sm);
+  trilerp<DERIV>(sm, tx, ty, tz, o);
+  const float sc = raw_scale(raw);
+  if (DT == FVR_F16) {
+    o.sr *= sc;
+    o.si *= sc;
+    if (DERIV) {
+      o.dxr *= sc;
+      o.dxi *= sc;
+      o.dyr *= sc;
+      o.dyi *= sc;
+      o.dzr *= sc;
+      o.dzi *= sc;
+    }
+  }
+}
+
+// Smem layout of the fused image kernels: the P x (P + 1) complex image, then
+// the 2P-entry tables.
+__host__ __device__ constexpr int64_t pou_image_smem(int P) {
+  return static_cast<int64_t>(P) * (P + 1) * 8 + 40 * 2 * static_cast<int64_t>(P) + 16;
+}
+
+// imgs[b][n] = Re fftshift(ifft2(ifftshift(S))) for the slice S of block b at
+// pose n (the reference's _slice_and_ifft, cone_beam_fvr.py:480-505).
+template <int DT, int M>
+__global__ void __launch_bounds__(kPouImgThreads, 1) pou_slice_ifft_kernel(PouSliceArgs a, float* __restrict__ imgs) {
+  constexpr int P = 32 * M, PITCH = P + 1, H = P / 2, NW = kPouImgThreads / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem);
+  const AxisTables tab = axis_tables(smem + ((static_cast<int64_t>(P) * PITCH * 8 + 15) / 16) * 16, 2 * P);
+  const int n = blockIdx.x, b = blockIdx.y;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const Stencil st = pou_block_stencil(a, b);
+  pou_image_tables(tab, a, a.geo + n * kGeo);
+  WarpFft<M, true> fft;
+  fft.init(lane);
+  __syncthreads();
+  // rows: gather the ifftshift-ordered slice row straight into registers
+  for (int r = wid; r < P; r += NW) {
+    const int i = r + H < P ? r + H : r - H;
+    const int4 ia = tab.idx[P + i];
+    const float4 fa = tab.frac[P + i];
+    Raw<DT> raw[M];
+    int jj[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int c = lane + 32 * m;
+      jj[m] = c + H < P ? c + H : c - H;
+      const TabCell cell = tab_cell(st, ia, fa, tab.idx[jj[m]], tab.frac[jj[m]]);
+      tab_load<DT>(st, cell, raw[m]);
+    }
+    Cx<float> x[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      Interp o;
+      pou_table_sample<DT, false>(st, raw[m], fa, tab.frac[jj[m]], o);
+      x[m] = Cx<float>{o.sr, o.si};
+    }
+    fft.run(x, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) buf[r * PITCH + lane + 32 * k] = x[k];
+  }
+  __syncthreads();
+  // columns, in place (each warp owns whole columns)
+  for (int cc = wid; cc < P; cc += NW) {
+    Cx<float> x[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) x[m] = buf[(lane + 32 * m) * PITCH + cc];
+    fft.run(x, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + cc] = x[k];
+  }
+  __syncthreads();
+  // fftshift-ordered real part, coalesced rows
+  const float scale = 1.f / static_cast<float>(P * P);
+  float* out = imgs + (static_cast<int64_t>(b) * a.N + n) * P * P;
+  for (int q = threadIdx.x; q < P * P; q += kPouImgThreads) {
+    const int y = q / P, xq = q - y * P;
+    const int ky = y + H < P ? y + H : y - H, kx = xq + H < P ? xq + H : xq - H;
+    out[q] = buf[wfft_pos<M>(ky) * PITCH + wfft_pos<M>(kx)].x * scale;
+  }
+}
+
+// Adjoint of pou_slice_ifft_kernel for one (pose, block): G = fftshift(fft2(
+// ifftshift(g))) / P^2 in shared memory, then per slice sample the products
+// of G with the spectrum's spatial derivatives, weighted by fx and fy:
+// partial[n][b][6] = sum (fx <G, dS/dp_k>, fy <G, dS/dp_k>), k = x, y, z.
+template <int DT, int M>
+__global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kernel(PouSliceArgs a,
+                                                                                  const float* __restrict__ gimg,
+                                                                                  double* __restrict__ partial) {
+  constexpr int P = 32 * M, PITCH = P + 1, H = P / 2, NW = kPouImgThreads / 32, GROUP = 4;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double red[6 * NW];
+  Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem);
+  const AxisTables tab = axis_tables(smem + ((static_cast<int64_t>(P) * PITCH * 8 + 15) / 16) * 16, 2 * P);
+  const int n = blockIdx.x, b = blockIdx.y;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const Stencil st = pou_block_stencil(a, b);
+  pou_image_tables(tab, a, a.geo + n * kGeo);
+  WarpFft<M, false> fft;
+  fft.init(lane);
+  const float* g = gimg + (static_cast<int64_t>(b) * a.N + n) * P * P;
+  for (int r = wid; r < P; r += NW) {
+    const int y = r + H < P ? r + H : r - H;
+    Cx<float> x[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int c = lane + 32 * m;
+      x[m] = Cx<float>{__ldg(g + y * P + (c + H < P ? c + H : c - H)), 0.f};
+    }
+    fft.run(x, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) buf[r * PITCH + lane + 32 * k] = x[k];
+  }
+  __syncthreads();
+  for (int cc = wid; cc < P; cc += NW) {
+    Cx<float> x[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) x[m] = buf[(lane + 32 * m) * PITCH + cc];
+    fft.run(x, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + cc] = x[k];
+  }
+  __syncthreads();
+  const float scale = 1.f / static_cast<float>(P * P);
+  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int q0 = threadIdx.x; q0 < P * P; q0 += kPouImgThreads * GROUP) {
+    Raw<DT> raw[GROUP];
+    int qq[GROUP];
+#pragma unroll
+    for (int u = 0; u < GROUP; ++u) {
+      const int q = q0 + u * kPouImgThreads;
+      qq[u] = q;
+      const int i = q < P * P ? q / P : 0, j = q < P * P ? q - (q / P) * P : 0;
+      TabCell cell = tab_cell(st, tab.idx[P + i], tab.frac[P + i], tab.idx[j], tab.frac[j]);
+      if (q >= P * P) cell.e = -1;
+      tab_load<DT>(st, cell, raw[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < GROUP; ++u) {
+      const int q = qq[u];
+      if (q >= P * P) continue;
+      const int i = q / P, j = q - i * P;
+      const float4 fa = tab.frac[P + i], fb = tab.frac[j];
+      Interp o;
+      pou_table_sample<DT, true>(st, raw[u], fa, fb, o);
+      const int ki = i + H < P ? i + H : i - H, kj = j + H < P ? j + H : j - H;
+      const Cx<float> G = buf[wfft_pos<M>(ki) * PITCH + wfft_pos<M>(kj)];
+      const float gx = G.x * scale, gy = G.y * scale;
+      const float e0 = gx * o.dxr + gy * o.dxi, e1 = gx * o.dyr + gy * o.dyi, e2 = gx * o.dzr + gy * o.dzi;
+      const float fx = fb.w, fy = fa.w;
+      acc[0] = fmaf(fx, e0, acc[0]);
+      acc[1] = fmaf(fx, e1, acc[1]);
+      acc[2] = fmaf(fx, e2, acc[2]);
+      acc[3] = fmaf(fy, e0, acc[3]);
+      acc[4] = fmaf(fy, e1, acc[4]);
+      acc[5] = fmaf(fy, e2, acc[5]);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const double v = warp_sum(static_cast<double>(acc[m]));
+    if (lane == 0) red[m * NW + wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double sum = 0.0;
+    for (int w = 0; w < NW; ++w) sum += red[threadIdx.x * NW + w];
+    partial[(static_cast<int64_t>(n) * gridDim.y + b) * 6 + threadIdx.x] = sum;
+  }
+}
+
 
 // ----------------------------------------------------------------------------
 // pinhole warp + sum  (triton_slice.py:348-407 / 409-496)
@@ -296,16 +502,58 @@ struct WarpArgs {
   int64_t ray_stride;
 };
 
+// Block culling for a CTA of detector pixels: the box of its live pixels'
+// ray coordinates (rx, ry), then per block whether any of those pixels can
+// sample inside the block image.  The image coordinate is the same monotone
+// fp64 expression of rx (or ry) that the sampling uses, evaluated at the box
+// corners, so a block is skipped only if no pixel would have sampled it.
+template <typename OT>
+__device__ __forceinline__ void warp_cull(const WarpArgs<OT>& a, int n, bool live, double rx, double ry,
+                                          unsigned char* touch) {
+  __shared__ double s_box[4][8];
+  __shared__ double box[4];
+  const double inf = 1e300;
+  double v[4] = {live ? rx : inf, live ? -rx : inf, live ? ry : inf, live ? -ry : inf};  // mins of +-r
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] = fmin(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+    if ((threadIdx.x & 31) == 0) s_box[k][threadIdx.x >> 5] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double m = inf;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) m = fmin(m, s_box[threadIdx.x][w]);
+    box[threadIdx.x] = m;
+  }
+  __syncthreads();
+  const bool any = box[0] < inf;
+  for (int b = threadIdx.x; b < a.B; b += blockDim.x) {
+    const int64_t bn = static_cast<int64_t>(b) * a.N + n;
+    const double db = static_cast<double>(a.db[bn * a.ostride]);
+    const double cu = static_cast<double>(a.cu[bn * a.ostride]), cv = static_cast<double>(a.cv[bn * a.ostride]);
+    const double x0 = (db * box[0] - cu) * a.inv_ds + a.c_idx, x1 = (db * -box[1] - cu) * a.inv_ds + a.c_idx;
+    const double y0 = (db * box[2] - cv) * a.inv_ds + a.c_idx, y1 = (db * -box[3] - cv) * a.inv_ds + a.c_idx;
+    const double P = static_cast<double>(a.P);
+    touch[b] = any && fmax(x0, x1) > -1.0 && fmin(x0, x1) < P && fmax(y0, y1) > -1.0 && fmin(y0, y1) < P;
+  }
+  __syncthreads();
+}
+
 template <typename OT>
 __global__ void __launch_bounds__(256) pou_warp_kernel(WarpArgs<OT> a, float* __restrict__ out) {
+  extern __shared__ unsigned char touch[];  // [B]
   const int n = blockIdx.y;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= a.K) return;
+  const bool live = q < a.K;
   const int64_t rq = n * a.ray_stride + q;
-  const double rx = __ldg(a.rx + rq), ry = __ldg(a.ry + rq);
+  const double rx = live ? __ldg(a.rx + rq) : 0.0, ry = live ? __ldg(a.ry + rq) : 0.0;
+  warp_cull(a, n, live, rx, ry, touch);
+  if (!live) return;
   const int P = a.P;
   float acc = 0.f;
   for (int b = 0; b < a.B; ++b) {
+    if (!touch[b]) continue;
     const int64_t bn = static_cast<int64_t>(b) * a.N + n;
     const double db = static_cast<double>(a.db[bn * a.ostride]);
     const double px = (db * rx - static_cast<double>(a.cu[bn * a.ostride])) * a.inv_ds + a.c_idx;
@@ -333,26 +581,30 @@ __global__ void __launch_bounds__(256) pou_warp_bwd_kernel(WarpArgs<OT> a, const
                                                            float* __restrict__ grad_imgs,
                                                            double* __restrict__ partial,
                                                            float* __restrict__ gray) {
-  extern __shared__ double sacc[];  // [B][3]
+  extern __shared__ double sacc[];  // [B][3], then touch[B]
+  unsigned char* touch = reinterpret_cast<unsigned char*>(sacc + 3 * a.B);
   const int n = blockIdx.y;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   for (int i = threadIdx.x; i < 3 * a.B; i += blockDim.x) sacc[i] = 0.0;
-  __syncthreads();
   const bool live = q < a.K;
   const int64_t rq = n * a.ray_stride + q;
   const double rx = live ? __ldg(a.rx + rq) : 0.0, ry = live ? __ldg(a.ry + rq) : 0.0;
+  warp_cull(a, n, live, rx, ry, touch);
   const float g = live ? __ldg(gout + static_cast<int64_t>(n) * a.K + q) * __ldg(a.ic + rq) : 0.f;
   const int P = a.P;
   const float inv_ds = static_cast<float>(a.inv_ds);
   float grx = 0.f, gry = 0.f, ssum = 0.f;  // explicit rays: dL/drx, dL/dry, sum_b sample
   for (int b = 0; b < a.B; ++b) {
+    if (!touch[b]) continue;  // no pixel of this CTA samples block b
     const int64_t bn = static_cast<int64_t>(b) * a.N + n;
     float gdb = 0.f, gcu = 0.f, gcv = 0.f;
+    bool hit = false;
     if (live) {
       const double db = static_cast<double>(a.db[bn * a.ostride]);
       const double px = (db * rx - static_cast<double>(a.cu[bn * a.ostride])) * a.inv_ds + a.c_idx;
       const double py = (db * ry - static_cast<double>(a.cv[bn * a.ostride])) * a.inv_ds + a.c_idx;
       if (px > -1.0 && px < static_cast<double>(P) && py > -1.0 && py < static_cast<double>(P)) {
+        hit = true;
         const double fx = floor(px), fy = floor(py);
         const int ix = static_cast<int>(fx), iy = static_cast<int>(fy);
         const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
@@ -382,6 +634,7 @@ __global__ void __launch_bounds__(256) pou_warp_bwd_kernel(WarpArgs<OT> a, const
         }
       }
     }
+    if (!__any_sync(0xffffffffu, hit)) continue;  // nothing to add from this warp
     const double s0 = warp_sum(static_cast<double>(gdb)), s1 = warp_sum(static_cast<double>(gcu)),
                  s2 = warp_sum(static_cast<double>(gcv));
     if ((threadIdx.x & 31) == 0) {
@@ -471,54 +724,74 @@ __global__ void pou_warp_bwd_finalize_kernel(const double* __restrict__ partial,
 // goffs[3][B][N] and (explicit rays) per-(pose, tile) partials [N][rtiles][12]
 // -> dL/d(src, u, v, n) [N][12] (gvec) and / or dL/dmats [N][4][4]
 // (cone_beam_fvr.py:485-521, 676-682)
-__global__ void pou_pose_bwd_kernel(const double* __restrict__ sl_part, int tiles, const double* __restrict__ goffs,
-                                    const double* __restrict__ ray_part, int rtiles, const double* __restrict__ geo,
-                                    const float* __restrict__ centers, int B, int N, PouBase base, double vscale,
-                                    float* __restrict__ gmats, float* __restrict__ gvec) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  double gux[3] = {0, 0, 0}, gvx[3] = {0, 0, 0};
-  for (int b = 0; b < B; ++b)
-    for (int t = 0; t < tiles; ++t) {
-      const double* p = sl_part + ((static_cast<int64_t>(n) * B + b) * tiles + t) * 6;
-      for (int k = 0; k < 3; ++k) {
-        gux[k] += p[k];
-        gvx[k] += p[3 + k];
-      }
-    }
+// dL/d(pose) for one pose per CTA: the slice-adjoint partials over all
+// (block, tile) records, the block-offset gradients and the explicit-ray
+// partials are summed in parallel (fixed thread strides, fp64 tree), then
+// mapped onto the source / detector axes and the pose matrix.
+__global__ void __launch_bounds__(256) pou_pose_bwd_kernel(const double* __restrict__ sl_part, int tiles,
+                                                           const double* __restrict__ goffs,
+                                                           const double* __restrict__ ray_part, int rtiles,
+                                                           const double* __restrict__ geo,
+                                                           const float* __restrict__ centers, int B, int N,
+                                                           PouBase base, double vscale, float* __restrict__ gmats,
+                                                           float* __restrict__ gvec) {
+  constexpr int NA = 18;  // gux[3], gvx[3], gs[3], gu[3], gv[3], gn[3]
+  __shared__ double red[NA * 8];
+  const int n = blockIdx.x;
   const double* g = geo + n * kGeo;
   const double s[3] = {g[0], g[1], g[2]}, u[3] = {g[3], g[4], g[5]}, v[3] = {g[6], g[7], g[8]},
                nn[3] = {g[9], g[10], g[11]};
-  // u_xyz = flip(u) * vscale
-  double gu[3], gv[3], gn[3] = {0, 0, 0}, gs[3] = {0, 0, 0};
-  for (int k = 0; k < 3; ++k) {
-    gu[k] = gux[2 - k] * vscale;
-    gv[k] = gvx[2 - k] * vscale;
+  double acc[NA];
+#pragma unroll
+  for (int k = 0; k < NA; ++k) acc[k] = 0.0;
+  const int64_t nrec = static_cast<int64_t>(B) * tiles;
+  for (int64_t r = threadIdx.x; r < nrec; r += blockDim.x) {
+    const double* p = sl_part + (static_cast<int64_t>(n) * nrec + r) * 6;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc[k] += p[k];
   }
   if (goffs) {
-    for (int b = 0; b < B; ++b) {
+    for (int b = threadIdx.x; b < B; b += blockDim.x) {
       const double gdb = goffs[(0 * static_cast<int64_t>(B) + b) * N + n];
       const double gcu = goffs[(1 * static_cast<int64_t>(B) + b) * N + n];
       const double gcv = goffs[(2 * static_cast<int64_t>(B) + b) * N + n];
+#pragma unroll
       for (int k = 0; k < 3; ++k) {
         const double d = static_cast<double>(centers[3 * b + k]) - s[k];
-        gn[k] += gdb * d;
-        gu[k] += gcu * d;
-        gv[k] += gcv * d;
-        gs[k] -= gdb * nn[k] + gcu * u[k] + gcv * v[k];
+        acc[15 + k] += gdb * d;
+        acc[9 + k] += gcu * d;
+        acc[12 + k] += gcv * d;
+        acc[6 + k] -= gdb * nn[k] + gcu * u[k] + gcv * v[k];
       }
     }
   }
   if (ray_part) {
-    for (int t = 0; t < rtiles; ++t) {
+    for (int t = threadIdx.x; t < rtiles; t += blockDim.x) {
       const double* p = ray_part + (static_cast<int64_t>(n) * rtiles + t) * 12;
-      for (int k = 0; k < 3; ++k) {
-        gs[k] += p[k];
-        gu[k] += p[3 + k];
-        gv[k] += p[6 + k];
-        gn[k] += p[9 + k];
-      }
+#pragma unroll
+      for (int k = 0; k < 12; ++k) acc[6 + k] += p[k];
     }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NA; ++k) {
+    const double t = warp_sum(acc[k]);
+    if (lane == 0) red[k * 8 + wid] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double tot[NA];
+  for (int k = 0; k < NA; ++k) {
+    tot[k] = 0.0;
+    for (int w = 0; w < nw; ++w) tot[k] += red[k * 8 + w];
+  }
+  // u_xyz = flip(u) * vscale
+  double gs[3], gu[3], gv[3], gn[3];
+  for (int k = 0; k < 3; ++k) {
+    gs[k] = tot[6 + k];
+    gu[k] = tot[9 + k] + tot[2 - k] * vscale;
+    gv[k] = tot[12 + k] + tot[3 + 2 - k] * vscale;
+    gn[k] = tot[15 + k];
   }
   if (gvec) {
     float* o = gvec + 12 * n;
@@ -564,6 +837,65 @@ static PouBase make_base(const double* base12) {
 }  // namespace fvr
 
 using namespace fvr;
+
+template <int DT, int M>
+static int pou_image_launch(bool adjoint, const PouSliceArgs& a, int B, const float* gimg, float* imgs,
+                            double* part, cudaStream_t s) {
+  const int64_t smem = pou_image_smem(32 * M);
+  dim3 grid(static_cast<unsigned>(a.N), static_cast<unsigned>(B));
+  if (adjoint) {
+    static bool attr = false;
+    if (!attr) {
+      if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)) != cudaSuccess)
+        return FVR_ERR_CUDA;
+      attr = true;
+    }
+    pou_fft_slice_adjoint_kernel<DT, M><<<grid, kPouImgThreads, smem, s>>>(a, gimg, part);
+  } else {
+    static bool attr = false;
+    if (!attr) {
+      if (cudaFuncSetAttribute(pou_slice_ifft_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)) != cudaSuccess)
+        return FVR_ERR_CUDA;
+      attr = true;
+    }
+    pou_slice_ifft_kernel<DT, M><<<grid, kPouImgThreads, smem, s>>>(a, imgs);
+  }
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+template <int DT>
+static int pou_image_dispatch(bool adjoint, const PouSliceArgs& a, int B, const float* gimg, float* imgs,
+                              double* part, cudaStream_t s) {
+  switch (a.P) {
+    case 64: return pou_image_launch<DT, 2>(adjoint, a, B, gimg, imgs, part, s);
+    case 96: return pou_image_launch<DT, 3>(adjoint, a, B, gimg, imgs, part, s);
+    case 128: return pou_image_launch<DT, 4>(adjoint, a, B, gimg, imgs, part, s);
+    case 160: return pou_image_launch<DT, 5>(adjoint, a, B, gimg, imgs, part, s);
+  }
+  return FVR_ERR_UNSUPPORTED;
+}
+
+static int pou_image_common(bool adjoint, int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
+                            const double* geo, int64_t N, const float* freqs, const float* gimg, float* imgs,
+                            double* part, void* stream) {
+  Stencil st;
+  int rc = pou_stencil(dtype, stencil, scales, P, &st);
+  if (rc) return rc;
+  if (!geo || !freqs || B < 1 || N < 1 || B > 65535 || N > 2147483647) return FVR_ERR_ARG;
+  if (!(P == 64 || P == 96 || P == 128 || P == 160)) return FVR_ERR_UNSUPPORTED;
+  PouSliceArgs a{st, fvr_stencil_bytes(P, P, P, dtype), fvr_stencil_scale_count(P, P, P), geo, freqs, (int)P, (int)N,
+                 static_cast<double>(P / 2)};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  switch (dtype) {
+    case FVR_F32: return pou_image_dispatch<FVR_F32>(adjoint, a, (int)B, gimg, imgs, part, s);
+    case FVR_BF16: return pou_image_dispatch<FVR_BF16>(adjoint, a, (int)B, gimg, imgs, part, s);
+    case FVR_F16: return pou_image_dispatch<FVR_F16>(adjoint, a, (int)B, gimg, imgs, part, s);
+  }
+  return FVR_ERR_DTYPE;
+}
 
 extern "C" {
 
@@ -664,6 +996,25 @@ int fvr_pou_slice_adjoint(int dtype, const void* stencil, const float* scales, i
   return FVR_OK;
 }
 
+int fvr_pou_image_supported(int64_t P) { return (P == 64 || P == 96 || P == 128 || P == 160) ? 1 : 0; }
+
+int fvr_pou_slice_image(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P, const double* geo,
+                        int64_t N, const float* freqs, float* imgs, void* stream) {
+  if (!imgs) return FVR_ERR_ARG;
+  return pou_image_common(false, dtype, stencil, scales, B, P, geo, N, freqs, nullptr, imgs, nullptr, stream);
+}
+
+int64_t fvr_pou_slice_image_adjoint_workspace(int64_t B, int64_t N) { return N * B * 6 * (int64_t)sizeof(double); }
+
+int fvr_pou_slice_image_adjoint(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
+                                const double* geo, int64_t N, const float* freqs, const float* grad_imgs,
+                                void* workspace, int64_t ws_bytes, void* stream) {
+  if (!grad_imgs || !workspace) return FVR_ERR_ARG;
+  if (ws_bytes < fvr_pou_slice_image_adjoint_workspace(B, N)) return FVR_ERR_WORKSPACE;
+  return pou_image_common(true, dtype, stencil, scales, B, P, geo, N, freqs, grad_imgs, nullptr,
+                          static_cast<double*>(workspace), stream);
+}
+
 int fvr_pou_warp(const float* imgs, int64_t B, int64_t N, int64_t P, const void* db, const void* cu, const void* cv,
                  int offs_f64, int64_t ostride, const float* rx, const float* ry, const float* ic, int64_t K,
                  int64_t ray_stride, double inv_ds, double c_idx, float* out, void* stream) {
@@ -675,12 +1026,12 @@ int fvr_pou_warp(const float* imgs, int64_t B, int64_t N, int64_t P, const void*
     WarpArgs<double> a{imgs, static_cast<const double*>(db), static_cast<const double*>(cu),
                        static_cast<const double*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
                        (int)P, (int)K, ray_stride};
-    pou_warp_kernel<double><<<grid, 256, 0, s>>>(a, out);
+    pou_warp_kernel<double><<<grid, 256, static_cast<size_t>(B), s>>>(a, out);
   } else {
     WarpArgs<float> a{imgs, static_cast<const float*>(db), static_cast<const float*>(cu),
                       static_cast<const float*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
                       (int)P, (int)K, ray_stride};
-    pou_warp_kernel<float><<<grid, 256, 0, s>>>(a, out);
+    pou_warp_kernel<float><<<grid, 256, static_cast<size_t>(B), s>>>(a, out);
   }
   FVR_LAUNCH_CHECK();
   return FVR_OK;
@@ -701,7 +1052,7 @@ int fvr_pou_warp_bwd(const float* imgs, int64_t B, int64_t N, int64_t P, const v
   const int tiles = static_cast<int>(cdiv64(K, 256));
   dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(N));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t sm = 3 * B * sizeof(double);
+  const size_t sm = 3 * B * sizeof(double) + B;
   double* part = static_cast<double*>(workspace);
   if (offs_f64) {
     WarpArgs<double> a{imgs, static_cast<const double*>(db), static_cast<const double*>(cu),
@@ -735,7 +1086,8 @@ int fvr_pou_pose_backward(const double* sl_part, int64_t tiles, const double* go
   if (!sl_part || !geo || !centers || (!gmats && !gvec) || (gmats && !base12) || B < 1 || N < 1 || tiles < 1)
     return FVR_ERR_ARG;
   const double zero12[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  pou_pose_bwd_kernel<<<static_cast<unsigned>(cdiv64(N, 64)), 64, 0, static_cast<cudaStream_t>(stream)>>>(
+  if (N > 2147483647) return FVR_ERR_ARG;
+  pou_pose_bwd_kernel<<<static_cast<unsigned>(N), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       sl_part, (int)tiles, goffs, ray_part, (int)rtiles, geo, centers, (int)B, (int)N,
       make_base(base12 ? base12 : zero12), vscale, gmats, gvec);
   FVR_LAUNCH_CHECK();

@@ -203,4 +203,105 @@ __device__ __forceinline__ bool stencil_sample_d(const Stencil& s, double px, do
   return c.e >= 0;
 }
 
+// ---- per-CTA split-position tables (shared by the slice kernels) ---------
+
+// Per-CTA sample tables.  The slice position s + ku*u + kv*v is split into a
+// row part (s + ku*u, ku = lin[i]) and a column part (kv*v, kv = lin[j]); each
+// is formed in FP64 once per CTA and kept as an integer cell index plus a
+// float fraction in [0, 1], so a sample's position (their sum) is the FP64
+// position to within 2^-24 of a cell with integer adds and one float add per
+// axis.  The phase ramp factorises the same way:
+//   e^{i pi kpi (ku tx + kv ty)} = e^{i pi kpi ku tx} . e^{i pi kpi kv ty},
+// each factor from FP64 sincospi.  Entry n < R is column n; entry R + r is row
+// row0 + r.  (Kernels without a phase ramp leave ph unused.)
+struct AxisTables {
+  int4* idx;    // (floor x, floor y, floor z, -)
+  float4* frac; // (frac x, frac y, frac z, k)
+  float2* ph;   // (cos, sin)
+};
+
+__device__ __forceinline__ AxisTables axis_tables(unsigned char* smem, int n_tab) {
+  AxisTables t;
+  t.idx = reinterpret_cast<int4*>(smem);
+  t.frac = reinterpret_cast<float4*>(smem + 16 * n_tab);
+  t.ph = reinterpret_cast<float2*>(smem + 32 * n_tab);
+  return t;
+}
+
+// Cell of sample (row entry a, column entry b); e = -1 when no corner of the
+// cell is inside (zero-padding partial: -1 <= p < n on every axis).
+struct TabCell {
+  int e;
+  float tx, ty, tz;
+  int ex, ey, ez;
+};
+
+__device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa, int4 ib, float4 fb) {
+  TabCell c;
+  c.tx = fa.x + fb.x;
+  c.ty = fa.y + fb.y;
+  c.tz = fa.z + fb.z;
+  int ix = ia.x + ib.x, iy = ia.y + ib.y, iz = ia.z + ib.z;
+  if (c.tx >= 1.f) { c.tx -= 1.f; ++ix; }
+  if (c.ty >= 1.f) { c.ty -= 1.f; ++iy; }
+  if (c.tz >= 1.f) { c.tz -= 1.f; ++iz; }
+  c.ex = ix + 1;
+  c.ey = iy + 1;
+  c.ez = iz + 1;
+  const bool ok = static_cast<unsigned>(c.ex) <= static_cast<unsigned>(s.W) &&
+                  static_cast<unsigned>(c.ey) <= static_cast<unsigned>(s.H) &&
+                  static_cast<unsigned>(c.ez) <= static_cast<unsigned>(s.D);
+  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + 1) + c.ex : -1;
+  return c;
+}
+
+// Entry load without the f16 brick scale applied (it multiplies the
+// interpolated value and derivatives instead: 8 products, not 16).
+template <int DT>
+__device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw<DT>& r) {
+  if constexpr (DT == FVR_F32) {
+    if (c.e < 0) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      return;
+    }
+    const float4* p = static_cast<const float4*>(s.data) + static_cast<int64_t>(c.e) * 4;
+    ldg256(p, r.q[0], r.q[1]);
+    ldg256(p + 2, r.q[2], r.q[3]);
+  } else {
+    if (c.e < 0) {
+      r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
+      if constexpr (DT == FVR_F16) r.sc = 0.f;
+      return;
+    }
+    ldg256(static_cast<const uint4*>(s.data) + static_cast<int64_t>(c.e) * 2, r.q[0], r.q[1]);
+    if constexpr (DT == FVR_F16) {
+      const int bx = (s.W + kBrick) / kBrick, by = (s.H + kBrick) / kBrick;
+      r.sc = __ldg(s.scales + ((c.ez / kBrick) * by + c.ey / kBrick) * bx + c.ex / kBrick);
+    }
+  }
+}
+
+template <int DT>
+__device__ __forceinline__ void tab_decode(const Raw<DT>& r, Sample8& v) {
+  if constexpr (DT == FVR_F16) {
+    const uint32_t w[8] = {r.q[0].x, r.q[0].y, r.q[0].z, r.q[0].w, r.q[1].x, r.q[1].y, r.q[1].z, r.q[1].w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v.re[i] = h_lo(w[i]);
+      v.im[i] = h_hi(w[i]);
+    }
+  } else {
+    raw_decode<DT>(r, v);
+  }
+}
+
+template <int DT>
+__device__ __forceinline__ float raw_scale(const Raw<DT>& r) {
+  if constexpr (DT == FVR_F16)
+    return r.sc;
+  else
+    return 1.f;
+}
+
 }  // namespace fvr

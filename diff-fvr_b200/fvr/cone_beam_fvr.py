@@ -158,6 +158,47 @@ def _prepared_lattice(lattice, device):
     return hit
 
 
+def _block_images(model, geo, N, s):
+    """imgs [B, N, P, P] = Re fftshift(ifft2(ifftshift(slice))) for every block
+    and pose (cone_beam_fvr.py:480-505): fused slice + inverse FFT in shared
+    memory where P allows, else slice kernel + batched 2D IFFT."""
+    dev = geo.device
+    B, P = model.B, model.P
+    st = model._stencil
+    imgs = torch.empty((B, N, P, P), dtype=torch.float32, device=dev)
+    if L.query("fvr_pou_image_supported", P):
+        L.call("fvr_pou_slice_image", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
+               L.ptr(model._freqs), L.ptr(imgs), s)
+        return imgs
+    slices = torch.empty((B, N, P, P), dtype=torch.complex64, device=dev)
+    L.call("fvr_pou_slice", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N, L.ptr(model._freqs),
+           L.ptr(slices), s)
+    RT.fft2d(slices, inverse=True, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P), out_mode=RT.OUT_REAL, out=imgs,
+             work=slices)
+    return imgs
+
+
+def _block_images_adjoint(model, geo, N, grad_imgs, s):
+    """Slice-adjoint partials (workspace, tiles per (pose, block)) from dL/dimgs:
+    fused FFT + slice adjoint where P allows, else batched 2D FFT + adjoint kernel."""
+    dev = geo.device
+    B, P = model.B, model.P
+    st = model._stencil
+    if L.query("fvr_pou_image_supported", P):
+        wsb = L.query("fvr_pou_slice_image_adjoint_workspace", B, N)
+        ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        L.call("fvr_pou_slice_image_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
+               L.ptr(model._freqs), L.ptr(grad_imgs), L.ptr(ws), wsb, s)
+        return ws, 1
+    # adjoint of S -> Re fftshift(ifft2(ifftshift(S))): fftshift(fft2(ifftshift(g))) / P^2
+    G = RT.fft2d(grad_imgs, inverse=False, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P))
+    wsb = L.query("fvr_pou_slice_adjoint_workspace", B, P, N)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    L.call("fvr_pou_slice_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
+           L.ptr(model._freqs), L.ptr(G), L.ptr(ws), wsb, s)
+    return ws, (P * P + 255) // 256
+
+
 class _PinholeFn(torch.autograd.Function):
     """SE(3)-invariant pinhole path (cone_beam_fvr.py:547-573, 670-686):
     mats -> pose geometry -> block slices -> batched IFFT -> warp-sum."""
@@ -174,15 +215,8 @@ class _PinholeFn(torch.autograd.Function):
         s = L.stream_ptr(dev)
         vscale = float(P) * model.ds_block
         L.call("fvr_pou_pose", L.ptr(m), None, N, base, vscale, L.ptr(model.centers), B, L.ptr(geo), L.ptr(offs), s)
-        st = model._stencil
-        slices = torch.empty((B, N, P, P), dtype=torch.complex64, device=dev)
         with profiling.section("pou_slice"):
-            L.call("fvr_pou_slice", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
-                   L.ptr(model._freqs), L.ptr(slices), s)
-        imgs = torch.empty((B, N, P, P), dtype=torch.float32, device=dev)
-        RT.fft2d(slices, inverse=True, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P), out_mode=RT.OUT_REAL, out=imgs,
-                 work=slices)
-        del slices
+            imgs = _block_images(model, geo, N, s)
         H, W = int(rx.shape[0]), int(rx.shape[1])
         out = torch.empty((N, 1, H, W), dtype=torch.float32, device=dev)
         with profiling.section("pou_warp"):
@@ -209,16 +243,9 @@ class _PinholeFn(torch.autograd.Function):
         L.call("fvr_pou_warp_bwd", L.ptr(imgs), B, N, P, L.ptr(offs), _ct.c_void_p(offs.data_ptr() + 8),
                _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), H * W, 0,
                1.0 / model.ds_block, float(P // 2), L.ptr(g), L.ptr(grad_imgs), L.ptr(goffs), None, L.ptr(ws), wsb, s)
-        # adjoint of S -> Re fftshift(ifft2(ifftshift(S))): fftshift(fft2(ifftshift(g))) / P^2
-        G = RT.fft2d(grad_imgs, inverse=False, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P))
+        ws2, tiles = _block_images_adjoint(model, geo, N, grad_imgs, s)
         del grad_imgs
-        st = model._stencil
-        wsb2 = L.query("fvr_pou_slice_adjoint_workspace", B, P, N)
-        ws2 = torch.empty(wsb2, dtype=torch.uint8, device=dev)
-        L.call("fvr_pou_slice_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
-               L.ptr(model._freqs), L.ptr(G), L.ptr(ws2), wsb2, s)
         gm = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
-        tiles = (P * P + 255) // 256
         L.call("fvr_pou_pose_backward", L.ptr(ws2), tiles, L.ptr(goffs), None, 0, L.ptr(geo), L.ptr(model.centers), B,
                N, _LATTICE_CACHE[base_key][1], float(P) * model.ds_block, L.ptr(gm), None, s)
         return gm.to(mdt), None, None, None, None, None

@@ -9,7 +9,6 @@ import ctypes as _ct
 import torch
 
 from . import _lib as L
-from . import _runtime as RT
 
 
 class _RaysFn(torch.autograd.Function):
@@ -34,14 +33,9 @@ class _RaysFn(torch.autograd.Function):
         ry = torch.empty((N, K), **f32)
         ic = torch.empty((N, K), **f32)
         L.call("fvr_pou_rays_prep", L.ptr(t), L.ptr(geo), N, K, L.ptr(rx), L.ptr(ry), L.ptr(ic), s)
-        st = model._stencil
-        slices = torch.empty((B, N, P, P), dtype=torch.complex64, device=dev)
-        L.call("fvr_pou_slice", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N, L.ptr(model._freqs),
-               L.ptr(slices), s)
-        imgs = torch.empty((B, N, P, P), **f32)
-        RT.fft2d(slices, inverse=True, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P), out_mode=RT.OUT_REAL, out=imgs,
-                 work=slices)
-        del slices
+        from .cone_beam_fvr import _block_images
+
+        imgs = _block_images(model, geo, N, s)
         out = torch.empty((N, H, W), **f32)
         L.call("fvr_pou_warp", L.ptr(imgs), B, N, P, L.ptr(offs), _ct.c_void_p(offs.data_ptr() + 8),
                _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), K, K, 1.0 / model.ds_block,
@@ -68,19 +62,16 @@ class _RaysFn(torch.autograd.Function):
         L.call("fvr_pou_warp_bwd", L.ptr(imgs), B, N, P, L.ptr(offs), _ct.c_void_p(offs.data_ptr() + 8),
                _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), K, K, 1.0 / model.ds_block,
                float(P // 2), L.ptr(g), L.ptr(grad_imgs), L.ptr(goffs), L.ptr(gray), L.ptr(ws), wsb, s)
-        G = RT.fft2d(grad_imgs, inverse=False, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P))
+        from .cone_beam_fvr import _block_images_adjoint
+
+        ws2, tiles = _block_images_adjoint(model, geo, N, grad_imgs, s)
         del grad_imgs
-        st = model._stencil
-        wsb2 = L.query("fvr_pou_slice_adjoint_workspace", B, P, N)
-        ws2 = torch.empty(wsb2, dtype=torch.uint8, device=dev)
-        L.call("fvr_pou_slice_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
-               L.ptr(model._freqs), L.ptr(G), L.ptr(ws2), wsb2, s)
         gtrg = torch.empty((N, K, 3), dtype=torch.float32, device=dev)
         wsb3 = L.query("fvr_pou_rays_bwd_workspace", N, K)
         ws3 = torch.empty(wsb3, dtype=torch.uint8, device=dev)
         L.call("fvr_pou_rays_bwd", L.ptr(t), L.ptr(geo), N, K, L.ptr(gray), L.ptr(gtrg), L.ptr(ws3), wsb3, s)
         gvec = torch.empty((N, 12), dtype=torch.float32, device=dev)
-        L.call("fvr_pou_pose_backward", L.ptr(ws2), (P * P + 255) // 256, L.ptr(goffs), L.ptr(ws3), (K + 255) // 256,
+        L.call("fvr_pou_pose_backward", L.ptr(ws2), tiles, L.ptr(goffs), L.ptr(ws3), (K + 255) // 256,
                L.ptr(geo), L.ptr(model.centers), B, N, None, float(P) * model.ds_block, None, L.ptr(gvec), s)
         return (gvec[:, 0:3].to(sdt), gtrg.view(N, H, W, 3).to(tdt), gvec[:, 3:6].to(sdt), gvec[:, 6:9].to(sdt),
                 gvec[:, 9:12].to(sdt), None)

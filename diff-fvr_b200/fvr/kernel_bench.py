@@ -76,6 +76,8 @@ def main():
     ap.add_argument("--det", type=int, default=256)
     ap.add_argument("--launches", type=int, default=3)
     args = ap.parse_args()
+    # backward on this thread, so the NVTX range below also covers the adjoint kernels
+    torch.autograd.set_multithreading_enabled(False)
     step = _sncc(args) if args.path == "sncc" else _pou(args)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

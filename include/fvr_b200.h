@@ -250,6 +250,23 @@ int64_t fvr_pou_slice_adjoint_workspace(int64_t B, int64_t P, int64_t N);
 int fvr_pou_slice_adjoint(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
                           const double* geo, int64_t N, const float* freqs, const void* G, void* workspace,
                           int64_t ws_bytes, void* stream);
+/* Fused block images for P in {64, 96, 128, 160} (fvr_pou_image_supported):
+ * one CTA per (pose, block) gathers the slice, runs the 2D inverse FFT in
+ * shared memory and writes imgs[B][N][P][P] = Re fftshift(ifft2(ifftshift(S)))
+ * (f32), i.e. fvr_pou_slice + fvr_fft2d without the complex intermediate.
+ * Replaces PerspectiveSlabFVR._slice_and_ifft, src/fvr/cone_beam_fvr.py:480-505. */
+int fvr_pou_image_supported(int64_t P);
+int fvr_pou_slice_image(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P, const double* geo,
+                        int64_t N, const float* freqs, float* imgs, void* stream);
+/* Its adjoint: from dL/dimgs [B][N][P][P] (f32), G = fftshift(fft2(ifftshift(
+ * g))) / P^2 in shared memory and the slice adjoint in the same CTA;
+ * workspace[N][B][6] fp64 (one tile per (pose, block)) feeds
+ * fvr_pou_pose_backward with tiles = 1.  Autograd backward of
+ * cone_beam_fvr.py:480-505. */
+int64_t fvr_pou_slice_image_adjoint_workspace(int64_t B, int64_t N);
+int fvr_pou_slice_image_adjoint(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
+                                const double* geo, int64_t N, const float* freqs, const float* grad_imgs,
+                                void* workspace, int64_t ws_bytes, void* stream);
 /* out[N][K] = ic[q] * sum_b bilinear(imgs[b][n], (d_b rx - cu)/ds + c, (d_b ry - cv)/ds + c),
  * zero padding; offsets float (offs_f64 = 0) or double, element (b, n) at
  * index (b*N + n) * ostride; ray tables shared (ray_stride 0) or per pose

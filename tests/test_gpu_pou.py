@@ -350,3 +350,58 @@ def test_edge_dominant_ncc_vs_torch64(B, Bt, C, H, W, crop, w, mean):
     assert rel_l2(val.detach().double().cpu().numpy(), ref.detach().cpu().numpy()) < 1e-6
     assert rel_l2(a.grad.double().cpu().numpy(), a64.grad.cpu().numpy()) < 1e-4
     assert rel_l2(b.grad.double().cpu().numpy(), b64.grad.cpu().numpy()) < 1e-4
+
+
+# ------------------------------------------------ fused block-image kernels
+
+
+@pytest.mark.parametrize("block_res,dtype", [(32, torch.float32), (48, torch.bfloat16), (64, torch.float32),
+                                             (64, torch.bfloat16), (80, torch.float32)])
+def test_fused_block_images_match_slice_plus_fft(block_res, dtype):
+    """fvr_pou_slice_image (slice + inverse FFT in one CTA) and its adjoint
+    equal the unfused slice kernel + batched FFT path, P = 2 x block_res in
+    {64, 96, 128, 160}."""
+    import ctypes
+
+    import fvr._lib as L
+    from fvr import _runtime as RT
+    from fvr.cone_beam_fvr import PerspectiveSlabFVR
+    from fvr.synthetic import make_ellipsoid_volume, make_pinhole_mats
+
+    vol = make_ellipsoid_volume(64, 3)
+    m = PerspectiveSlabFVR.from_volume(vol, vox_mm=1.5, grid_blocks=(2, 2, 2), block_res=block_res, overlap=0.5,
+                                       dtype=dtype)
+    B, P, N = m.B, m.P, 3
+    assert L.query("fvr_pou_image_supported", P) == 1
+    dev = m._dev
+    mats = make_pinhole_mats(N, 4, sad_mm=400.0, device=dev).to(torch.float32).contiguous()
+    geo = torch.empty((N, int(L.query("fvr_pou_geo_stride"))), dtype=torch.float64, device=dev)
+    offs = torch.empty((B, N, 3), dtype=torch.float64, device=dev)
+    base = (ctypes.c_double * 12)(*([0.0] * 3 + [1.0, 0, 0] + [0, 1.0, 0] + [0, 0, 1.0]))
+    s = L.stream_ptr(dev)
+    L.call("fvr_pou_pose", L.ptr(mats), None, N, base, float(P) * m.ds_block, L.ptr(m.centers), B, L.ptr(geo),
+           L.ptr(offs), s)
+    st = m._stencil
+    fused = torch.empty((B, N, P, P), dtype=torch.float32, device=dev)
+    L.call("fvr_pou_slice_image", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
+           L.ptr(m._freqs), L.ptr(fused), s)
+    slices = torch.empty((B, N, P, P), dtype=torch.complex64, device=dev)
+    L.call("fvr_pou_slice", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N, L.ptr(m._freqs),
+           L.ptr(slices), s)
+    ref = RT.fft2d(slices, inverse=True, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P), out_mode=RT.OUT_REAL)
+    assert rel_l2(fused.cpu().numpy(), ref.cpu().numpy()) < 2e-6
+    # adjoint against the unfused FFT + slice adjoint (tile sums)
+    g = torch.from_numpy(np.random.default_rng(1).standard_normal((B, N, P, P)).astype(np.float32)).to(dev)
+    wsb = L.query("fvr_pou_slice_image_adjoint_workspace", B, N)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    L.call("fvr_pou_slice_image_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
+           L.ptr(m._freqs), L.ptr(g), L.ptr(ws), wsb, s)
+    got = ws[: N * B * 6 * 8].view(torch.float64).view(N, B, 6).cpu().numpy()
+    G = RT.fft2d(g, inverse=False, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P))
+    wsb2 = L.query("fvr_pou_slice_adjoint_workspace", B, P, N)
+    ws2 = torch.empty(wsb2, dtype=torch.uint8, device=dev)
+    L.call("fvr_pou_slice_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
+           L.ptr(m._freqs), L.ptr(G), L.ptr(ws2), wsb2, s)
+    tiles = (P * P + 255) // 256
+    want = ws2[: N * B * tiles * 6 * 8].view(torch.float64).view(N, B, tiles, 6).sum(2).cpu().numpy()
+    assert rel_l2(got, want) < 2e-5
