@@ -257,6 +257,8 @@ def run_b200(args, torch):
         e2e_eager()
     t_eager, _ = _time_steps(torch, e2e_eager, K, flush)
 
+    pou = _pou_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
+
     res = None
     if rank == 0:
         peak, peak_kind = _peak_hbm()
@@ -330,6 +332,7 @@ def run_b200(args, torch):
             "gpu_launches": int(f16["kernels_per_step"] * K),
             "kernels_per_step": int(f16["kernels_per_step"]),
             "clocks": f16["clocks"],
+            "pou_cone_beam": pou,
         }
     if ws > 1:
         dist.barrier()
@@ -347,6 +350,44 @@ def _f16_from_f32(eng, vol, dev, torch):
     fresh.to_precision(torch.float16)
     eng._stencil = fresh._stencil
     eng.f_vol_5d = fresh.f_vol_5d
+
+
+def _pou_leg(torch, dev, flush, warmup, steps):
+    """Secondary line: the PoU-FVR cone-beam step (192^3 ellipsoid volume, 4x4x4
+    blocks at 50 % overlap, block_res 64 -> P = 128; pinhole SDD 1020 / SAD 765
+    mm, 256^2 detector at 0.8 mm; 64 candidate poses, forward + pose gradient
+    through the reference API forward_pinhole(...).sum().backward())."""
+    from fvr import synthetic
+    from fvr.cone_beam_fvr import PerspectiveSlabFVR
+
+    out = {}
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+        vol = synthetic.make_ellipsoid_volume(192, SEED)
+        m = PerspectiveSlabFVR.from_volume(vol, vox_mm=1.0, grid_blocks=(4, 4, 4), block_res=64, overlap=0.5,
+                                           dtype=dt, device=dev)
+        f = 1020.0 / 0.8
+        k_inv = torch.tensor([[1.0 / f, 0.0, -128.0 / f], [0.0, 1.0 / f, -128.0 / f], [0.0, 0.0, 1.0]], device=dev)
+        lattice = m.make_pinhole_lattice(k_inv, 1020.0, 256, 256)
+        mats = synthetic.make_pinhole_mats(CANDIDATES, SEED + 1, sad_mm=765.0, device=dev)
+
+        def step():
+            mm = mats.detach().requires_grad_(True)
+            m.forward_pinhole(mm, lattice).sum().backward()
+            return mm.grad
+
+        for _ in range(warmup):
+            step()
+        t, _ = _time_steps(torch, step, steps, flush)
+        ms = statistics.mean(t)
+        out[name] = {"value": CANDIDATES / (ms / 1e3), "ms_per_step": ms, "blocks": int(m.B), "P": int(m.P)}
+        del m, lattice
+        torch.cuda.empty_cache()
+    out["unit"] = UNIT
+    out["workload"] = ("PoU-FVR cone-beam: seeded 192^3 ellipsoid volume (1 mm), 4x4x4 blocks, 50% overlap, "
+                       "block_res 64 (P = 128), SDD 1020 / SAD 765 mm, 256x256 detector at 0.8 mm, 64 poses, "
+                       "forward + pose gradient (eager autograd through forward_pinhole)")
+    out["l2"] = "flushed before every timed step (256 MiB write)"
+    return out
 
 
 def _cpu_baseline_leg(vol, poses_np, f_ap, f_lat, results):
