@@ -51,6 +51,8 @@ SIGNATURES = {
     "fvr_tc_sncc_fused_workspace": (I64, [I64, I64, I64]),
     "fvr_tc_sncc_value_and_grad_static": (I32, [I32, P, P, I64, I64, I64, P, I64, I32, P, P, P, P, I64, F64, I32, P,
                                                 I64, P, P, P, I32, P]),
+    "fvr_se3_exp": (I32, [P, I64, P, P]),
+    "fvr_se3_exp_backward": (I32, [P, P, I64, P, P]),
     "fvr_edge_ncc_workspace": (I64, [I64, I64, I64, I64, I64]),
     "fvr_edge_ncc_stats_count": (I64, []),
     "fvr_edge_ncc_forward": (I32, [P, P, I64, I64, I64, I64, I64, I64, F32, I32, P, I64, P, P, P]),

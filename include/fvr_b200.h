@@ -338,6 +338,16 @@ int fvr_cncc_forward(const void* Fp, const void* Ft, int64_t B, int64_t Bt, int6
 int fvr_cncc_backward(const void* Fp, const void* Ft, int64_t B, int64_t Bt, int64_t n, const float* hp,
                       const double* mom, const float* g, void* X, void* stream);
 
+/* ------------------------------------------------------ SE(3) exp map -- */
+/* theta[N][6] = (w_x, w_y, w_z, t_x, t_y, t_z) (rad, mm) -> mats[N][4][4]
+ * = [[exp([w]x), t], [0, 1]] (Rodrigues, fp64 inside).  The map the
+ * reference builds with torch.matrix_exp of the skew matrix:
+ * experiments/exp30_gpu_multistart_registration.py:42-55,
+ * tests/test_cone_beam_fvr.py:221-229. */
+int fvr_se3_exp(const float* theta, int64_t N, float* mats, void* stream);
+/* grad_theta[N][6] from grad_mats[N][4][4] (dR/dw in closed form). */
+int fvr_se3_exp_backward(const float* theta, const float* grad_mats, int64_t N, float* grad_theta, void* stream);
+
 /* ------------------------------------------ edge-dominant gradient NCC -- */
 /* pred a[B][C][H][W], target b[Bt][C][H][W] (Bt = 1 broadcast, or B), f32.
  * Sobel-x / Sobel-y responses (zero padding) on the interior [crop, H-crop) x
