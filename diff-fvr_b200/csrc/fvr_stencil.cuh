@@ -68,6 +68,50 @@ __device__ __forceinline__ void trilerp(const Sample8& v, float tx, float ty, fl
   }
 }
 
+// ---- packed (re, im) form: sm_100 FP32x2 arithmetic ------------------------
+//
+// Every step of the trilinear lerp treats the real and imaginary parts alike,
+// so a corner kept as a float2 (re, im) pair goes through one fma.rn.f32x2 /
+// add.rn.f32x2 per step instead of two scalar instructions.  Each component
+// is rounded exactly as the scalar form rounds it: a - b is formed as
+// fma(b, -1, a), a single rounding of the exact difference.
+
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
+struct Sample8c {
+  float2 c[8];  // corner (re, im), c = dz*4 + dy*2 + dx
+};
+
+struct Interp2 {
+  float2 s;           // value
+  float2 d[3];        // d/dx, d/dy, d/dz
+};
+
+// trilerp in packed form: the same nested lerps, component for component.
+template <bool DERIV>
+__device__ __forceinline__ void trilerp2(const Sample8c& v, float tx, float ty, float tz, Interp2& o) {
+  const float2 TX = f2(tx), TY = f2(ty), TZ = f2(tz);
+  float2 a[4], x[4];
+#pragma unroll
+  for (int zy = 0; zy < 4; ++zy) {
+    x[zy] = sub2(v.c[2 * zy + 1], v.c[2 * zy]);
+    a[zy] = fma2(TX, x[zy], v.c[2 * zy]);
+  }
+  const float2 by0 = sub2(a[1], a[0]), by1 = sub2(a[3], a[2]);
+  const float2 b0 = fma2(TY, by0, a[0]), b1 = fma2(TY, by1, a[2]);
+  o.d[2] = sub2(b1, b0);
+  o.s = fma2(TZ, o.d[2], b0);
+  if (DERIV) {
+    o.d[1] = fma2(TZ, sub2(by1, by0), by0);
+    const float2 cx0 = fma2(TY, sub2(x[1], x[0]), x[0]);
+    const float2 cx1 = fma2(TY, sub2(x[3], x[2]), x[2]);
+    o.d[0] = fma2(TZ, sub2(cx1, cx0), cx0);
+  }
+}
+
 // ---- split load / decode, so a thread can put several samples' loads in flight
 
 // One 256-bit read-only load (sm_100 ld.global.nc.v8): a whole 32-byte stencil
@@ -293,6 +337,27 @@ __device__ __forceinline__ void tab_decode(const Raw<DT>& r, Sample8& v) {
     }
   } else {
     raw_decode<DT>(r, v);
+  }
+}
+
+// Corners as (re, im) pairs, f16 without its brick scale (as tab_decode).
+template <int DT>
+__device__ __forceinline__ void tab_decode2(const Raw<DT>& r, Sample8c& v) {
+  if constexpr (DT == FVR_F32) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      v.c[2 * i] = make_float2(r.q[i].x, r.q[i].y);
+      v.c[2 * i + 1] = make_float2(r.q[i].z, r.q[i].w);
+    }
+  } else {
+    const uint32_t w[8] = {r.q[0].x, r.q[0].y, r.q[0].z, r.q[0].w, r.q[1].x, r.q[1].y, r.q[1].z, r.q[1].w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      if constexpr (DT == FVR_BF16)
+        v.c[i] = make_float2(bf_lo(w[i]), bf_hi(w[i]));
+      else
+        v.c[i] = make_float2(h_lo(w[i]), h_hi(w[i]));
+    }
   }
 }
 

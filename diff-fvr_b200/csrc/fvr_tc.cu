@@ -12,6 +12,7 @@
 //    ifftshift order for the 2D IFFT, and the per-sample slice adjoint.
 //  * FP64 pose maps: Euler (yaw Z, pitch Y, roll X) -> slice axes and the
 //    Euler vector-Jacobian product (torch_engine.py:139-211).
+#include <algorithm>
 #include <mutex>
 
 #include "fvr_pose.cuh"
@@ -111,16 +112,14 @@ constexpr int kMaxViews = 4;
 constexpr int kSnccThreads = 256;
 
 // Launch variants of the moments kernel (chosen per shape by the caller's
-// autotuner): samples whose loads are in flight per thread, and the resident
-// CTAs per SM the register budget is sized for.
+// autotuner): rows per thread whose loads are in flight together (a group),
+// and the resident CTAs per SM the register budget is sized for.
 struct SnccVariant {
   int group, min_blocks;
 };
-constexpr int kSnccVariants = 6;
-__host__ __device__ constexpr SnccVariant sncc_variant(int v) {
-  return v == 1 ? SnccVariant{2, 4} : v == 2 ? SnccVariant{4, 3} : v == 3 ? SnccVariant{8, 1}
-                : v == 4 ? SnccVariant{2, 3} : v == 5 ? SnccVariant{3, 3} : SnccVariant{4, 2};
-}
+constexpr SnccVariant kSnccVariantTable[] = {{4, 2}, {2, 4}, {4, 3}, {8, 1}, {2, 3}, {3, 3}, {6, 1}, {3, 2}};
+constexpr int kSnccVariants = sizeof(kSnccVariantTable) / sizeof(kSnccVariantTable[0]);
+constexpr SnccVariant sncc_variant(int v) { return kSnccVariantTable[v]; }
 
 struct SnccArgs {
   Stencil st;
@@ -129,13 +128,13 @@ struct SnccArgs {
   int lateral[kMaxViews];
   const float* hp;   // [R*R] or null
   const float* lin;  // [R]
-  int R, C, tile;    // tile = samples per CTA
-  int tab_rows;      // row-table entries per CTA (>= rows a tile touches)
+  int R, C, nv;
+  int tile_rows;     // slice rows per CTA (= row-table entries)
+  int tiles;         // CTAs per (candidate, view): record (v * C + c) * tiles + tile
   double kpi;        // kappa / pi
   double sx, sy, sz;
-  double* partial;  // [nv][C][tiles][NM]
-  // fused epilogue (value_and_grad launch) only
-  unsigned* counters;  // [C + 1], zero on entry, left zero on exit
+  double* partial;  // partial-moment records of NM doubles
+  // value-and-gradient epilogue only
   double* mom;         // [nv][C][kMomStride]
   double* jac;         // [nv][C][18]: slice-axes Jacobian per (view, candidate)
   float* loss;         // [nv + 1]
@@ -210,7 +209,26 @@ __device__ __forceinline__ void block_reduce_d(T (&acc)[NV], double* red, double
   }
 }
 
-__device__ __forceinline__ void build_axis_tables(const AxisTables& t, int R, int row0, int n_row,
+// Per-(candidate, view) sample tables of the moments kernels (see
+// AxisTables): integer cell, fraction, and (k, k, cos, sin) with the grid
+// value k kept as a pair for the packed moment products.  48 B per entry.
+// Column entries' integer parts include the stencil's +1 entry offset.
+struct SnccTab {
+  int4* idx;    // (floor x, floor y, floor z, -), columns + 1
+  float4* frac; // (frac x, frac y, frac z, k)
+  float4* kph;  // (k, k, cos, sin)
+};
+constexpr int kSnccTabEntryBytes = 48;
+
+__device__ __forceinline__ SnccTab sncc_tab(unsigned char* smem, int n_tab) {
+  SnccTab t;
+  t.idx = reinterpret_cast<int4*>(smem);
+  t.frac = reinterpret_cast<float4*>(smem + 16 * n_tab);
+  t.kph = reinterpret_cast<float4*>(smem + 32 * n_tab);
+  return t;
+}
+
+__device__ __forceinline__ void build_sncc_tables(const SnccTab& t, int R, int row0, int n_row,
                                                   const float* __restrict__ lin, const double* ax, double sx,
                                                   double sy, double sz, double kpi) {
   for (int n = threadIdx.x; n < R + n_row; n += blockDim.x) {
@@ -221,238 +239,351 @@ __device__ __forceinline__ void build_axis_tables(const AxisTables& t, int R, in
     const double py = col ? k * ax[4] : fma(k, ax[1], sy);
     const double pz = col ? k * ax[5] : fma(k, ax[2], sz);
     const double fx = floor(px), fy = floor(py), fz = floor(pz);
-    t.idx[n] = make_int4(static_cast<int>(fx), static_cast<int>(fy), static_cast<int>(fz), 0);
+    const int one = col ? 1 : 0;  // entry = voxel + 1, carried by the column part
+    t.idx[n] = make_int4(static_cast<int>(fx) + one, static_cast<int>(fy) + one, static_cast<int>(fz) + one, 0);
     t.frac[n] = make_float4(static_cast<float>(px - fx), static_cast<float>(py - fy), static_cast<float>(pz - fz), kf);
     double sn, cs;
     sincospi(kpi * k * (col ? ax[7] : ax[6]), &sn, &cs);
-    t.ph[n] = make_float2(static_cast<float>(cs), static_cast<float>(sn));
+    t.kph[n] = make_float4(kf, kf, static_cast<float>(cs), static_cast<float>(sn));
   }
 }
 
+// view v's parameters without dynamic indexing of the kernel parameter space
+__device__ __forceinline__ int view_lateral(const SnccArgs& a, int v) {
+  return v == 0 ? a.lateral[0] : v == 1 ? a.lateral[1] : v == 2 ? a.lateral[2] : a.lateral[3];
+}
+__device__ __forceinline__ const float2* view_target(const SnccArgs& a, int v) {
+  return v == 0 ? a.ftarg[0] : v == 1 ? a.ftarg[1] : v == 2 ? a.ftarg[2] : a.ftarg[3];
+}
 
-// Ticket protocol (as a grid barrier does it): the CTA barrier orders every
-// thread's stores before thread 0, whose fence publishes them at device scope
-// before it takes a ticket; the thread that takes a last ticket fences again
-// before its CTA reads the other CTAs' records (through L2).  The candidate
-// epilogue needs one round of loads (tile sums and the stored axes
-// Jacobians) and fp64 arithmetic in one thread; the losses one more round.
-__device__ __forceinline__ void sncc_fused_epilogue(const SnccArgs& a, int c) {
-  __shared__ int s_last;
-  __shared__ double s_mom[kMaxViews][kMomStride];
-  __shared__ double s_jac[kMaxViews][18];
-  const int tiles = gridDim.x, nv = gridDim.z, C = a.C;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const bool last = atomicAdd(a.counters + c, 1u) == static_cast<unsigned>(tiles * nv - 1);
-    if (last) __threadfence();
-    s_last = last;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  // candidate c is complete: tile sums (fixed order) and Jacobians in one round
-  for (int t = threadIdx.x; t < nv * (M_NGRAD + 18); t += blockDim.x) {
-    if (t < nv * M_NGRAD) {
-      const int v = t / M_NGRAD, m = t - v * M_NGRAD;
-      const double* src = a.partial + (static_cast<int64_t>(v) * C + c) * tiles * M_NGRAD + m;
-      double sum = 0.0;
-      for (int k0 = 0; k0 < tiles; k0 += 4) {  // four independent loads in flight
-        double x[4];
+// Slice axes of (candidate c, view v) into ax[8].
+__device__ __forceinline__ void sncc_item_axes(const SnccArgs& a, int v, int c, double* ax) {
+  slice_axes(a.poses + 6 * c, view_lateral(a, v), a.sx, a.sy, a.sz, ax);
+}
+
+// Programmatic dependent launch (sm_90+): a kernel launched after this one
+// with programmatic stream serialisation may start once every CTA of this
+// grid has signalled; griddepcontrol.wait in that kernel still returns only
+// when this grid has completed and its memory is visible.  Both are no-ops
+// without such a launch.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Cell of the sample at (row entry a, column entry b) for the moments
+// kernels: the column table's integer part already carries the +1 entry
+// offset of the stencil (entry = voxel + 1); e = -1 when no corner of the
+// cell is inside (zero-padding partial: -1 <= p < n on every axis).
+struct SCell {
+  int e;
+  float tx, ty, tz;
+  int ex, ey, ez;
+};
+
+__device__ __forceinline__ SCell sncc_cell(const Stencil& s, int4 ia, float4 fa, int4 ib1, float4 fb) {
+  SCell c;
+  c.tx = fa.x + fb.x;
+  c.ty = fa.y + fb.y;
+  c.tz = fa.z + fb.z;
+  c.ex = ia.x + ib1.x;
+  c.ey = ia.y + ib1.y;
+  c.ez = ia.z + ib1.z;
+  if (c.tx >= 1.f) { c.tx -= 1.f; ++c.ex; }
+  if (c.ty >= 1.f) { c.ty -= 1.f; ++c.ey; }
+  if (c.tz >= 1.f) { c.tz -= 1.f; ++c.ez; }
+  const bool ok = static_cast<unsigned>(c.ex) <= static_cast<unsigned>(s.W) &&
+                  static_cast<unsigned>(c.ey) <= static_cast<unsigned>(s.H) &&
+                  static_cast<unsigned>(c.ez) <= static_cast<unsigned>(s.D);
+  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + 1) + c.ex : -1;
+  return c;
+}
+
+// Entry load of cell c (zeros when e < 0); f16: the brick scale, unapplied.
+template <int DT>
+__device__ __forceinline__ void sncc_load(const Stencil& s, const SCell& c, Raw<DT>& r) {
+  if constexpr (DT == FVR_F32) {
+    if (c.e < 0) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = k0 + u < tiles ? __ldcg(src + (k0 + u) * M_NGRAD) : 0.0;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) sum += x[u];
-      }
-      s_mom[v][m] = sum;
-    } else {
-      const int k = t - nv * M_NGRAD, v = k / 18;
-      s_jac[v][k - v * 18] = __ldcg(a.jac + (static_cast<int64_t>(v) * C + c) * 18 + (k - v * 18));
+      for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      return;
     }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    // ncc per view and dL/dpose: per axis gc (a A + 2 b B) through the Jacobian
-    double ga[3] = {0.0, 0.0, 0.0}, gtx = 0.0, gty = 0.0;
-    const double s3[3] = {a.sx, a.sy, a.sz};
-    for (int v = 0; v < nv; ++v) {
-      double* m = s_mom[v];
-      const double sq = sqrt(m[M_EP] * m[M_ET]);
-      const double inv = 1.0 / (sq + 1e-8);
-      m[17] = m[M_CROSS] * inv;
-      const double bb = sq > 0.0 ? -0.5 * m[M_CROSS] * m[M_ET] * inv * inv / sq : 0.0;
-      const double gc = -(a.g ? static_cast<double>(a.g[v * a.g_stride]) : 1.0) / C;
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const double du = gc * (inv * m[M_AU + i] + 2.0 * bb * m[M_BU + i]) * s3[i];
-        const double dv = gc * (inv * m[M_AV + i] + 2.0 * bb * m[M_BV + i]) * s3[i];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) ga[k] += du * s_jac[v][(k * 2 + 0) * 3 + i] + dv * s_jac[v][(k * 2 + 1) * 3 + i];
-      }
-      gtx += gc * inv * a.kappa * m[M_PHU];
-      gty += gc * inv * a.kappa * m[M_PHV];
-      if (a.ncc_out) a.ncc_out[v * C + c] = static_cast<float>(m[17]);
-      double* out = a.mom + (static_cast<int64_t>(v) * C + c) * kMomStride;
-      for (int k = 0; k < kMomStride; ++k) out[k] = m[k];
+    const float4* p = static_cast<const float4*>(s.data) + static_cast<int64_t>(c.e) * 4;
+    ldg256(p, r.q[0], r.q[1]);
+    ldg256(p + 2, r.q[2], r.q[3]);
+  } else {
+    if (c.e < 0) {
+      r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
+      if constexpr (DT == FVR_F16) r.sc = 0.f;
+      return;
     }
-    float* o = a.grad + 6 * c;
-    const float r[6] = {static_cast<float>(ga[0]), static_cast<float>(ga[1]), static_cast<float>(ga[2]),
-                        static_cast<float>(gtx), static_cast<float>(gty), 0.f};
-    for (int k = 0; k < 6; ++k) o[k] = a.accumulate ? o[k] + r[k] : r[k];
-    a.counters[c] = 0u;  // every ticket of candidate c has been taken
-    // global ticket: the CTA that completes the last candidate forms the losses
-    __threadfence();
-    const bool last = atomicAdd(a.counters + C, 1u) == static_cast<unsigned>(C - 1);
-    if (last) __threadfence();
-    s_last = last;
-  }
-  __syncthreads();
-  if (!s_last || threadIdx.x >= 32) return;
-  // one warp: loss[v] = 1 - mean_c ncc (fixed lane order), loss[nv] = their sum;
-  // every view's loads are issued before any sum
-  double part[kMaxViews] = {0.0, 0.0, 0.0, 0.0};
-  for (int k = threadIdx.x; k < C; k += 32) {
-#pragma unroll
-    for (int v = 0; v < kMaxViews; ++v)
-      if (v < nv) part[v] += __ldcg(a.mom + (static_cast<int64_t>(v) * C + k) * kMomStride + 17);
-  }
-  double total = 0.0;
-#pragma unroll
-  for (int v = 0; v < kMaxViews; ++v) {
-    if (v < nv) {
-      const double l = 1.0 - warp_sum(part[v]) / C;
-      if (threadIdx.x == 0) a.loss[v] = static_cast<float>(l);
-      total += l;
+    ldg256(static_cast<const uint4*>(s.data) + static_cast<int64_t>(c.e) * 2, r.q[0], r.q[1]);
+    if constexpr (DT == FVR_F16) {
+      const unsigned bx = static_cast<unsigned>(s.W + kBrick) / kBrick, by = static_cast<unsigned>(s.H + kBrick) / kBrick;
+      const unsigned ex = static_cast<unsigned>(c.ex) / kBrick, ey = static_cast<unsigned>(c.ey) / kBrick,
+                     ez = static_cast<unsigned>(c.ez) / kBrick;
+      r.sc = __ldg(s.scales + (ez * by + ey) * bx + ex);
     }
-  }
-  if (threadIdx.x == 0) {
-    a.loss[nv] = static_cast<float>(total);
-    a.counters[C] = 0u;
   }
 }
 
-// FUSE: the last CTA to finish a candidate (ticket per candidate) sums its
-// tiles, writes its moments, ncc and pose gradient; the last candidate to
-// finish (global ticket) forms the view losses.  Tickets reset themselves, so
-// the counters stay zero between launches.  No CTA ever waits on another.
-template <int DT, bool GRAD, int GROUP, int MINB, bool FUSE>
+// The per-sample reduction.  With S the interpolated sample, D_k its
+// derivative along axis k, P = e^{i phi} the phase factor, T the target and h
+// the high-pass weight (f16: times the brick scale), and M = h conj(P) T:
+//   cross = S.M    Ep = h^2 S.S    Et = T.T    ph = S x M = Im(conj(S) M)
+//   A_k = M.D_k    B_k = h^2 S.D_k,    (PHU, AU, BU) weighted by ku, (PHV, AV, BV) by kv,
+// where x.y = Re(x conj y).  Pair accumulators hold the two component
+// products in packed (re, im) form; acc.x + acc.y is the moment (acc.y -
+// acc.x for the ph pair, which multiplies (si, sr) by M).
+template <int DT, bool GRAD, int NM>
+__device__ __forceinline__ void sncc_accumulate(const Raw<DT>& raw, float tx, float ty, float tz, float4 ka,
+                                                float4 kb, float2 T, float h, float2 (&acc)[NM]) {
+  Sample8c sm;
+  tab_decode2<DT>(raw, sm);
+  Interp2 o;
+  trilerp2<GRAD>(sm, tx, ty, tz, o);
+  const float cs = ka.z * kb.z - ka.w * kb.w, sn = ka.w * kb.z + ka.z * kb.w;
+  const float htx = h * T.x, hty = h * T.y;
+  const float2 M = make_float2(cs * htx + sn * hty, cs * hty - sn * htx);
+  const float2 hS = mul2(f2(h * h), o.s);
+  acc[M_CROSS] = fma2(o.s, M, acc[M_CROSS]);
+  acc[M_EP] = fma2(hS, o.s, acc[M_EP]);
+  acc[M_ET] = fma2(T, T, acc[M_ET]);
+  if constexpr (GRAD) {
+    const float2 kU = make_float2(ka.x, ka.y), kV = make_float2(kb.x, kb.y);
+    const float2 uM = mul2(kU, M), vM = mul2(kV, M), uH = mul2(kU, hS), vH = mul2(kV, hS);
+    const float2 sw = make_float2(o.s.y, o.s.x);
+    acc[M_PHU] = fma2(sw, uM, acc[M_PHU]);
+    acc[M_PHV] = fma2(sw, vM, acc[M_PHV]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      acc[M_AU + k] = fma2(uM, o.d[k], acc[M_AU + k]);
+      acc[M_AV + k] = fma2(vM, o.d[k], acc[M_AV + k]);
+      acc[M_BU + k] = fma2(uH, o.d[k], acc[M_BU + k]);
+      acc[M_BV + k] = fma2(vH, o.d[k], acc[M_BV + k]);
+    }
+  }
+}
+
+// Rows [row_begin, row_end) of one (candidate, view), column-stationary: the
+// CTA's 256 threads cover min(R, 256) columns x 256 / min(R, 256) rows per
+// pass, so a thread keeps its column's table entry in registers for the
+// whole range and every lane of a warp reads the same row entry (a
+// broadcast).  GROUP rows' loads are in flight before any of them is used.
+// Threads past the last whole column set (R < 256 not dividing 256) idle.
+template <int DT, bool GRAD, int GROUP, int NM>
+__device__ __forceinline__ void sncc_run(const SnccArgs& a, const SnccTab& tab, const float2* __restrict__ ft,
+                                         int row_begin, int row_end, float2 (&acc)[NM]) {
+  const int R = a.R, t = threadIdx.x;
+  const int cpp = min(R, kSnccThreads), rpp = kSnccThreads / cpp;
+  const int r_off = t / cpp;
+  if (r_off >= rpp) return;
+  for (int j = t - r_off * cpp; j < R; j += cpp) {
+    const int4 ib = tab.idx[j];
+    const float4 fb = tab.frac[j], kb = tab.kph[j];
+    for (int i = row_begin + r_off; i < row_end; i += rpp * GROUP) {
+      Raw<DT> raw[GROUP];
+      float hs[GROUP];
+      float2 Ts[GROUP];
+      // issue every load of the group before using any of them
+#pragma unroll
+      for (int g = 0; g < GROUP; ++g) {
+        const int ig = i + g * rpp;
+        const bool ok = ig < row_end;
+        const int rn = R + (ok ? ig : row_begin) - row_begin;
+        SCell cell = sncc_cell(a.st, tab.idx[rn], tab.frac[rn], ib, fb);
+        if (!ok) cell.e = -1;
+        sncc_load<DT>(a.st, cell, raw[g]);
+        const int q = ig * R + j;
+        Ts[g] = ok ? __ldg(ft + q) : make_float2(0.f, 0.f);
+        hs[g] = ok ? (a.hp ? __ldg(a.hp + q) : 1.f) : 0.f;
+      }
+#pragma unroll
+      for (int g = 0; g < GROUP; ++g) {
+        const int ig = i + g * rpp;
+        const int rn = R + (ig < row_end ? ig : row_begin) - row_begin;
+        const float4 fa = tab.frac[rn];
+        float tx = fa.x + fb.x, ty = fa.y + fb.y, tz = fa.z + fb.z;
+        if (tx >= 1.f) tx -= 1.f;
+        if (ty >= 1.f) ty -= 1.f;
+        if (tz >= 1.f) tz -= 1.f;
+        // f16: the brick scale rides on the high-pass weight (every moment is
+        // linear in h S or quadratic in it) instead of rescaling 8 values
+        const float h = DT == FVR_F16 ? hs[g] * raw_scale(raw[g]) : hs[g];
+        sncc_accumulate<DT, GRAD, NM>(raw[g], tx, ty, tz, tab.kph[rn], kb, Ts[g], h, acc);
+      }
+    }
+  }
+}
+
+// Pair accumulators -> CTA moment sums (fp64 across warps), written to record rec.
+template <int NM>
+__device__ __forceinline__ void sncc_store_record(const float2 (&acc)[NM], double* red, double* partial,
+                                                  int64_t rec) {
+  float m[NM];
+#pragma unroll
+  for (int k = 0; k < NM; ++k) m[k] = (k == M_PHU || k == M_PHV) ? acc[k].y - acc[k].x : acc[k].x + acc[k].y;
+  double tot;
+  block_reduce_d<NM, float>(m, red, &tot);
+  if (threadIdx.x < NM) partial[rec * NM + threadIdx.x] = tot;
+}
+
+// Tile grid: CTA (tile, c, v) reduces rows [tile * a.tile_rows, ...) of
+// (candidate c, view v) into one partial record.
+template <int DT, bool GRAD, int GROUP, int MINB>
 __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(SnccArgs a) {
   constexpr int NM = GRAD ? M_NGRAD : 3;
   __shared__ double red[NM * (kSnccThreads / 32)];
   __shared__ double ax_s[8];
   extern __shared__ __align__(16) unsigned char tab_smem[];
   const int tile = blockIdx.x, c = blockIdx.y, v = blockIdx.z;
-  // select the view's parameters without dynamic indexing of the parameter space
-  const int lateral = v == 0 ? a.lateral[0] : v == 1 ? a.lateral[1] : v == 2 ? a.lateral[2] : a.lateral[3];
-  const float2* __restrict__ ft = v == 0 ? a.ftarg[0] : v == 1 ? a.ftarg[1] : v == 2 ? a.ftarg[2] : a.ftarg[3];
-  const int R = a.R, K = R * R;
-  const int q_begin = tile * a.tile;
-  const int q_end = min(q_begin + a.tile, K);
-  const int row0 = q_begin / R;
-  const AxisTables tab = axis_tables(tab_smem, R + a.tab_rows);
-  if (threadIdx.x == 0) {
-    if (FUSE && GRAD) {
-      double jac[18];
-      slice_axes_jac(a.poses + 6 * c, lateral, a.sx, a.sy, a.sz, ax_s, jac);
-      if (tile == 0)  // one CTA per (view, candidate) stores the axes Jacobian for the epilogue
-        for (int k = 0; k < 18; ++k) a.jac[(static_cast<int64_t>(v) * a.C + c) * 18 + k] = jac[k];
-    } else {
-      slice_axes(a.poses + 6 * c, lateral, a.sx, a.sy, a.sz, ax_s);
-    }
-  }
+  const int R = a.R;
+  const int row_begin = tile * a.tile_rows;
+  const int row_end = min(row_begin + a.tile_rows, R);
+  const SnccTab tab = sncc_tab(tab_smem, R + a.tile_rows);
+  pdl_launch_dependents();
+  if (threadIdx.x == 0) sncc_item_axes(a, v, c, ax_s);
   __syncthreads();
-  build_axis_tables(tab, R, row0, (q_end - 1) / R - row0 + 1, a.lin, ax_s, a.sx, a.sy, a.sz, a.kpi);
+  build_sncc_tables(tab, R, row_begin, row_end - row_begin, a.lin, ax_s, a.sx, a.sy, a.sz, a.kpi);
   __syncthreads();
-  float acc[NM];  // per-thread partial over ~K*C*nv/(2*SMs*256) samples
+  float2 acc[NM];
 #pragma unroll
-  for (int m = 0; m < NM; ++m) acc[m] = 0.f;
-
-  // this thread's samples: q = q_begin + threadIdx.x + 256 m, (i, j) = divmod(q, R)
-  const int di = kSnccThreads / R, dj = kSnccThreads - di * R;
-  int q = q_begin + threadIdx.x;
-  int i = q / R, j = q - i * R;
-  while (q < q_end) {
-    Raw<DT> raw[GROUP];
-    int rc[GROUP];  // row entry << 16 | column entry
-    float hs[GROUP];
-    float2 Ts[GROUP];
-    // issue every load of the group before using any of them; only the loads
-    // and the table entries stay live, positions and phases are re-derived
-#pragma unroll
-    for (int g = 0; g < GROUP; ++g) {
-      const bool ok = q < q_end;
-      const int rn = ok ? R + i - row0 : 0, cn = ok ? j : 0;
-      rc[g] = (rn << 16) | cn;
-      TabCell cell = tab_cell(a.st, tab.idx[rn], tab.frac[rn], tab.idx[cn], tab.frac[cn]);
-      if (!ok) cell.e = -1;
-      tab_load<DT>(a.st, cell, raw[g]);
-      Ts[g] = ok ? __ldg(ft + q) : make_float2(0.f, 0.f);
-      hs[g] = ok ? (a.hp ? __ldg(a.hp + q) : 1.f) : 0.f;
-      q += kSnccThreads;
-      i += di;
-      j += dj;
-      if (j >= R) {
-        j -= R;
-        ++i;
-      }
-    }
-#pragma unroll
-    for (int g = 0; g < GROUP; ++g) {
-      const int rn = rc[g] >> 16, cn = rc[g] & 0xffff;
-      const float4 fa = tab.frac[rn], fb = tab.frac[cn];
-      const float2 pa = tab.ph[rn], pb = tab.ph[cn];
-      float tx = fa.x + fb.x, ty = fa.y + fb.y, tz = fa.z + fb.z;
-      if (tx >= 1.f) tx -= 1.f;
-      if (ty >= 1.f) ty -= 1.f;
-      if (tz >= 1.f) tz -= 1.f;
-      Sample8 sm;
-      tab_decode<DT>(raw[g], sm);
-      Interp o;
-      trilerp<GRAD>(sm, tx, ty, tz, o);
-      // f16: the brick scale rides on the high-pass weight (every moment is
-      // linear in h S or quadratic in it) instead of rescaling 8 values
-      const float ku = fa.w, kv = fb.w, h = DT == FVR_F16 ? hs[g] * raw_scale(raw[g]) : hs[g];
-      const float cs = pa.x * pb.x - pa.y * pb.y, sn = pa.y * pb.x + pa.x * pb.y;
-      const float2 T = Ts[g];
-      const float shr = h * (o.sr * cs - o.si * sn);
-      const float shi = h * (o.sr * sn + o.si * cs);
-      acc[M_CROSS] = fmaf(shr, T.x, fmaf(shi, T.y, acc[M_CROSS]));
-      acc[M_EP] = fmaf(shr, shr, fmaf(shi, shi, acc[M_EP]));
-      acc[M_ET] = fmaf(T.x, T.x, fmaf(T.y, T.y, acc[M_ET]));
-      if constexpr (GRAD) {
-        // dL/dphi direction: Re(conj(T) i S_hat) = T.y*shr - T.x*shi
-        const float ph = T.y * shr - T.x * shi;
-        acc[M_PHU] += ku * ph;
-        acc[M_PHV] += kv * ph;
-        // M_T = h e^{-i phi} T ;  A_k = <M_T, dS/dp_k> ;  B_k = h^2 <S, dS/dp_k>
-        const float mtr = h * (cs * T.x + sn * T.y);
-        const float mti = h * (cs * T.y - sn * T.x);
-        const float h2 = h * h;
-        const float a0 = mtr * o.dxr + mti * o.dxi, a1 = mtr * o.dyr + mti * o.dyi, a2 = mtr * o.dzr + mti * o.dzi;
-        const float b0 = h2 * (o.sr * o.dxr + o.si * o.dxi), b1 = h2 * (o.sr * o.dyr + o.si * o.dyi),
-                    b2 = h2 * (o.sr * o.dzr + o.si * o.dzi);
-        acc[M_AU + 0] += ku * a0;
-        acc[M_AU + 1] += ku * a1;
-        acc[M_AU + 2] += ku * a2;
-        acc[M_AV + 0] += kv * a0;
-        acc[M_AV + 1] += kv * a1;
-        acc[M_AV + 2] += kv * a2;
-        acc[M_BU + 0] += ku * b0;
-        acc[M_BU + 1] += ku * b1;
-        acc[M_BU + 2] += ku * b2;
-        acc[M_BV + 0] += kv * b0;
-        acc[M_BV + 1] += kv * b1;
-        acc[M_BV + 2] += kv * b2;
-      }
-    }
-  }
-  double tot;
-  block_reduce_d<NM, float>(acc, red, &tot);
-  if (threadIdx.x < NM)
-    a.partial[((static_cast<int64_t>(v) * a.C + c) * gridDim.x + tile) * NM + threadIdx.x] = tot;
-  if constexpr (FUSE && GRAD) sncc_fused_epilogue(a, c);
+  for (int m = 0; m < NM; ++m) acc[m] = make_float2(0.f, 0.f);
+  sncc_run<DT, GRAD, GROUP, NM>(a, tab, view_target(a, v), row_begin, row_end, acc);
+  sncc_store_record<NM>(acc, red, a.partial, (static_cast<int64_t>(v) * a.C + c) * gridDim.x + tile);
 }
 
-// Tile sums (fp64, fixed order) -> mom[v][c][0..NM), ncc in mom[v][c][17];
+// Value-and-gradient epilogue, launched right after the moments kernel as its
+// programmatic dependent (one CTA of 1024 threads): the slice-axes Jacobians
+// per (view, candidate) are formed while the moments kernel still runs; after
+// griddepcontrol.wait, every item's records are summed in fp64 in record
+// order, then one thread per candidate forms its per-view ncc and pose
+// gradient (per axis gc (a A + 2 b B) through the Jacobian, translations from
+// the phase moments), and the view losses are reduced in a fixed order.
+constexpr int kFinalThreads = 1024;
+
+__global__ void __launch_bounds__(kFinalThreads) tc_sncc_final_kernel(SnccArgs a) {
+  __shared__ double red[kMaxViews][kFinalThreads / 32];
+  const int t = threadIdx.x, nv = a.nv, C = a.C;
+  const int64_t items = static_cast<int64_t>(nv) * C;
+  for (int64_t k = t; k < items; k += kFinalThreads) {
+    const int v = static_cast<int>(k / C), c = static_cast<int>(k - static_cast<int64_t>(v) * C);
+    double ax[8], jac[18];
+    slice_axes_jac(a.poses + 6 * c, view_lateral(a, v), a.sx, a.sy, a.sz, ax, jac);
+    for (int m = 0; m < 18; ++m) a.jac[k * 18 + m] = jac[m];
+  }
+  pdl_wait();
+  // record sums: four (item, moment) pairs per thread and pass, two records
+  // of each in flight per round
+  const int64_t npairs = items * M_NGRAD;
+  for (int64_t p0 = t; p0 < npairs; p0 += 4 * kFinalThreads) {
+    int64_t st[4];
+    int n[4], nmax = 0;
+    double sum[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int64_t p = p0 + u * kFinalThreads;
+      n[u] = 0;
+      st[u] = 0;
+      sum[u] = 0.0;
+      if (p < npairs) {
+        st[u] = (p / M_NGRAD) * a.tiles * M_NGRAD + p % M_NGRAD;
+        n[u] = a.tiles;
+        nmax = max(nmax, n[u]);
+      }
+    }
+    for (int k0 = 0; k0 < nmax; k0 += 2) {
+      double x[4][2];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk)
+          x[u][kk] = k0 + kk < n[u] ? __ldcg(a.partial + st[u] + static_cast<int64_t>(k0 + kk) * M_NGRAD) : 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) sum[u] += x[u][0] + x[u][1];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int64_t p = p0 + u * kFinalThreads;
+      if (p < npairs) a.mom[(p / M_NGRAD) * kMomStride + p % M_NGRAD] = sum[u];
+    }
+  }
+  __syncthreads();
+  double lsum[kMaxViews] = {0.0, 0.0, 0.0, 0.0};
+  const double s3[3] = {a.sx, a.sy, a.sz};
+  for (int c = t; c < C; c += kFinalThreads) {
+    double ga[3] = {0.0, 0.0, 0.0}, gtx = 0.0, gty = 0.0;
+    for (int v = 0; v < nv; ++v) {
+      const int64_t it = static_cast<int64_t>(v) * C + c;
+      double m[M_NGRAD];
+#pragma unroll
+      for (int k = 0; k < M_NGRAD; ++k) m[k] = __ldcg(a.mom + it * kMomStride + k);
+      const double sq = sqrt(m[M_EP] * m[M_ET]);
+      const double inv = 1.0 / (sq + 1e-8);
+      const double ncc = m[M_CROSS] * inv;
+      const double bb = sq > 0.0 ? -0.5 * m[M_CROSS] * m[M_ET] * inv * inv / sq : 0.0;
+      const double gc = -(a.g ? static_cast<double>(a.g[v * a.g_stride]) : 1.0) / C;
+      const double* jac = a.jac + it * 18;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const double du = gc * (inv * m[M_AU + i] + 2.0 * bb * m[M_BU + i]) * s3[i];
+        const double dv = gc * (inv * m[M_AV + i] + 2.0 * bb * m[M_BV + i]) * s3[i];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ga[k] += du * __ldcg(jac + (k * 2 + 0) * 3 + i) + dv * __ldcg(jac + (k * 2 + 1) * 3 + i);
+      }
+      gtx += gc * inv * a.kappa * m[M_PHU];
+      gty += gc * inv * a.kappa * m[M_PHV];
+      a.mom[it * kMomStride + 17] = ncc;
+      if (a.ncc_out) a.ncc_out[it] = static_cast<float>(ncc);
+      if (v == 0) lsum[0] += ncc;
+      else if (v == 1) lsum[1] += ncc;
+      else if (v == 2) lsum[2] += ncc;
+      else lsum[3] += ncc;
+    }
+    float* o = a.grad + 6 * c;
+    const float r[6] = {static_cast<float>(ga[0]), static_cast<float>(ga[1]), static_cast<float>(ga[2]),
+                        static_cast<float>(gtx), static_cast<float>(gty), 0.f};
+    for (int k = 0; k < 6; ++k) o[k] = a.accumulate ? o[k] + r[k] : r[k];
+  }
+  // loss[v] = 1 - mean_c ncc (fixed order: per thread, per warp, across warps)
+  const int lane = t & 31, w = t >> 5;
+#pragma unroll
+  for (int v = 0; v < kMaxViews; ++v) {
+    const double s = warp_sum(lsum[v]);
+    if (lane == 0) red[v][w] = s;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double total = 0.0;
+    for (int v = 0; v < nv; ++v) {
+      double s = 0.0;
+      for (int k = 0; k < kFinalThreads / 32; ++k) s += red[v][k];
+      const double l = 1.0 - s / C;
+      a.loss[v] = static_cast<float>(l);
+      total += l;
+    }
+    a.loss[nv] = static_cast<float>(total);
+  }
+}
+
+// Launch the epilogue as a programmatic dependent of the kernel before it on
+// the stream (plain launch where the attribute is refused).
+static void launch_sncc_final(cudaStream_t s, const SnccArgs& a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(1);
+  cfg.blockDim = dim3(kFinalThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, tc_sncc_final_kernel, a) != cudaSuccess) {
+    (void)cudaGetLastError();
+    tc_sncc_final_kernel<<<1, kFinalThreads, 0, s>>>(a);
+  }
+}
+
+// Record sums (fp64, fixed order) -> mom[v][c][0..NM), ncc in mom[v][c][17];
 // loss[v] = 1 - mean_c ncc, loss[nv] = sum_v loss[v].  One CTA, warp per (v, c).
 __global__ void __launch_bounds__(1024) tc_sncc_finalize_kernel(const double* __restrict__ partial, int C, int nv,
                                                                 int tiles, int NM, double* __restrict__ mom,
@@ -627,47 +758,61 @@ static int stencil_from(int dtype, const void* data, const float* scales, int64_
 
 static double half_extent(int64_t n) { return 0.5 * static_cast<double>(n > 1 ? n - 1 : 1); }
 
-// Samples per CTA: one wave of min_blocks resident CTAs per SM (never more
-// CTAs than slots), at least 256 samples (one per thread) per CTA.
-static int sncc_tile(int64_t C, int64_t K, int nv, int variant) {
+static int device_sms() {
   static int sms = 0;
   if (sms == 0) {
-    int dev = 0;
+    int dev = 0, n = 0;
     cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    sms = (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0) ? n : 148;
   }
-  const SnccVariant v = sncc_variant(variant);
-  const int64_t items = C * nv;
-  int64_t tiles = (static_cast<int64_t>(v.min_blocks) * sms) / items;
-  const int64_t max_tiles = cdiv64(K, kSnccThreads);
-  if (tiles > max_tiles) tiles = max_tiles;
-  if (tiles < 1) tiles = 1;
-  return static_cast<int>(cdiv64(K, tiles));
+  return sms;
 }
 
-// Row-table entries and dynamic shared memory of one moments CTA.
-static int sncc_tab_rows(int64_t R, int tile) { return static_cast<int>(tile / R + 2); }
-static int64_t sncc_smem(int64_t R, int tile) { return (R + sncc_tab_rows(R, tile)) * 40; }
+// Grid and tables of one moments launch: one wave of min_blocks resident
+// CTAs per SM split over the (candidate, view) items in whole slice rows
+// (never more CTAs than slots), at least 256 samples per CTA.
+struct SnccPlan {
+  dim3 grid;
+  int tile_rows, tiles;
+};
+
+static SnccPlan sncc_plan(int64_t C, int64_t R, int nv, int variant) {
+  const SnccVariant v = sncc_variant(variant);
+  const int64_t items = C * nv, min_rows = cdiv64(kSnccThreads, R);
+  int64_t tiles = (static_cast<int64_t>(v.min_blocks) * device_sms()) / items;
+  tiles = std::max<int64_t>(1, std::min(tiles, R / min_rows));
+  const int64_t tile_rows = cdiv64(R, tiles);
+  tiles = cdiv64(R, tile_rows);
+  SnccPlan p{};
+  p.grid = dim3(static_cast<unsigned>(tiles), static_cast<unsigned>(C), static_cast<unsigned>(nv));
+  p.tile_rows = static_cast<int>(tile_rows);
+  p.tiles = static_cast<int>(tiles);
+  return p;
+}
+
+// Dynamic shared memory: the tables (R columns + tile rows).
+static int64_t sncc_smem(int64_t R, int tile_rows) { return (R + tile_rows) * kSnccTabEntryBytes; }
 constexpr int64_t kSnccMaxSmem = 200 * 1024;
 
-template <int DT, bool GRAD, int GROUP, int MINB, bool FUSE>
-static void launch_sncc_v(dim3 grid, int smem, cudaStream_t s, const SnccArgs& a) {
-  auto k = tc_sncc_moments_kernel<DT, GRAD, GROUP, MINB, FUSE>;
+template <int DT, bool GRAD, int VI>
+static void launch_sncc_v(dim3 grid, int smem, cudaStream_t st, const SnccArgs& a) {
+  constexpr SnccVariant v = sncc_variant(VI);
+  auto k = tc_sncc_moments_kernel<DT, GRAD, v.group, v.min_blocks>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  k<<<grid, kSnccThreads, smem, s>>>(a);
+  k<<<grid, kSnccThreads, smem, st>>>(a);
 }
 
-template <int DT, bool GRAD, bool FUSE = false>
+template <int DT, bool GRAD>
 static void launch_sncc(int variant, dim3 grid, int smem, cudaStream_t s, const SnccArgs& a) {
   switch (variant) {
-    case 1: launch_sncc_v<DT, GRAD, 2, 4, FUSE>(grid, smem, s, a); break;
-    case 2: launch_sncc_v<DT, GRAD, 4, 3, FUSE>(grid, smem, s, a); break;
-    case 3: launch_sncc_v<DT, GRAD, 8, 1, FUSE>(grid, smem, s, a); break;
-    case 4: launch_sncc_v<DT, GRAD, 2, 3, FUSE>(grid, smem, s, a); break;
-    case 5: launch_sncc_v<DT, GRAD, 3, 3, FUSE>(grid, smem, s, a); break;
-    default: launch_sncc_v<DT, GRAD, 4, 2, FUSE>(grid, smem, s, a); break;
+#define FVR_V(n) \
+  case n: launch_sncc_v<DT, GRAD, n>(grid, smem, s, a); break;
+    FVR_V(0) FVR_V(1) FVR_V(2) FVR_V(3) FVR_V(4) FVR_V(5) FVR_V(6) FVR_V(7)
+#undef FVR_V
+    default: break;
   }
 }
+static_assert(kSnccVariants == 8, "launch_sncc lists every variant");
 
 // Shared argument set-up of the moments launches.
 static int sncc_setup(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
@@ -681,8 +826,7 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
   if (nviews < 1 || nviews > kMaxViews || R * R > (int64_t)1 << 30) return FVR_ERR_ARG;
   if (variant < 0 || variant >= kSnccVariants) return FVR_ERR_ARG;
   if ((D + 1) * (H + 1) * (W + 1) > INT32_MAX) return FVR_ERR_UNSUPPORTED;  // 32-bit entry index
-  const int64_t K = R * R;
-  const int tile = sncc_tile(C, K, nviews, variant);
+  const SnccPlan plan = sncc_plan(C, R, nviews, variant);
   *a = SnccArgs{};
   a->st = st;
   a->poses = poses;
@@ -695,16 +839,17 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
   a->lin = lin;
   a->R = (int)R;
   a->C = (int)C;
-  a->tile = tile;
-  a->tab_rows = sncc_tab_rows(R, tile);
-  *smem = sncc_smem(R, tile);
+  a->nv = nviews;
+  a->tile_rows = plan.tile_rows;
+  a->tiles = plan.tiles;
+  *smem = sncc_smem(R, plan.tile_rows);
   if (*smem > kSnccMaxSmem) return FVR_ERR_UNSUPPORTED;
   a->kpi = kappa / 3.14159265358979323846;
   a->kappa = kappa;
   a->sx = half_extent(W);
   a->sy = half_extent(H);
   a->sz = half_extent(D);
-  *grid = dim3(static_cast<unsigned>(cdiv64(K, tile)), static_cast<unsigned>(C), static_cast<unsigned>(nviews));
+  *grid = plan.grid;
   return FVR_OK;
 }
 
@@ -719,17 +864,15 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
 // an allocator between steps (cudaMalloc / cudaFree may synchronise the
 // device).
 //
-// Size (about 428 KB per device): kStaticRecords partial-moment records of
-// 17 doubles, kStaticItems (candidate, view) moment records and axes
-// Jacobians of 18 doubles each, and kStaticItems + 1 ticket counters.  Calls
-// needing more -- more than 512 (candidate, view) pairs, or more than 2048
-// (candidate, view, tile) partial records for the launch variant -- are
-// refused with FVR_ERR_WORKSPACE before anything is launched.
+// Size (about 426 KB per device): kStaticRecords partial-moment records of
+// 17 doubles, and kStaticItems (candidate, view) moment records and axes
+// Jacobians of 18 doubles each.  Calls needing more -- more than 512
+// (candidate, view) pairs, or more than 2048 partial records for the launch
+// variant (sncc_records) -- are refused with FVR_ERR_WORKSPACE before
+// anything is launched.
 //
-// Start state: the ticket counters must be zero before a launch; the static
-// initialiser zeroes them and every completed launch leaves them zero.  The
-// partial, moment and Jacobian records are written by every launch before
-// they are read, so nothing else needs to start at zero.
+// Start state: none.  The partial, moment and Jacobian records are written
+// by every call before they are read.
 //
 // Set-up: the first call on each device, made with that device current,
 // resolves the array's device address with cudaGetSymbolAddress and caches
@@ -738,16 +881,14 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
 // Races: one array per device is shared by every caller in the process.
 // Calls on the same device must be ordered (one stream, or explicit
 // synchronisation); two calls that overlap in time corrupt each other's
-// scratch and tickets.
+// scratch.
 // ----------------------------------------------------------------------------
 constexpr int64_t kStaticItems = 512;
 constexpr int64_t kStaticRecords = 2048;
 constexpr int64_t kStaticPartialDoubles = kStaticRecords * M_NGRAD;
 constexpr int64_t kStaticMomDoubles = kStaticItems * kMomStride;
 constexpr int64_t kStaticJacDoubles = kStaticItems * 18;
-constexpr int64_t kStaticTicketDoubles = (kStaticItems + 1 + 1) / 2;  // unsigned counters, two per double
-constexpr int64_t kStaticDoubles = kStaticPartialDoubles + kStaticMomDoubles + kStaticJacDoubles +
-                                   kStaticTicketDoubles;
+constexpr int64_t kStaticDoubles = kStaticPartialDoubles + kStaticMomDoubles + kStaticJacDoubles;
 constexpr int kStaticMaxDevices = 64;
 
 static __device__ __align__(256) double g_sncc_static_scratch[kStaticDoubles];
@@ -786,6 +927,7 @@ int fvr_tc_axes(const float* poses, int64_t C, int view, int64_t D, int64_t H, i
   return FVR_OK;
 }
 
+// Partial records: at most ceil(K / 256) tiles per (candidate, view).
 int64_t fvr_tc_sncc_workspace(int64_t C, int64_t R, int64_t nviews) {
   return nviews * C * cdiv64(R * R, kSnccThreads) * M_NGRAD * (int64_t)sizeof(double);
 }
@@ -825,11 +967,10 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
 }
 
 // Fused workspace: partial records | moments [nv][C][18] | axes Jacobians
-// [nv][C][18] | tickets [C + 1] (the last region must start zeroed).
+// [nv][C][18]; every region is written by a call before it is read.
 int64_t fvr_tc_sncc_fused_workspace(int64_t C, int64_t R, int64_t nviews) {
   if (C < 1 || R < 1 || nviews < 1) return 0;
-  return fvr_tc_sncc_workspace(C, R, nviews) + 2 * nviews * C * kMomStride * (int64_t)sizeof(double) +
-         cdiv64((C + 1) * (int64_t)sizeof(unsigned), 256) * 256;
+  return fvr_tc_sncc_workspace(C, R, nviews) + 2 * nviews * C * kMomStride * (int64_t)sizeof(double);
 }
 
 int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
@@ -852,7 +993,6 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
   const int64_t mom_bytes = nviews * C * kMomStride * (int64_t)sizeof(double);
   a.mom = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews));
   a.jac = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews) + mom_bytes);
-  a.counters = reinterpret_cast<unsigned*>(ws + fvr_tc_sncc_workspace(C, R, nviews) + 2 * mom_bytes);
   a.loss = loss;
   a.ncc_out = ncc_out;
   a.grad = grad_poses;
@@ -861,10 +1001,12 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
   a.accumulate = accumulate;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (dtype) {
-    case FVR_F32: launch_sncc<FVR_F32, true, true>(variant, grid, (int)smem, s, a); break;
-    case FVR_BF16: launch_sncc<FVR_BF16, true, true>(variant, grid, (int)smem, s, a); break;
-    case FVR_F16: launch_sncc<FVR_F16, true, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_F32: launch_sncc<FVR_F32, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_BF16: launch_sncc<FVR_BF16, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a); break;
   }
+  FVR_LAUNCH_CHECK();
+  launch_sncc_final(s, a);
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }
@@ -873,10 +1015,9 @@ int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews
                          double* mom, float* loss, float* ncc_out, void* stream) {
   if (!workspace || !mom || !loss || C < 1 || R < 1 || nviews < 1 || nviews > kMaxViews) return FVR_ERR_ARG;
   if (variant < 0 || variant >= kSnccVariants) return FVR_ERR_ARG;
-  const int64_t K = R * R;
-  const int tiles = static_cast<int>(cdiv64(K, sncc_tile(C, K, nviews, variant)));
+  const SnccPlan plan = sncc_plan(C, R, nviews, variant);
   tc_sncc_finalize_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(
-      static_cast<const double*>(workspace), (int)C, nviews, tiles, with_grad ? M_NGRAD : 3, mom, loss, ncc_out);
+      static_cast<const double*>(workspace), (int)C, nviews, plan.tiles, with_grad ? M_NGRAD : 3, mom, loss, ncc_out);
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }
@@ -977,14 +1118,13 @@ int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const floa
   if (rc) return rc;
   if (!loss || !grad_poses) return FVR_ERR_ARG;
   const int64_t items = C * nviews;
-  if (items > kStaticItems || items * static_cast<int64_t>(grid.x) > kStaticRecords) return FVR_ERR_WORKSPACE;
+  if (items > kStaticItems || items * a.tiles > kStaticRecords) return FVR_ERR_WORKSPACE;
   double* scratch = nullptr;
   rc = static_scratch(&scratch);
   if (rc) return rc;
   a.partial = scratch;
   a.mom = scratch + kStaticPartialDoubles;
   a.jac = scratch + kStaticPartialDoubles + kStaticMomDoubles;
-  a.counters = reinterpret_cast<unsigned*>(scratch + kStaticPartialDoubles + kStaticMomDoubles + kStaticJacDoubles);
   a.loss = loss;
   a.ncc_out = ncc_out;
   a.grad = grad_poses;
@@ -993,10 +1133,12 @@ int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const floa
   a.accumulate = accumulate;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (dtype) {
-    case FVR_F32: launch_sncc<FVR_F32, true, true>(variant, grid, (int)smem, s, a); break;
-    case FVR_BF16: launch_sncc<FVR_BF16, true, true>(variant, grid, (int)smem, s, a); break;
-    case FVR_F16: launch_sncc<FVR_F16, true, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_F32: launch_sncc<FVR_F32, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_BF16: launch_sncc<FVR_BF16, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a); break;
   }
+  FVR_LAUNCH_CHECK();
+  launch_sncc_final(s, a);
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }

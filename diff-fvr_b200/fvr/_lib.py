@@ -142,6 +142,8 @@ KERNELS_PER_CALL = {
     "fvr_np_ncc_moments": 2,
     "fvr_np_pair_moments": 2,
     "fvr_edge_ncc_forward": 2,
+    "fvr_tc_sncc_value_and_grad": 2,
+    "fvr_tc_sncc_value_and_grad_static": 2,
 }
 launch_count = [0]
 

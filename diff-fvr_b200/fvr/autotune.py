@@ -2,7 +2,8 @@
 
 On the first call for a new shape key, every launch variant the library
 offers is timed with CUDA events (after one warm-up launch each) and the
-fastest is cached for the process.  Inside CUDA-graph capture (where nothing
+fastest is cached for the process (a variant the library refuses for the
+shape is skipped).  Inside CUDA-graph capture (where nothing
 can be timed) a cached choice or variant 0 is used; ``FVR_SNCC_VARIANT``
 pins a variant.
 """
@@ -30,7 +31,11 @@ def choose(kind, key, run, n_variants, reps=3):
         return 0
     best, best_ms, times = 0, float("inf"), []
     for v in range(n_variants):
-        run(v)
+        try:
+            run(v)
+        except L.FvrError:  # this shape does not fit the variant (e.g. its shared memory)
+            times.append(float("inf"))
+            continue
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         for _ in range(reps):

@@ -16,34 +16,62 @@ from . import _lib as L
 class GraphedCallable:
     """Capture ``fn(*static_inputs)`` in one CUDA graph; calling copies the new
     inputs into the static buffers and replays.  Outputs are the static output
-    tensors of the capture (overwritten by the next call)."""
+    tensors of the capture (overwritten by the next call).
 
-    def __init__(self, fn, *example_inputs, warmup=3, capture_context=None):
+    With ``host_io=True`` the graph also holds the transfers: pinned host
+    input buffers (``host_in``) are copied to the device, ``fn`` runs, and its
+    outputs are copied into pinned host buffers (``host_out``), so one replay
+    is the whole host-to-host step.  Calling then takes host tensors (or
+    writes nothing when given ``host_in`` itself), replays, and returns
+    ``host_out`` after waiting for the stream (``sync=False``: without
+    waiting; ``host_out`` is complete once the current stream is)."""
+
+    def __init__(self, fn, *example_inputs, warmup=3, capture_context=None, host_io=False):
         import contextlib
 
         for x in example_inputs:
             L.require_cuda(x)
         self.fn = fn
+        self.host_io = bool(host_io)
         self.static_in = [x.detach().clone() for x in example_inputs]
         side = torch.cuda.Stream()
         side.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(side):
             for _ in range(max(1, int(warmup))):
-                fn(*self.static_in)
+                out = fn(*self.static_in)
         torch.cuda.current_stream().wait_stream(side)
         torch.cuda.synchronize()
+        if self.host_io:
+            outs = out if isinstance(out, (tuple, list)) else (out,)
+            self.host_in = [torch.empty(x.shape, dtype=x.dtype).pin_memory() for x in self.static_in]
+            self.host_out = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in outs]
         self.graph = torch.cuda.CUDAGraph()
         n0 = L.launch_count[0]
         with capture_context if capture_context is not None else contextlib.nullcontext():
             with torch.cuda.graph(self.graph):
+                if self.host_io:
+                    for s, h in zip(self.static_in, self.host_in):
+                        s.copy_(h, non_blocking=True)
                 self.static_out = fn(*self.static_in)
+                if self.host_io:
+                    outs = self.static_out if isinstance(self.static_out, (tuple, list)) else (self.static_out,)
+                    for h, o in zip(self.host_out, outs):
+                        h.copy_(o, non_blocking=True)
         self.kernels_per_replay = L.launch_count[0] - n0
 
     def replay(self):
         self.graph.replay()
         return self.static_out
 
-    def __call__(self, *inputs):
+    def __call__(self, *inputs, sync=True):
+        if self.host_io:
+            for h, x in zip(self.host_in, inputs):
+                if x.data_ptr() != h.data_ptr():
+                    h.copy_(x)
+            self.graph.replay()
+            if sync:
+                torch.cuda.current_stream().synchronize()
+            return tuple(self.host_out) if len(self.host_out) > 1 else self.host_out[0]
         for s, x in zip(self.static_in, inputs):
             s.copy_(x, non_blocking=True)
         return self.replay()
@@ -59,11 +87,15 @@ class BiplanarSpectralNCCStep:
     With ``graph=True`` (default) the whole step is a single CUDA-graph replay
     that uses the engine's spectrum storage of the time of capture (the step
     keeps that storage alive; capture again after ``to_precision``).
-    Returns ``(loss, grad)`` device tensors (scalar, ``[C, 6]``).
+    Returns ``(loss, grad)`` device tensors (scalar, ``[C, 6]``).  With
+    ``host_io=True`` (graph only) the step takes host poses and returns pinned
+    host ``(loss, grad)`` tensors: the host-to-device copy, the kernels and the
+    device-to-host copies are one graph replay (``host_poses`` is the pinned
+    input buffer; writing poses there directly skips one host copy).
     """
 
     def __init__(self, engine, f_targ_ap, f_targ_lat, n_candidates, high_pass=True, cutoff_sigma=4.0, graph=True,
-                 warmup=3, capture_context=None):
+                 warmup=3, capture_context=None, host_io=False):
         self.engine = engine
         self._stencil = engine._stencil
         self.f_ap = f_targ_ap
@@ -71,13 +103,17 @@ class BiplanarSpectralNCCStep:
         self.hp = bool(high_pass)
         self.sigma = float(cutoff_sigma)
         ex = torch.zeros((int(n_candidates), 6), dtype=torch.float32, device=engine._dev)
-        self._g = GraphedCallable(self._step, ex, warmup=warmup, capture_context=capture_context) if graph else None
+        self._g = (GraphedCallable(self._step, ex, warmup=warmup, capture_context=capture_context, host_io=host_io)
+                   if graph else None)
+        io = graph and host_io
+        self.host_poses = self._g.host_in[0] if io else None
+        self.host_loss, self.host_grad = self._g.host_out if io else (None, None)
 
     def _step(self, poses):
         return self.engine.spectral_ncc_value_and_grad(poses, (self.f_ap, self.f_lat), ("ap", "lateral"),
                                                        high_pass=self.hp, cutoff_sigma=self.sigma)
 
-    def __call__(self, poses):
+    def __call__(self, poses, sync=True):
         if self._g is None:
             return self._step(poses.to(self.engine._dev))
-        return self._g(poses)
+        return self._g(poses, sync=sync) if self._g.host_io else self._g(poses)

@@ -76,11 +76,10 @@ def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
 
 
 def _sncc_fused(eng, p, views, ftargs, hp, R, out=None):
-    """One launch: moments, per-candidate finalize and pose gradient, view losses.
-    Returns (loss [nv + 1] f32, grad [C, 6] f32).  The workspace (with its
-    self-resetting ticket region, zeroed once here) is cached per shape on the
-    engine, so captured graphs keep a stable pointer; launches sharing it are
-    ordered on the engine's stream."""
+    """Moments kernel + its dependent epilogue: per-candidate finalize and pose
+    gradient, view losses.  Returns (loss [nv + 1] f32, grad [C, 6] f32).  The
+    workspace is cached per shape on the engine, so captured graphs keep a
+    stable pointer; launches sharing it are ordered on the engine's stream."""
     dev = eng._dev
     C = int(p.shape[0])
     nv = len(views)
@@ -311,7 +310,7 @@ class TorchDiffFVREngine(nn.Module):
         del spec
         self.register_buffer("f_vol_5d", planar.to(dtype=dtype))
         self._stencil = RT.Stencil(self.f_vol_5d[0], True, self.pad_shape, self._stencil_dtype(dtype))
-        self._fused_ws = {}  # (C, R, views, device) -> workspace of the single-launch value_and_grad
+        self._fused_ws = {}  # (C, R, views, device) -> workspace of the fused value_and_grad
 
     @staticmethod
     def _stencil_dtype(dtype):

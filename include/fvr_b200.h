@@ -118,11 +118,12 @@ int64_t fvr_tc_sncc_mom_stride(void);
  * (within 2^-24 of a cell of the fp64 position), applies the phase ramp
  * kappa*(ku tx + kv ty) (per-row x per-column factors from fp64 sincospi) and
  * the high-pass table hp (NULL = none), and reduces the NCC moments; with
- * with_grad also the 14 pose-gradient moments.  Per-tile partial sums go to
- * `workspace`.  lin = torch.linspace(-1, 1, R).  `variant` in
- * [0, fvr_tc_sncc_variants()) selects the launch shape (samples in flight per
- * thread, resident CTAs per SM); results do not depend on it beyond fp64
- * summation order.
+ * with_grad also the 14 pose-gradient moments.  Partial sums (one record per
+ * CTA and (candidate, view) it covers) go to `workspace`.
+ * lin = torch.linspace(-1, 1, R).  `variant` in [0, fvr_tc_sncc_variants())
+ * selects the launch shape (tile grid or one equal sample range per resident
+ * CTA, samples in flight per thread, resident CTAs per SM); results do not
+ * depend on it beyond float summation order.
  * Replaces TorchDiffFVREngine._spectral_ncc_core / forward_spectral_ncc,
  * src/fvr/torch_engine.py:269-307 (the gather of :176-234 included). */
 int fvr_tc_sncc_variants(void);
@@ -130,7 +131,7 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
                         const float* poses, int64_t C, int nviews, const int* views, const void* const* ftargs,
                         const float* hp, const float* lin, int64_t R, double kappa, int with_grad, int variant,
                         void* workspace, int64_t ws_bytes, void* stream);
-/* Pass 2 (same variant): tile sums in fp64 -> mom[nviews][C][stride] (kept
+/* Pass 2 (same variant): record sums in fp64 -> mom[nviews][C][stride] (kept
  * for the backward); loss[v] = 1 - mean_c ncc (f32), loss[nviews] = sum of the
  * view losses; ncc_out[nviews][C] optional. */
 int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews, int with_grad, int variant,
@@ -142,15 +143,15 @@ int fvr_tc_sncc_finalize(const void* workspace, int64_t C, int64_t R, int nviews
 int fvr_tc_sncc_backward(const double* mom, int nviews, const int* views, const float* g, int64_t g_stride,
                          const float* poses, int64_t C, int64_t D, int64_t H, int64_t W, double kappa,
                          float* grad_poses, int accumulate, void* stream);
-/* Single-launch loss + pose gradient (moments, finalize and backward fused):
- * the last CTA to finish a candidate writes that candidate's fp64 moments,
- * ncc_out[v][c] (optional) and grad_poses[c][6] (g = dL/dloss_v at
- * g[v * g_stride], NULL = all ones; accumulate != 0 adds), and the last
- * candidate writes loss[nviews + 1] as fvr_tc_sncc_finalize does.
- * `workspace` (>= fvr_tc_sncc_fused_workspace bytes, 256-byte aligned) ends
- * in a ticket region that must be zero before the first call (zero the
- * whole workspace once after allocating it); every completed call leaves it
- * zero.  Calls sharing one workspace must be stream-ordered.
+/* Loss + pose gradient in two stream-ordered launches (moments, finalize and
+ * backward fused): the moments kernel, then one epilogue kernel launched as
+ * its programmatic dependent, which forms the slice-axes Jacobians while the
+ * moments run and then writes every candidate's fp64 moments, ncc_out[v][c]
+ * (optional) and grad_poses[c][6] (g = dL/dloss_v at g[v * g_stride], NULL =
+ * all ones; accumulate != 0 adds), and loss[nviews + 1] as
+ * fvr_tc_sncc_finalize does.  `workspace` (>= fvr_tc_sncc_fused_workspace
+ * bytes, 256-byte aligned) needs no initialisation.  Calls sharing one
+ * workspace must be stream-ordered.
  * Replaces the forward + autograd backward of TorchDiffFVREngine.
  * forward_spectral_ncc over several views, src/fvr/torch_engine.py:269-307. */
 int64_t fvr_tc_sncc_fused_workspace(int64_t C, int64_t R, int64_t nviews);
@@ -162,17 +163,18 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
                                void* stream);
 /* Allocation-free form of fvr_tc_sncc_value_and_grad (no counterpart in the
  * reference): same arguments and results, but the workspace is a fixed
- * per-device scratch array inside the library (about 428 KB), so the call
+ * per-device scratch array inside the library (about 426 KB), so the call
  * allocates nothing.  For callers that cannot allocate device memory where
  * they call (a host linking only this C ABI, with no device allocator; a
  * loop that must not enter an allocator between steps).
- * Limits: C * nviews <= 512 and C * nviews * tiles <= 2048 partial records
- * (tiles per (candidate, view) as the launch variant sizes them); larger
- * calls return FVR_ERR_WORKSPACE without launching.
+ * Limits: C * nviews <= 512 and at most 2048 partial records (tile grid:
+ * C * nviews * tiles; one range per CTA: CTAs + C * nviews - 1, as the launch
+ * variant sizes them); larger calls return FVR_ERR_WORKSPACE without
+ * launching.
  * The first call on a device (that device current) resolves the scratch
  * address once; make it before any stream capture begins.  Nothing has to be
- * zeroed by the caller: the scratch's ticket counters start at zero and each
- * completed call leaves them zero.  All callers in the process share one
+ * zeroed by the caller: every call writes the scratch before reading it.
+ * All callers in the process share one
  * scratch per device, so calls on one device must not overlap in time (use
  * one stream or synchronise between them). */
 int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H,

@@ -364,9 +364,9 @@ def test_cpu_inputs_are_moved_and_outputs_finite(big):
 
 
 def test_fused_value_and_grad_every_variant_repeatable(big, monkeypatch):
-    """The single-launch value_and_grad (per-candidate and global tickets) agrees
-    with the autograd path for every launch variant, is bitwise repeatable, and
-    leaves its ticket region zero."""
+    """The fused value_and_grad (moments kernel + dependent epilogue) agrees
+    with the autograd path for every launch variant and is bitwise
+    repeatable."""
     import fvr._lib as L
 
     _, eng, _ = big
@@ -384,5 +384,50 @@ def test_fused_value_and_grad_every_variant_repeatable(big, monkeypatch):
         assert torch.equal(la, lb) and torch.equal(ga, gb), variant
         assert abs(float(la) - float(l1)) < 1e-6, variant
         assert torch.allclose(ga, p1.grad, rtol=1e-5, atol=1e-9), variant
-        ws = eng._fused_ws[(24, 128, 2, poses.device)]
-        assert int(ws[-256:].count_nonzero()) == 0
+
+
+@pytest.mark.parametrize("C,R", [(1024, 16), (3, 100), (7, 37)])
+def test_fused_segmented_split_matches_tile_grid(big, monkeypatch, C, R):
+    """Every launch variant against tile-grid variant 0 on shapes that stress
+    the equal-range split: at R = 16 with 2048 (candidate, view) items a CTA
+    covers pieces of more than eight items (slice axes formed inside the
+    segment loop), at R = 37 ranges are shorter than one pass of a CTA, at
+    R = 100 the rows straddle range ends.  Same moments up to float summation
+    order."""
+    import fvr._lib as L
+
+    _, eng, _ = big
+    poses = _t(tc.make_poses(C, 11))
+    tp = _t(tc.make_poses(1, 12))
+    fa = eng.prepare_spectral_target(eng(tp, view="ap", out_res=R))
+    fl = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=R))
+    monkeypatch.setenv("FVR_SNCC_FUSED_VARIANT", "0")
+    l0, g0 = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
+    scale = float(g0.abs().max())
+    for variant in range(1, L.load().fvr_tc_sncc_variants()):
+        monkeypatch.setenv("FVR_SNCC_FUSED_VARIANT", str(variant))
+        la, ga = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
+        assert abs(float(la) - float(l0)) < 2e-6, variant
+        assert torch.allclose(ga, g0, rtol=1e-4, atol=1e-5 * scale), variant
+
+
+def test_host_io_graph_step_matches_device_step(big):
+    """The host-to-host graph (pinned H2D copy, kernels, D2H copies in one
+    replay) returns exactly the device step's loss and gradient."""
+    from fvr.graphs import BiplanarSpectralNCCStep
+
+    _, eng, _ = big
+    poses = tc.make_poses(8, 13)
+    tp = _t(tc.make_poses(1, 14))
+    fa = eng.prepare_spectral_target(eng(tp, view="ap", out_res=128))
+    fl = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=128))
+    dev_step = BiplanarSpectralNCCStep(eng, fa, fl, 8)
+    io_step = BiplanarSpectralNCCStep(eng, fa, fl, 8, host_io=True)
+    ld, gd = dev_step(_t(poses))
+    lh, gh = io_step(torch.from_numpy(poses))
+    assert lh.device.type == "cpu" and gh.is_pinned()
+    assert float(lh) == float(ld) and torch.equal(gh, gd.cpu())
+    io_step.host_poses.copy_(torch.from_numpy(tc.make_poses(8, 15)))
+    lh2, gh2 = io_step(io_step.host_poses)
+    ld2, gd2 = dev_step(_t(tc.make_poses(8, 15)))
+    assert float(lh2) == float(ld2) and torch.equal(gh2, gd2.cpu())

@@ -56,7 +56,7 @@ def test_static_scratch_matches_workspace_entry(dtype):
     loss_ref, grad_ref = _outputs(C, dev)
     assert lib.fvr_tc_sncc_value_and_grad(*head, L.ptr(ws), ws_bytes, L.ptr(loss_ref), None, L.ptr(grad_ref), 0,
                                           s) == 0
-    for _ in range(2):  # two calls in a row: the static tickets must have reset
+    for _ in range(2):  # two calls in a row on the same scratch
         loss, grad = _outputs(C, dev)
         assert lib.fvr_tc_sncc_value_and_grad_static(*head, L.ptr(loss), None, L.ptr(grad), 0, s) == 0
         torch.cuda.synchronize()
