@@ -387,13 +387,12 @@ def test_fused_value_and_grad_every_variant_repeatable(big, monkeypatch):
 
 
 @pytest.mark.parametrize("C,R", [(1024, 16), (3, 100), (7, 37)])
-def test_fused_segmented_split_matches_tile_grid(big, monkeypatch, C, R):
-    """Every launch variant against tile-grid variant 0 on shapes that stress
-    the equal-range split: at R = 16 with 2048 (candidate, view) items a CTA
-    covers pieces of more than eight items (slice axes formed inside the
-    segment loop), at R = 37 ranges are shorter than one pass of a CTA, at
-    R = 100 the rows straddle range ends.  Same moments up to float summation
-    order."""
+def test_fused_variants_agree_on_ragged_shapes(big, monkeypatch, C, R):
+    """Every launch variant against variant 0 on shapes that stress the
+    column-stationary thread mapping and the row tiling: R = 16 (16 rows per
+    pass, 2048 (candidate, view) items, one tile each), R = 37 (6 rows per
+    pass, 34 idle threads), R = 100 (2 rows per pass, 56 idle threads, tiles
+    of uneven row counts).  Same moments up to float summation order."""
     import fvr._lib as L
 
     _, eng, _ = big
