@@ -265,6 +265,11 @@ def run_b200(args, torch):
     npl = _numpy_leg(torch, dev, max(3, min(W, 5)), max(5, min(K, 20)), rank == 0)
     reg = _registration_leg(torch, dev)
 
+    # the memory system's ceiling for this gather: the same 32-byte entries in
+    # the moments kernel's sweep order through a load-only kernel, L2 flushed
+    cells = profiling.sncc_cell_sequence(eng, poses, ("ap", "lateral"), OUT_RES)
+    gather_ms = profiling.gather_ceiling_ms(eng, cells, flush=flush, reps=7)
+
     res = None
     if rank == 0:
         peak, peak_kind = _peak_hbm()
@@ -302,8 +307,8 @@ def run_b200(args, torch):
                 "spectrum_storage": "f16 stencil with per-16^3-brick power-of-two scales (32-byte entry of 8 "
                                     "complex corners); f32 interpolation, positions and phases from fp64 "
                                     "per-row/column tables, fp64 reductions",
-                "step": "CUDA-graph replay of one kernel: gather + NCC/pose moments for both views, with the "
-                        "per-candidate fp64 finalize and pose gradient in the last CTA of each candidate",
+                "step": "CUDA-graph replay of two kernels: gather + NCC/pose moments for both views, then the "
+                        "fp64 finalize, pose gradient and losses as its programmatic dependent launch",
                 "l2": "flushed before every timed step (256 MiB write)",
                 "parallelism": f"replicas x{ws}",
             },
@@ -316,7 +321,8 @@ def run_b200(args, torch):
             "f16_batched_over_fp32_single": value / ws / single_value,
             "roofline": {
                 "bound": "hbm",
-                "kernel": "tc_sncc_moments_kernel<f16, grad, fused> (both views, 64 candidates)",
+                "kernel": "tc_sncc_moments_kernel<f16, grad> + its dependent tc_sncc_final_kernel (timed together; "
+                          "both views, 64 candidates)",
                 "achieved": achieved,
                 "peak": peak,
                 "unit": "GB/s",
@@ -328,6 +334,15 @@ def run_b200(args, torch):
                 "alg_bytes_note": "2 views x 64 candidates x 16384 samples x (32 B stencil entry + 8 B target)",
                 "kernel_ms": kern_avg_ms,
                 "kernel_launches_timed": len(f16["kern_ms"]),
+                "gather_ceiling": {
+                    "ms": gather_ms,
+                    "entries": int(cells.numel()),
+                    "achieved_gbs_of_entries": int(cells.numel()) * 32 / (gather_ms * 1e-3) / 1e9,
+                    "kernel_frac": gather_ms / kern_avg_ms,
+                    "note": "fvr_bench_gather32 over the same 32-byte stencil entries in the moments kernel's "
+                            "sweep order, no arithmetic, L2 flushed (python -m fvr.kernel_bench gather); "
+                            "kernel_frac = ceiling time / kernel time",
+                },
             },
             "cpu_baseline": cpu["baseline"],
             "e2e": {"value": CANDIDATES * ws / (statistics.mean(t_e2e) / 1e3), "unit": UNIT,

@@ -8,9 +8,29 @@ once and replayed, which removes every per-kernel launch and Python cost.
 """
 from __future__ import annotations
 
+import contextlib
+import functools
+import gc
+
 import torch
 
 from . import _lib as L
+
+
+@contextlib.contextmanager
+def no_gc_during_capture():
+    """Collect garbage now and keep the cyclic collector off until the block
+    ends: collecting an unreachable object that owns a CUDA graph destroys
+    that graph, which a capturing stream does not permit (the capture would
+    be invalidated)."""
+    gc.collect()
+    enabled = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if enabled:
+            gc.enable()
 
 
 class GraphedCallable:
@@ -27,8 +47,6 @@ class GraphedCallable:
     waiting; ``host_out`` is complete once the current stream is)."""
 
     def __init__(self, fn, *example_inputs, warmup=3, capture_context=None, host_io=False):
-        import contextlib
-
         for x in example_inputs:
             L.require_cuda(x)
         self.fn = fn
@@ -47,8 +65,15 @@ class GraphedCallable:
             self.host_out = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in outs]
         self.graph = torch.cuda.CUDAGraph()
         n0 = L.launch_count[0]
+        with no_gc_during_capture():
+            self._capture(fn, capture_context)
+        self.kernels_per_replay = L.launch_count[0] - n0
+
+    def _capture(self, fn, capture_context):
         with capture_context if capture_context is not None else contextlib.nullcontext():
-            with torch.cuda.graph(self.graph):
+            # thread-local: an unrelated CUDA call from another thread of the
+            # process (autograd workers, samplers) cannot invalidate the capture
+            with torch.cuda.graph(self.graph, capture_error_mode="thread_local"):
                 if self.host_io:
                     for s, h in zip(self.static_in, self.host_in):
                         s.copy_(h, non_blocking=True)
@@ -57,7 +82,6 @@ class GraphedCallable:
                     outs = self.static_out if isinstance(self.static_out, (tuple, list)) else (self.static_out,)
                     for h, o in zip(self.host_out, outs):
                         h.copy_(o, non_blocking=True)
-        self.kernels_per_replay = L.launch_count[0] - n0
 
     def replay(self):
         self.graph.replay()
@@ -75,6 +99,11 @@ class GraphedCallable:
         for s, x in zip(self.static_in, inputs):
             s.copy_(x, non_blocking=True)
         return self.replay()
+
+
+def _biplanar_value_and_grad(engine, f_ap, f_lat, high_pass, sigma, poses):
+    return engine.spectral_ncc_value_and_grad(poses, (f_ap, f_lat), ("ap", "lateral"), high_pass=high_pass,
+                                              cutoff_sigma=sigma)
 
 
 class BiplanarSpectralNCCStep:
@@ -103,15 +132,17 @@ class BiplanarSpectralNCCStep:
         self.hp = bool(high_pass)
         self.sigma = float(cutoff_sigma)
         ex = torch.zeros((int(n_candidates), 6), dtype=torch.float32, device=engine._dev)
-        self._g = (GraphedCallable(self._step, ex, warmup=warmup, capture_context=capture_context, host_io=host_io)
+        # the captured callable holds no reference back to this object (no
+        # reference cycle: the step and its graph are freed as soon as dropped)
+        fn = functools.partial(_biplanar_value_and_grad, engine, f_targ_ap, f_targ_lat, self.hp, self.sigma)
+        self._g = (GraphedCallable(fn, ex, warmup=warmup, capture_context=capture_context, host_io=host_io)
                    if graph else None)
         io = graph and host_io
         self.host_poses = self._g.host_in[0] if io else None
         self.host_loss, self.host_grad = self._g.host_out if io else (None, None)
 
     def _step(self, poses):
-        return self.engine.spectral_ncc_value_and_grad(poses, (self.f_ap, self.f_lat), ("ap", "lateral"),
-                                                       high_pass=self.hp, cutoff_sigma=self.sigma)
+        return _biplanar_value_and_grad(self.engine, self.f_ap, self.f_lat, self.hp, self.sigma, poses)
 
     def __call__(self, poses, sync=True):
         if self._g is None:

@@ -3,6 +3,12 @@
     python -m fvr.kernel_bench sncc  [--precision f16|bf16|f32] [--volume 128] [--candidates 64] [--out-res 128]
     python -m fvr.kernel_bench pou   [--precision f32|bf16] [--volume 192] [--grid 4] [--block-res 64]
                                      [--candidates 64] [--det 256]
+    python -m fvr.kernel_bench gather [--precision f16|bf16] [--volume 128] [--candidates 64] [--out-res 128]
+
+``gather`` times fvr_bench_gather32 over exactly the stencil entries one
+spectral-NCC launch of the ``sncc`` workload reads, in its sweep order, with
+and without an L2 flush before each launch: the memory system's ceiling for
+that gather with no arithmetic around it.
 
 Builds the workload, lets the autotuner settle, then runs ``--launches``
 steps inside an NVTX range named ``fvr_profile`` (so a profiler can select
@@ -64,9 +70,29 @@ def _pou(args):
     return step
 
 
+def _gather(args):
+    from . import profiling
+    from .torch_engine import TorchDiffFVREngine
+
+    dev = torch.device("cuda", 0)
+    vol = synthetic.make_ellipsoid_volume(args.volume, 0)
+    poses = torch.from_numpy(synthetic.make_poses(args.candidates, 1)).to(dev)
+    eng = TorchDiffFVREngine(torch.from_numpy(vol), device=dev)
+    eng.to_precision(PRECISION[args.precision])
+    cells = profiling.sncc_cell_sequence(eng, poses, ("ap", "lateral"), args.out_res)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    cold = profiling.gather_ceiling_ms(eng, cells, flush=flush, reps=9)
+    warm = profiling.gather_ceiling_ms(eng, cells, reps=9)
+    n = int(cells.numel())
+    print(json.dumps({"path": "gather", "precision": args.precision, "entries": n,
+                      "unique_entries": int(torch.unique(cells).numel()),
+                      "cold_ms": cold, "warm_ms": warm, "cold_gbs_of_entries": n * 32 / cold / 1e6,
+                      "warm_gbs_of_entries": n * 32 / warm / 1e6}))
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("path", choices=["sncc", "pou"])
+    ap.add_argument("path", choices=["sncc", "pou", "gather"])
     ap.add_argument("--precision", default="f16")
     ap.add_argument("--volume", type=int, default=128)
     ap.add_argument("--candidates", type=int, default=64)
@@ -78,6 +104,9 @@ def main():
     args = ap.parse_args()
     # backward on this thread, so the NVTX range below also covers the adjoint kernels
     torch.autograd.set_multithreading_enabled(False)
+    if args.path == "gather":
+        _gather(args)
+        return
     step = _sncc(args) if args.path == "sncc" else _pou(args)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -22,6 +22,7 @@ import torch
 
 from . import _lib as L
 from .cone_beam_fvr import edge_dominant_ncc
+from .graphs import no_gc_during_capture
 
 
 class _SE3ExpFn(torch.autograd.Function):
@@ -118,7 +119,7 @@ class MultistartRegistration:
             torch.cuda.current_stream(dev).wait_stream(side)
             self.reset(self._start)
             self._graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(self._graph):
+            with no_gc_during_capture(), torch.cuda.graph(self._graph, capture_error_mode="thread_local"):
                 self._iteration()
             self.reset(self._start)
 

@@ -327,6 +327,13 @@ int fvr_np_pair_moments(const void* a, const void* b, int64_t sh, int64_t sw, vo
  * : 0): lets a caller time one kernel inside a captured CUDA graph (no
  * reference counterpart; measurement utility). */
 int fvr_event_record(void* event, void* stream, int external);
+/* Gather ceiling of a cell sequence (no reference counterpart; measurement
+ * utility): reads the 32-byte entries entries[idx[i]], i < n (an index
+ * outside [0, n_entries) reads nothing), three 256-bit loads in flight
+ * per thread on `blocks` CTAs of 256 threads, and writes one folded word per
+ * thread to out[blocks * 256] (out_len elements available). */
+int fvr_bench_gather32(const void* entries, int64_t n_entries, const int* idx, int64_t n, unsigned* out,
+                       int64_t out_len, int blocks, void* stream);
 
 /* ------------------------------------------- image-domain spectral NCC -- */
 /* Between centred spectra Fp[B][n] and Ft[Bt][n] (Bt = 1 or B, complex), both
