@@ -452,111 +452,140 @@ __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(Snc
 }
 
 // Value-and-gradient epilogue, launched right after the moments kernel as its
-// programmatic dependent (one CTA of 1024 threads): the slice-axes Jacobians
-// per (view, candidate) are formed while the moments kernel still runs; after
-// griddepcontrol.wait, every item's records are summed in fp64 in record
-// order, then one thread per candidate forms its per-view ncc and pose
-// gradient (per axis gc (a A + 2 b B) through the Jacobian, translations from
-// the phase moments), and the view losses are reduced in a fixed order.
-constexpr int kFinalThreads = 1024;
+// programmatic dependent (one CTA of 512 threads).  The work goes in chunks
+// of candidates whose (view, candidate) items fit in shared memory:
+//  0. the slice-axes Jacobians of the first chunk's items, formed while the
+//     moments kernel still runs (later chunks: before their record sums);
+//  1. after griddepcontrol.wait, one thread per (item, moment): the item's
+//     records summed in record order, every load of a thread issued in one
+//     round, kept in shared memory;
+//  2. one thread per item: its ncc and its per-view part of the pose gradient
+//     (per axis gc (a A + 2 b B) through the Jacobian, translations from the
+//     phase moments);
+//  3. one thread per candidate: the views summed in order; the ncc sums for
+//     the losses accumulate per thread across chunks and are reduced in a
+//     fixed order at the end.
+constexpr int kFinalThreads = 512;
+constexpr int kFinalChunkItems = 128;  // 128 items x 44 doubles = 44 KB of shared memory
+constexpr int kFinalPairs = (kFinalChunkItems * M_NGRAD + kFinalThreads - 1) / kFinalThreads;  // per thread
+constexpr int kFinalRecords = 4;  // records per (item, moment) per load round
 
 __global__ void __launch_bounds__(kFinalThreads) tc_sncc_final_kernel(SnccArgs a) {
+  __shared__ double s_mom[kFinalChunkItems][M_NGRAD];
+  __shared__ double s_jac[kFinalChunkItems][18];
+  __shared__ double s_part[kFinalChunkItems][6];  // ga[3], gtx, gty, ncc
   __shared__ double red[kMaxViews][kFinalThreads / 32];
-  const int t = threadIdx.x, nv = a.nv, C = a.C;
-  const int64_t items = static_cast<int64_t>(nv) * C;
-  for (int64_t k = t; k < items; k += kFinalThreads) {
-    const int v = static_cast<int>(k / C), c = static_cast<int>(k - static_cast<int64_t>(v) * C);
-    double ax[8], jac[18];
-    slice_axes_jac(a.poses + 6 * c, view_lateral(a, v), a.sx, a.sy, a.sz, ax, jac);
-    for (int m = 0; m < 18; ++m) a.jac[k * 18 + m] = jac[m];
-  }
-  pdl_wait();
-  // record sums: four (item, moment) pairs per thread and pass, two records
-  // of each in flight per round
-  const int64_t npairs = items * M_NGRAD;
-  for (int64_t p0 = t; p0 < npairs; p0 += 4 * kFinalThreads) {
-    int64_t st[4];
-    int n[4], nmax = 0;
-    double sum[4];
+  const int t = threadIdx.x, nv = a.nv, C = a.C, tiles = a.tiles;
+  const double s3[3] = {a.sx, a.sy, a.sz};
+  double lsum[kMaxViews] = {0.0, 0.0, 0.0, 0.0};
+  const int cch = kFinalChunkItems / nv;  // candidates per chunk; chunk item li = v * cn + (c - c0)
+  for (int c0 = 0; c0 < C; c0 += cch) {
+    const int cn = min(cch, C - c0), ni = cn * nv;
+    if (c0 > 0) __syncthreads();  // the previous chunk is done with the shared arrays
+    if (t < ni) {
+      const int v = t / cn, c = c0 + (t - v * cn);
+      double ax[8];
+      slice_axes_jac(a.poses + 6 * c, view_lateral(a, v), a.sx, a.sy, a.sz, ax, s_jac[t]);
+    }
+    if (c0 == 0) pdl_wait();  // the moments kernel has completed and its records are visible
+    // record sums: the thread's pairs p = t + k * 512, all their loads in one round
+    const double* src[kFinalPairs];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int64_t p = p0 + u * kFinalThreads;
-      n[u] = 0;
-      st[u] = 0;
-      sum[u] = 0.0;
-      if (p < npairs) {
-        st[u] = (p / M_NGRAD) * a.tiles * M_NGRAD + p % M_NGRAD;
-        n[u] = a.tiles;
-        nmax = max(nmax, n[u]);
+    for (int k = 0; k < kFinalPairs; ++k) {
+      const int p = t + k * kFinalThreads;
+      src[k] = nullptr;
+      if (p < ni * M_NGRAD) {
+        const int li = p / M_NGRAD, m = p - li * M_NGRAD, v = li / cn;
+        const int64_t it = static_cast<int64_t>(v) * C + c0 + (li - v * cn);
+        src[k] = a.partial + it * tiles * M_NGRAD + m;
       }
     }
-    for (int k0 = 0; k0 < nmax; k0 += 2) {
-      double x[4][2];
+    double sum[kFinalPairs];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+    for (int k = 0; k < kFinalPairs; ++k) sum[k] = 0.0;
+    for (int r0 = 0; r0 < tiles; r0 += kFinalRecords) {
+      double x[kFinalPairs][kFinalRecords];
 #pragma unroll
-        for (int kk = 0; kk < 2; ++kk)
-          x[u][kk] = k0 + kk < n[u] ? __ldcg(a.partial + st[u] + static_cast<int64_t>(k0 + kk) * M_NGRAD) : 0.0;
+      for (int k = 0; k < kFinalPairs; ++k)
 #pragma unroll
-      for (int u = 0; u < 4; ++u) sum[u] += x[u][0] + x[u][1];
+        for (int r = 0; r < kFinalRecords; ++r)
+          x[k][r] = src[k] && r0 + r < tiles ? __ldcg(src[k] + static_cast<int64_t>(r0 + r) * M_NGRAD) : 0.0;
+#pragma unroll
+      for (int k = 0; k < kFinalPairs; ++k)
+#pragma unroll
+        for (int r = 0; r < kFinalRecords; ++r) sum[k] += x[k][r];
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int64_t p = p0 + u * kFinalThreads;
-      if (p < npairs) a.mom[(p / M_NGRAD) * kMomStride + p % M_NGRAD] = sum[u];
+    for (int k = 0; k < kFinalPairs; ++k) {
+      const int p = t + k * kFinalThreads;
+      if (p < ni * M_NGRAD) s_mom[p / M_NGRAD][p % M_NGRAD] = sum[k];
     }
-  }
-  __syncthreads();
-  double lsum[kMaxViews] = {0.0, 0.0, 0.0, 0.0};
-  const double s3[3] = {a.sx, a.sy, a.sz};
-  for (int c = t; c < C; c += kFinalThreads) {
-    double ga[3] = {0.0, 0.0, 0.0}, gtx = 0.0, gty = 0.0;
-    for (int v = 0; v < nv; ++v) {
+    __syncthreads();
+    if (t < ni) {
+      const int li = t, v = li / cn, c = c0 + (li - v * cn);
       const int64_t it = static_cast<int64_t>(v) * C + c;
-      double m[M_NGRAD];
-#pragma unroll
-      for (int k = 0; k < M_NGRAD; ++k) m[k] = __ldcg(a.mom + it * kMomStride + k);
+      const double* m = s_mom[li];
+      const double* j = s_jac[li];
       const double sq = sqrt(m[M_EP] * m[M_ET]);
       const double inv = 1.0 / (sq + 1e-8);
       const double ncc = m[M_CROSS] * inv;
       const double bb = sq > 0.0 ? -0.5 * m[M_CROSS] * m[M_ET] * inv * inv / sq : 0.0;
       const double gc = -(a.g ? static_cast<double>(a.g[v * a.g_stride]) : 1.0) / C;
-      const double* jac = a.jac + it * 18;
+      double ga[3] = {0.0, 0.0, 0.0};
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         const double du = gc * (inv * m[M_AU + i] + 2.0 * bb * m[M_BU + i]) * s3[i];
         const double dv = gc * (inv * m[M_AV + i] + 2.0 * bb * m[M_BV + i]) * s3[i];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) ga[k] += du * __ldcg(jac + (k * 2 + 0) * 3 + i) + dv * __ldcg(jac + (k * 2 + 1) * 3 + i);
+        for (int k = 0; k < 3; ++k) ga[k] += du * j[(k * 2 + 0) * 3 + i] + dv * j[(k * 2 + 1) * 3 + i];
       }
-      gtx += gc * inv * a.kappa * m[M_PHU];
-      gty += gc * inv * a.kappa * m[M_PHV];
-      a.mom[it * kMomStride + 17] = ncc;
+      double* o = s_part[li];
+      o[0] = ga[0];
+      o[1] = ga[1];
+      o[2] = ga[2];
+      o[3] = gc * inv * a.kappa * m[M_PHU];
+      o[4] = gc * inv * a.kappa * m[M_PHV];
+      o[5] = ncc;
+      double* mo = a.mom + it * kMomStride;
+      for (int k = 0; k < M_NGRAD; ++k) mo[k] = m[k];
+      mo[17] = ncc;
+      double* jo = a.jac + it * 18;
+      for (int k = 0; k < 18; ++k) jo[k] = j[k];
       if (a.ncc_out) a.ncc_out[it] = static_cast<float>(ncc);
-      if (v == 0) lsum[0] += ncc;
-      else if (v == 1) lsum[1] += ncc;
-      else if (v == 2) lsum[2] += ncc;
-      else lsum[3] += ncc;
     }
-    float* o = a.grad + 6 * c;
-    const float r[6] = {static_cast<float>(ga[0]), static_cast<float>(ga[1]), static_cast<float>(ga[2]),
-                        static_cast<float>(gtx), static_cast<float>(gty), 0.f};
-    for (int k = 0; k < 6; ++k) o[k] = a.accumulate ? o[k] + r[k] : r[k];
+    __syncthreads();
+    if (t < cn) {
+      const int c = c0 + t;
+      double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int v = 0; v < nv; ++v) {
+        const double* o = s_part[v * cn + t];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) r[k] += o[k];
+        if (v == 0) lsum[0] += o[5];
+        else if (v == 1) lsum[1] += o[5];
+        else if (v == 2) lsum[2] += o[5];
+        else lsum[3] += o[5];
+      }
+      float* g = a.grad + 6 * c;
+      const float rf[6] = {static_cast<float>(r[0]), static_cast<float>(r[1]), static_cast<float>(r[2]),
+                           static_cast<float>(r[3]), static_cast<float>(r[4]), 0.f};
+      for (int k = 0; k < 6; ++k) g[k] = a.accumulate ? g[k] + rf[k] : rf[k];
+    }
   }
   // loss[v] = 1 - mean_c ncc (fixed order: per thread, per warp, across warps)
   const int lane = t & 31, w = t >> 5;
 #pragma unroll
   for (int v = 0; v < kMaxViews; ++v) {
-    const double s = warp_sum(lsum[v]);
-    if (lane == 0) red[v][w] = s;
+    const double sv = warp_sum(lsum[v]);
+    if (lane == 0) red[v][w] = sv;
   }
   __syncthreads();
   if (t == 0) {
     double total = 0.0;
     for (int v = 0; v < nv; ++v) {
-      double s = 0.0;
-      for (int k = 0; k < kFinalThreads / 32; ++k) s += red[v][k];
-      const double l = 1.0 - s / C;
+      double sv = 0.0;
+      for (int k = 0; k < kFinalThreads / 32; ++k) sv += red[v][k];
+      const double l = 1.0 - sv / C;
       a.loss[v] = static_cast<float>(l);
       total += l;
     }

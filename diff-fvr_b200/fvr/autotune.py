@@ -1,9 +1,11 @@
 """Launch-shape autotuner for the hot kernels.
 
 On the first call for a new shape key, every launch variant the library
-offers is timed with CUDA events (after one warm-up launch each) and the
-fastest is cached for the process (a variant the library refuses for the
-shape is skipped).  Inside CUDA-graph capture (where nothing
+offers is timed with CUDA events (after one warm-up launch each, then the
+median of several launches that each follow an L2 rewrite: cold-cache
+conditions, which is how a step meets the spectrum) and the fastest is
+cached for the process (a variant the library refuses for the shape is
+skipped).  Inside CUDA-graph capture (where nothing
 can be timed) a cached choice or variant 0 is used; ``FVR_SNCC_VARIANT``
 pins a variant.
 """
@@ -19,8 +21,24 @@ _cache = {}
 _timings = {}
 
 
-def choose(kind, key, run, n_variants, reps=3):
-    """Return the fastest variant of ``run(variant)`` (launches one kernel) for ``key``."""
+_flush = {}
+
+
+def _l2_flush(device):
+    """A 192 MiB buffer (more than the 126 MB L2) rewritten before each timed
+    launch, so variants are compared on a cold L2 (allocated once per device)."""
+    t = _flush.get(device)
+    if t is None:
+        t = torch.zeros(48 * 1024 * 1024, dtype=torch.float32, device=device)
+        _flush[device] = t
+    return t
+
+
+def choose(kind, key, run, n_variants, reps=5):
+    """Return the fastest variant of ``run(variant)`` (launches one kernel) for
+    ``key``: the median of ``reps`` launches per variant, each after an L2
+    rewrite (the flush also keeps the device busy while the launch is
+    enqueued, so the events time the launch alone)."""
     env = os.environ.get(f"FVR_{kind.upper()}_VARIANT")
     if env is not None:
         return int(env)
@@ -29,6 +47,7 @@ def choose(kind, key, run, n_variants, reps=3):
         return _cache[k]
     if torch.cuda.is_current_stream_capturing():
         return 0
+    flush = _l2_flush(torch.cuda.current_device())
     best, best_ms, times = 0, float("inf"), []
     for v in range(n_variants):
         try:
@@ -36,13 +55,17 @@ def choose(kind, key, run, n_variants, reps=3):
         except L.FvrError:  # this shape does not fit the variant (e.g. its shared memory)
             times.append(float("inf"))
             continue
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
+        ts = []
         for _ in range(reps):
+            flush.add_(1.0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
             run(v)
-        b.record()
-        b.synchronize()
-        ms = a.elapsed_time(b) / reps
+            b.record()
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        ts.sort()
+        ms = ts[len(ts) // 2]
         times.append(ms)
         if ms < best_ms:
             best, best_ms = v, ms
