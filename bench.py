@@ -273,6 +273,7 @@ def run_b200(args, torch):
     pou = _pou_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
     npl = _numpy_leg(torch, dev, max(3, min(W, 5)), max(5, min(K, 20)), rank == 0)
     reg = _registration_leg(torch, dev)
+    cfg4 = _cfg4_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
 
     # the memory system's ceiling for this gather: the same 32-byte entries in
     # the moments kernel's sweep order through a load-only kernel, L2 flushed
@@ -372,6 +373,7 @@ def run_b200(args, torch):
             "pou_cone_beam": pou,
             "numpy_renderer": npl,
             "registration": reg,
+            "cfg4_512": cfg4,
         }
     if ws > 1:
         dist.barrier()
@@ -427,6 +429,61 @@ def _pou_leg(torch, dev, flush, warmup, steps):
                        "forward + pose gradient (eager autograd through forward_pinhole)")
     out["l2"] = "flushed before every timed step (256 MiB write)"
     return out
+
+
+def _cfg4_leg(torch, dev, flush, warmup, steps):
+    """Secondary line: the large torch-convention case.  Seeded 256^3
+    ellipsoid volume (spacing 0.8 x 0.8 x 1.5 mm: voxel-unit spectrum, spacing[0]
+    in the phase as the reference uses it) -> 512^3 spectrum, R = 192, 256
+    candidates x 2 views, loss + pose gradient as one graph replay per step,
+    per storage precision; f16 / bf16 errors against this run's f32 path."""
+    import fvr
+    from fvr import synthetic
+    from fvr.graphs import BiplanarSpectralNCCStep
+
+    n, C, R = 256, 256, 192
+    vol = synthetic.make_ellipsoid_volume(n, SEED)
+    poses = torch.from_numpy(synthetic.make_poses(C, SEED + 1)).to(dev)
+    tp = torch.from_numpy(synthetic.make_poses(1, SEED + 2)).to(dev)
+    eng = fvr.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(0.8, 0.8, 1.5), pad_factor=2.0, device=dev)
+    with torch.no_grad():
+        f_ap = eng.prepare_spectral_target(eng(tp, view="ap", out_res=R))
+        f_lat = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=R))
+    sub = poses[:4]
+    out, ref = {}, None
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
+        if name == "bf16":
+            eng.to_precision(dt)
+        elif name == "f16":  # brick-scaled f16 from the full-precision spectrum, not from the bf16 cast
+            fresh = fvr.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(0.8, 0.8, 1.5), pad_factor=2.0, device=dev)
+            fresh.to_precision(dt)
+            eng._stencil, eng.f_vol_5d = fresh._stencil, fresh.f_vol_5d
+            del fresh
+        step = BiplanarSpectralNCCStep(eng, f_ap, f_lat, C, warmup=warmup)
+        loss, grad = step(poses)
+        img = torch.cat([eng(sub, view=v, out_res=R) for v in ("ap", "lateral")]).cpu().numpy()
+        res = {"loss": float(loss), "grad": grad.detach().cpu().numpy().copy(), "img": img}
+        for _ in range(warmup):
+            step._g.replay()
+        st, _ = _time_steps(torch, step._g.replay, steps, flush)
+        ms = statistics.mean(st)
+        entry = {"value": C / (ms / 1e3), "ms_per_step": ms, "ms_per_step_min_median_max":
+                 [min(st), statistics.median(st), max(st)]}
+        if ref is None:
+            ref = res
+        else:
+            g0 = ref["grad"][:, :5]
+            entry["loss_abs_err_vs_f32"] = abs(res["loss"] - ref["loss"])
+            entry["grad_rel_l2_vs_f32"] = float(np.linalg.norm(res["grad"][:, :5] - g0) / np.linalg.norm(g0))
+            entry["image_rel_l2_vs_f32"] = float(np.linalg.norm(res["img"] - ref["img"]) / np.linalg.norm(ref["img"]))
+        out[name] = entry
+        del step
+    stencil_bytes = {"f32": 513 ** 3 * 64, "f16": 513 ** 3 * 32, "bf16": 513 ** 3 * 32}
+    return {"unit": UNIT, "precisions": out, "stencil_bytes": stencil_bytes,
+            "workload": "seeded 256^3 ellipsoid volume -> 512^3 spectrum (f32 / brick-scaled f16 / bf16 stencils), "
+                        "R = 192, 256 candidates x 2 views, loss + 6-DOF gradient per step (CUDA-graph replay, "
+                        "L2 flushed before each step)",
+            "error_reference": "this run's f32 path (the f32 path is pinned to the fp64 oracle at 128^3 -> 256^3)"}
 
 
 def _registration_leg(torch, dev, iters=200, n_cand=CANDIDATES):

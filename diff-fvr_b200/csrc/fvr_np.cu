@@ -144,6 +144,48 @@ __global__ void np_ncc_finalize_kernel(const double* __restrict__ partial, int n
 
 constexpr int kNpTiles = 64;
 
+// Articulated (multi-segment) spectrum: output o is the sum, in segment order,
+// of the phase-ramped slices of segment spectra f[s] at item (o, s)
+// (articulated_spine.py:39-71, Fourier linearity); every segment spectrum has
+// the same padded shape.  Items are [n_out][n_seg]; output o is written at
+// the offset of item (o, 0).
+constexpr int kMaxSegments = 16;
+struct SegSpectra {
+  const double2* f[kMaxSegments];
+};
+
+__global__ void __launch_bounds__(256) np_segment_sum_kernel(const __grid_constant__ SegSpectra sp, int n_seg, int D,
+                                                             int H, int W, const NpItem* __restrict__ items,
+                                                             double2* __restrict__ out) {
+  __shared__ NpItem s_it[kMaxSegments];
+  __shared__ double s_uv[kMaxSegments][6];
+  const int o = blockIdx.y;
+  if (threadIdx.x < n_seg) {
+    const NpItem it = items[static_cast<int64_t>(o) * n_seg + threadIdx.x];
+    double u[3], v[3];
+    np_basis(it, u, v);
+    s_it[threadIdx.x] = it;
+    for (int k = 0; k < 3; ++k) {
+      s_uv[threadIdx.x][k] = u[k];
+      s_uv[threadIdx.x][3 + k] = v[k];
+    }
+  }
+  __syncthreads();
+  const int sh = s_it[0].sh, sw = s_it[0].sw;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= sh * sw) return;
+  const int i = q / sw, j = q - (q / sw) * sw;
+  double2 sum = make_double2(0.0, 0.0);
+  for (int s = 0; s < n_seg; ++s) {
+    const double u[3] = {s_uv[s][0], s_uv[s][1], s_uv[s][2]}, v[3] = {s_uv[s][3], s_uv[s][4], s_uv[s][5]};
+    double uu, vv;
+    const double2 x = np_slice_value(sp.f[s], D, H, W, s_it[s], u, v, i, j, uu, vv);
+    sum.x += x.x;
+    sum.y += x.y;
+  }
+  out[s_it[0].off + q] = sum;
+}
+
 // Moments of two complex fp64 [sh][sw] arrays on the slice grid
 // u = j - sw/2, v = i - sh/2: (Re sum a conj b, sum |a|^2, sum |b|^2,
 // sum u Im(a conj b), sum v Im(a conj b))
@@ -190,6 +232,24 @@ int fvr_np_slices(const void* f3d, int64_t D, int64_t H, int64_t W, const void* 
                     static_cast<cudaStream_t>(stream)>>>(static_cast<const double2*>(f3d), (int)D, (int)H, (int)W,
                                                         static_cast<const NpItem*>(items),
                                                         static_cast<double2*>(out));
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int fvr_np_segment_slices(const void* const* f3ds, int64_t n_seg, int64_t D, int64_t H, int64_t W, const void* items,
+                          int64_t n_out, int64_t max_n, void* out, void* stream) {
+  if (!f3ds || !items || !out || n_seg < 1 || n_seg > kMaxSegments || n_out < 1 || n_out > 65535 || max_n < 1 ||
+      D < 2 || H < 2 || W < 2)
+    return FVR_ERR_ARG;
+  SegSpectra sp{};
+  for (int64_t k = 0; k < n_seg; ++k) {
+    if (!f3ds[k]) return FVR_ERR_ARG;
+    sp.f[k] = static_cast<const double2*>(f3ds[k]);
+  }
+  np_segment_sum_kernel<<<dim3((unsigned)cdiv64(max_n, 256), (unsigned)n_out), 256, 0,
+                          static_cast<cudaStream_t>(stream)>>>(sp, (int)n_seg, (int)D, (int)H, (int)W,
+                                                               static_cast<const NpItem*>(items),
+                                                               static_cast<double2*>(out));
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }

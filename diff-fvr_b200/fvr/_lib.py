@@ -94,6 +94,9 @@ SIGNATURES = {
     "fvr_np_ncc_workspace": (I64, [I64]),
     "fvr_np_ncc_moments": (I32, [P, I64, I64, I64, P, I64, P, P, I64, P, P]),
     "fvr_np_pair_workspace": (I64, []),
+    "fvr_ingest_resample": (I32, [P, I64, I64, I64, F64, F64, F64, I64, I32, P, P, P]),
+    "fvr_hu_to_attenuation": (I32, [P, I64, P, P]),
+    "fvr_np_segment_slices": (I32, [P, I64, I64, I64, I64, P, I64, I64, P, P]),
     "fvr_np_pair_moments": (I32, [P, P, I64, I64, P, I64, P, P]),
     "fvr_cncc_workspace": (I64, [I64, I64]),
     "fvr_cncc_forward": (I32, [P, P, I64, I64, I64, P, P, I64, P, P, P]),

@@ -170,3 +170,24 @@ def _pair_moments(a, b):
     L.call("fvr_np_pair_moments", L.ptr(a.contiguous()), L.ptr(b.contiguous()), sh, sw, L.ptr(ws), ws_bytes,
            L.ptr(mom), L.stream_ptr(dev))
     return mom.cpu().numpy()
+
+
+def prepare_target_spectrum(renderer: DifferentiableFourierVolumeRenderer, img: np.ndarray, view: str,
+                            keep_on_device: bool = False):
+    """Target spectrum for the NumPy-convention spectral NCC
+    (RobustDiffFVREngine._prepare_spectrum, core_engine.py:71-85): the image
+    zero-padded into the view's slice frame (lateral (pz, py), ap (pz, px),
+    else (py, px); low-side offset (S - n) // 2) and
+    ``fftshift(fft2(ifftshift(.)))`` in complex128, on the GPU.  Returns a
+    NumPy array, or with ``keep_on_device`` the device tensor that
+    ``compute_spectral_ncc`` style moments can use without a copy."""
+    slice_h, slice_w = renderer._dims(view)
+    im = np.asarray(img, dtype=np.float64)
+    th, tw = im.shape
+    if th > slice_h or tw > slice_w:
+        raise ValueError(f"target {th}x{tw} does not fit the {slice_h}x{slice_w} slice frame")
+    padded = torch.zeros((slice_h, slice_w), dtype=torch.float64, device=renderer._dev)
+    sh, sw = (slice_h - th) // 2, (slice_w - tw) // 2
+    padded[sh:sh + th, sw:sw + tw] = torch.from_numpy(np.ascontiguousarray(im)).to(renderer._dev)
+    f = RT.fft2d(padded, inverse=False, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT)
+    return f if keep_on_device else f.cpu().numpy()

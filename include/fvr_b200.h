@@ -301,6 +301,15 @@ int fvr_pou_pose_backward(const double* sl_part, int64_t tiles, const double* go
  * rows x columns; off = element offset of the item's slice / target).  The
  * spectrum f3d[D][H][W] is complex fp64 (fftshift(fftn(ifftshift(...)))). */
 int64_t fvr_np_item_bytes(void);
+/* Articulated multi-segment spectra: out[o] = sum over s < n_seg (in order) of
+ * the phase-ramped slice of segment spectrum f3ds[s] (host array of device
+ * pointers to complex128 [D][H][W] spectra of one common padded shape) at
+ * item (o, s) of items[n_out][n_seg] (fvr_np_item_bytes each); output o is
+ * written at the offset of item (o, 0); max_n = largest sh * sw; n_seg <= 16.
+ * Replaces ArticulatedSpineModel.render_articulated_spectrum,
+ * src/fvr/articulated_spine.py:39-71 (one launch for all segments). */
+int fvr_np_segment_slices(const void* const* f3ds, int64_t n_seg, int64_t D, int64_t H, int64_t W, const void* items,
+                          int64_t n_out, int64_t max_n, void* out, void* stream);
 /* Phase-ramped frequency slices (complex fp64) with map_coordinates
  * (order 1, mode 'constant') sampling and the basis rz(yaw).ry(roll).rx(pitch)
  * on (Z, Y, X).  Replaces DifferentiableFourierVolumeRenderer._euler_to_basis /
@@ -321,6 +330,22 @@ int64_t fvr_np_pair_workspace(void);
  * gradient, gradients.py:27-74). */
 int fvr_np_pair_moments(const void* a, const void* b, int64_t sh, int64_t sw, void* workspace, int64_t ws_bytes,
                         double* mom, void* stream);
+
+/* ------------------------------------------------------- volume ingest -- */
+/* CT (HU, float32 [Z][Y][X], spacing sz, sy, sx mm) -> isotropic cube
+ * out[target_res]^3 keeping the whole physical field of view centred:
+ * voxel_mm = max(n_k * s_k) / target_res; input coordinate
+ * c_k = (voxel_mm / s_k) * o_k + (n_k - 1) / 2 - (voxel_mm / s_k) (target_res - 1) / 2,
+ * linear interpolation, -1000 HU unless 0 <= c_k <= n_k - 1 on every axis;
+ * with to_mu the float32 attenuation max(0, (HU + 1000) / 1000) instead of HU.
+ * *voxel_mm (optional, host) receives the cube's voxel size.  Replaces
+ * resample_isotropic_cube + hu_to_attenuation, src/fvr/dicom_loader.py:11-30,
+ * 179-188 (scipy affine_transform, order 1, mode 'constant', cval -1000). */
+int fvr_ingest_resample(const float* hu, int64_t Z, int64_t Y, int64_t X, double sz, double sy, double sx,
+                        int64_t target_res, int to_mu, float* out, double* voxel_mm, void* stream);
+/* out[i] = max(0, (hu[i] + 1000) / 1000) in float32 (hu_to_attenuation,
+ * src/fvr/dicom_loader.py:179-188). */
+int fvr_hu_to_attenuation(const float* hu, int64_t n, float* out, void* stream);
 
 /* ----------------------------------------------------------- timing ---- */
 /* cudaEventRecordWithFlags(event, stream, external ? cudaEventRecordExternal

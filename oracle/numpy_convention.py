@@ -125,3 +125,78 @@ def biplanar_loss_and_gradients(f3d, pose, t_ap, t_lat, delta=0.2):
         g[i] = -0.5 * (d_ap + d_lat)
     g[3], g[4], g[5] = -0.5 * d_ap_x, -0.5 * d_lat_y, -0.5 * (d_ap_z + d_lat_z)
     return float(loss), g
+
+
+def articulated_spectrum(f3ds, base_pose, arts, view):
+    """Sum over segments of their phase-ramped slices, each at the base pose
+    plus the accumulated joint articulations below it; lateral slices take
+    (ty, tz), ap (tx, tz), anything else the axial slice with (tx, ty)
+    (articulated_spine.py:39-71)."""
+    curr = np.array(base_pose, np.float64)
+    total = None
+    for i, f3d in enumerate(f3ds):
+        if i > 0 and len(arts) >= i:
+            curr = curr + np.asarray(arts[i - 1], np.float64)
+        yaw, pitch, roll, tx, ty, tz = curr
+        if view == "lateral":
+            s = extract_frequency_slice(f3d, yaw, pitch, roll, ty, tz, "lateral")
+        elif view == "ap":
+            s = extract_frequency_slice(f3d, yaw, pitch, roll, tx, tz, "ap")
+        else:
+            s = extract_frequency_slice(f3d, yaw, pitch, roll, tx, ty, "axial")
+        total = s if total is None else total + s
+    return total
+
+
+def articulated_drr(f3ds, base_pose, arts, view):
+    """max(real(fftshift(ifft2(ifftshift(F)))), 0) (articulated_spine.py:73-85)."""
+    f = articulated_spectrum(f3ds, base_pose, arts, view)
+    return np.maximum(np.real(np.fft.fftshift(np.fft.ifft2(np.fft.ifftshift(f)))), 0.0)
+
+
+def resample_isotropic_cube(volume_hu, spacing, target_res):
+    """Isotropic cube keeping the CT's physical field of view centred
+    (dicom_loader.py:11-30): input coordinate ratio * index + offset per axis,
+    linear interpolation, -1000 HU unless every coordinate lies in [0, n-1]."""
+    vol = np.asarray(volume_hu, np.float32).astype(np.float64)
+    sp = np.asarray(spacing, np.float64)
+    shape = np.array(vol.shape)
+    vmm = float(np.max(shape * sp) / target_res)
+    ratio = vmm / sp
+    off = (shape - 1) / 2 - ratio * (target_res - 1) / 2
+    o = np.arange(target_res, dtype=np.float64)
+    cz, cy, cx = (off[k] + ratio[k] * o for k in range(3))
+    Z, Y, X = np.meshgrid(cz, cy, cx, indexing="ij")
+    inside = (Z >= 0) & (Z <= vol.shape[0] - 1) & (Y >= 0) & (Y <= vol.shape[1] - 1) & (X >= 0) & \
+        (X <= vol.shape[2] - 1)
+    fz, fy, fx = np.floor(Z), np.floor(Y), np.floor(X)
+    tz, ty, tx = Z - fz, Y - fy, X - fx
+    iz, iy, ix = (np.clip(a, 0, n - 1).astype(int) for a, n in ((fz, vol.shape[0]), (fy, vol.shape[1]),
+                                                                 (fx, vol.shape[2])))
+    iz1, iy1, ix1 = (np.minimum(a + 1, n - 1) for a, n in ((iz, vol.shape[0]), (iy, vol.shape[1]),
+                                                           (ix, vol.shape[2])))
+    out = np.zeros(Z.shape)
+    for zi, wz in ((iz, 1 - tz), (iz1, tz)):
+        for yi, wy in ((iy, 1 - ty), (iy1, ty)):
+            for xi, wx in ((ix, 1 - tx), (ix1, tx)):
+                out += wz * wy * wx * vol[zi, yi, xi]
+    out = np.where(inside, out, -1000.0).astype(np.float32)
+    return out, (vmm,) * 3
+
+
+def hu_to_attenuation(volume_hu):
+    """mu = max(0, (HU + 1000) / 1000) in float32 (dicom_loader.py:179-188)."""
+    h = np.asarray(volume_hu, np.float32)
+    return np.maximum(np.float32(0.0), (h + np.float32(1000.0)) / np.float32(1000.0)).astype(np.float32)
+
+
+def prepare_spectrum(shape_pad, img, view):
+    """Target image zero-padded into the view's slice frame (low side
+    (S - n) // 2) and fftshift(fft2(ifftshift(.))) (core_engine.py:71-85)."""
+    sh, sw = dims(shape_pad, view)
+    img = np.asarray(img, np.float64)
+    th, tw = img.shape
+    padded = np.zeros((sh, sw))
+    r0, c0 = (sh - th) // 2, (sw - tw) // 2
+    padded[r0:r0 + th, c0:c0 + tw] = img
+    return np.fft.fftshift(np.fft.fft2(np.fft.ifftshift(padded)))

@@ -2,7 +2,10 @@
 
 Usage (needs the reference checkout; run from the repository root):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py /root/reference [name,name,...]
+
+(names: slice_warp, torch_engine, pou, numpy_renderer, articulated,
+ingest_targets; all of them when none is given)
 
 It imports the reference's ``fvr`` package (``src/fvr``) with empty stand-ins
 for ``pydicom`` / ``SimpleITK`` (only ``dicom_loader`` needs them, and nothing
@@ -264,16 +267,77 @@ def gen_numpy(df, gr):
     np.savez_compressed(HERE / "numpy_renderer.npz", **out)
 
 
+def gen_articulated(ref_root: Path):
+    """ArticulatedSpineModel (articulated_spine.py): three segments of one
+    shape, spectra and DRRs at an articulated pose, the biplanar objective's
+    building blocks at two poses."""
+    from fvr import articulated_spine as asp
+
+    out = {}
+    segs = []
+    for k in range(3):
+        sub = _ellipsoids(16, 30 + k, shape=(12, 14, 16)).astype(np.float64)
+        out[f"sub{k}"] = sub
+        segs.append(asp.VertebralSegment(f"L{3 + k}", sub, nominal_offset_z=12.0 * k))
+    model = asp.ArticulatedSpineModel(segs)
+    base = np.array([2.0, -1.5, 1.0, 0.75, -0.5, 1.25])
+    arts = [np.array([1.5, -0.5, 0.8, 0.3, -0.2, 0.4]), np.array([-1.0, 1.2, -0.6, -0.25, 0.35, -0.3])]
+    out["base"] = base
+    out["arts"] = np.stack(arts)
+    for view in ("ap", "lateral"):
+        out[f"spec_{view}"] = model.render_articulated_spectrum(base, arts, view=view)
+        out[f"drr_{view}"] = model.render_drr(base, arts, view=view)
+    out["spec_ap_noart"] = model.render_articulated_spectrum(base, [], view="ap")
+    t_ap = model.render_articulated_spectrum(np.zeros(6), [np.zeros(6)] * 2, view="ap")
+    t_lat = model.render_articulated_spectrum(np.zeros(6), [np.zeros(6)] * 2, view="lateral")
+    out["ncc_ap"] = np.array(segs[0].renderer.compute_spectral_ncc(out["spec_ap"], t_ap))
+    out["ncc_lat"] = np.array(segs[0].renderer.compute_spectral_ncc(out["spec_lateral"], t_lat))
+    np.savez_compressed(HERE / "articulated.npz", **out)
+
+
+def gen_ingest_and_targets(ref_root: Path):
+    """resample_isotropic_cube / hu_to_attenuation (dicom_loader.py) on a small
+    anisotropic HU volume, and RobustDiffFVREngine._prepare_spectrum
+    (core_engine.py:71-85) for the three views."""
+    from fvr import core_engine, diff_fvr, dicom_loader
+
+    out = {}
+    rng = np.random.default_rng(11)
+    hu = (rng.uniform(-1000.0, 1500.0, size=(9, 13, 11))).astype(np.float32)
+    spacing = (2.5, 0.8, 1.1)
+    out["hu"] = hu
+    out["spacing"] = np.array(spacing)
+    for n in (16, 23):
+        res, sp = dicom_loader.resample_isotropic_cube(hu, spacing, n)
+        out[f"resampled_{n}"] = res
+        out[f"voxel_mm_{n}"] = np.array(sp[0])
+        out[f"mu_{n}"] = dicom_loader.hu_to_attenuation(res)
+    vol = _ellipsoids(16, 9, shape=(14, 12, 16)).astype(np.float64)
+    out["vol"] = vol
+    ren = diff_fvr.DifferentiableFourierVolumeRenderer(vol, pad_factor=2.0)
+    holder = type("Holder", (), {})()
+    holder.renderer = ren
+    for view, shape in (("ap", (14, 16)), ("lateral", (13, 11)), ("axial", (12, 16))):
+        img = rng.uniform(0.0, 1.0, size=shape)
+        out[f"img_{view}"] = img
+        out[f"target_{view}"] = core_engine.RobustDiffFVREngine._prepare_spectrum(holder, img, view)
+    np.savez_compressed(HERE / "ingest_targets.npz", **out)
+
+
 def main():
     ref_root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    only = set(sys.argv[2].split(",")) if len(sys.argv) > 2 else None
     import torch
 
     torch.set_num_threads(4)
     te, ts, cb, df, gr = _import_reference(ref_root)
-    gen_slice_and_warp(ts)
-    gen_torch_engine(te)
-    gen_pou(cb)
-    gen_numpy(df, gr)
+    gens = {"slice_warp": lambda: gen_slice_and_warp(ts), "torch_engine": lambda: gen_torch_engine(te),
+            "pou": lambda: gen_pou(cb), "numpy_renderer": lambda: gen_numpy(df, gr),
+            "articulated": lambda: gen_articulated(ref_root),
+            "ingest_targets": lambda: gen_ingest_and_targets(ref_root)}
+    for name, gen in gens.items():
+        if only is None or name in only:
+            gen()
     for f in sorted(HERE.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

@@ -272,3 +272,36 @@ def test_numpy_convention_oracle(golden):
     assert abs(loss - float(g["bip_loss"])) < 1e-12
     assert np.allclose(grad, g["bip_grad"], rtol=1e-9, atol=1e-12)
     assert np.allclose(nc.ncc_and_grad_translation(g["slice_lateral"], t_lat), g["tgrad"], rtol=1e-10, atol=1e-13)
+
+
+def test_articulated_oracle(golden):
+    """Segment-sum restatement against ArticulatedSpineModel's own outputs."""
+    from oracle import numpy_convention as nc
+
+    g = golden("articulated")
+    f3ds = [nc.spectrum(g[f"sub{k}"], 2.0) for k in range(3)]
+    arts = list(g["arts"])
+    for view in ("ap", "lateral"):
+        assert rel_l2(nc.articulated_spectrum(f3ds, g["base"], arts, view), g[f"spec_{view}"]) < 1e-12
+        assert rel_l2(nc.articulated_drr(f3ds, g["base"], arts, view), g[f"drr_{view}"]) < 1e-12
+    assert rel_l2(nc.articulated_spectrum(f3ds, g["base"], [], "ap"), g["spec_ap_noart"]) < 1e-12
+    t_ap = nc.articulated_spectrum(f3ds, np.zeros(6), [np.zeros(6)] * 2, "ap")
+    assert abs(nc.spectral_ncc(g["spec_ap"], t_ap) - float(g["ncc_ap"])) < 1e-12
+
+
+def test_ingest_and_target_oracle(golden):
+    """Resample / HU->mu / target-spectrum restatements against
+    dicom_loader.py and core_engine.py outputs."""
+    from oracle import numpy_convention as nc
+
+    g = golden("ingest_targets")
+    for n in (16, 23):
+        res, sp = nc.resample_isotropic_cube(g["hu"], g["spacing"], n)
+        assert sp[0] == float(g[f"voxel_mm_{n}"])
+        ref = g[f"resampled_{n}"]
+        assert res.dtype == np.float32 and res.shape == ref.shape
+        assert np.max(np.abs(res - ref)) <= 2e-4  # a float32 ulp of the largest HU values
+        assert np.array_equal(nc.hu_to_attenuation(ref), g[f"mu_{n}"])
+    shape_pad = tuple(int(round(s * 2.0)) for s in g["vol"].shape)
+    for view in ("ap", "lateral", "axial"):
+        assert rel_l2(nc.prepare_spectrum(shape_pad, g[f"img_{view}"], view), g[f"target_{view}"]) < 1e-13
