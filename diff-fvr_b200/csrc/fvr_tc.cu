@@ -136,7 +136,6 @@ struct SnccArgs {
   double* partial;  // partial-moment records of NM doubles
   // value-and-gradient epilogue only
   double* mom;         // [nv][C][kMomStride]
-  double* jac;         // [nv][C][18]: slice-axes Jacobian per (view, candidate)
   float* loss;         // [nv + 1]
   float* ncc_out;      // [nv][C] or null
   float* grad;         // [C][6]
@@ -518,7 +517,12 @@ __global__ void __launch_bounds__(kFinalThreads) tc_sncc_final_kernel(SnccArgs a
 #pragma unroll
     for (int k = 0; k < kFinalPairs; ++k) {
       const int p = t + k * kFinalThreads;
-      if (p < ni * M_NGRAD) s_mom[p / M_NGRAD][p % M_NGRAD] = sum[k];
+      if (p < ni * M_NGRAD) {
+        const int li = p / M_NGRAD, m = p - li * M_NGRAD, v = li / cn;
+        s_mom[li][m] = sum[k];
+        // the moment record (consecutive threads, consecutive doubles)
+        a.mom[(static_cast<int64_t>(v) * C + c0 + (li - v * cn)) * kMomStride + m] = sum[k];
+      }
     }
     __syncthreads();
     if (t < ni) {
@@ -546,11 +550,7 @@ __global__ void __launch_bounds__(kFinalThreads) tc_sncc_final_kernel(SnccArgs a
       o[3] = gc * inv * a.kappa * m[M_PHU];
       o[4] = gc * inv * a.kappa * m[M_PHV];
       o[5] = ncc;
-      double* mo = a.mom + it * kMomStride;
-      for (int k = 0; k < M_NGRAD; ++k) mo[k] = m[k];
-      mo[17] = ncc;
-      double* jo = a.jac + it * 18;
-      for (int k = 0; k < 18; ++k) jo[k] = j[k];
+      a.mom[it * kMomStride + 17] = ncc;
       if (a.ncc_out) a.ncc_out[it] = static_cast<float>(ncc);
     }
     __syncthreads();
@@ -893,15 +893,15 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
 // an allocator between steps (cudaMalloc / cudaFree may synchronise the
 // device).
 //
-// Size (about 426 KB per device): kStaticRecords partial-moment records of
-// 17 doubles, and kStaticItems (candidate, view) moment records and axes
-// Jacobians of 18 doubles each.  Calls needing more -- more than 512
-// (candidate, view) pairs, or more than 2048 partial records for the launch
-// variant (sncc_records) -- are refused with FVR_ERR_WORKSPACE before
-// anything is launched.
+// Size (about 352 KB per device): kStaticRecords partial-moment records of
+// 17 doubles and kStaticItems (candidate, view) moment records of 18
+// doubles.  Calls needing more -- more than 512 (candidate, view) pairs, or
+// more than 2048 partial records (pairs x tiles, as the launch variant sizes
+// the tiles) -- are refused with FVR_ERR_WORKSPACE before anything is
+// launched.
 //
-// Start state: none.  The partial, moment and Jacobian records are written
-// by every call before they are read.
+// Start state: none.  The partial and moment records are written by every
+// call before they are read.
 //
 // Set-up: the first call on each device, made with that device current,
 // resolves the array's device address with cudaGetSymbolAddress and caches
@@ -916,8 +916,7 @@ constexpr int64_t kStaticItems = 512;
 constexpr int64_t kStaticRecords = 2048;
 constexpr int64_t kStaticPartialDoubles = kStaticRecords * M_NGRAD;
 constexpr int64_t kStaticMomDoubles = kStaticItems * kMomStride;
-constexpr int64_t kStaticJacDoubles = kStaticItems * 18;
-constexpr int64_t kStaticDoubles = kStaticPartialDoubles + kStaticMomDoubles + kStaticJacDoubles;
+constexpr int64_t kStaticDoubles = kStaticPartialDoubles + kStaticMomDoubles;
 constexpr int kStaticMaxDevices = 64;
 
 static __device__ __align__(256) double g_sncc_static_scratch[kStaticDoubles];
@@ -995,11 +994,11 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
   return FVR_OK;
 }
 
-// Fused workspace: partial records | moments [nv][C][18] | axes Jacobians
-// [nv][C][18]; every region is written by a call before it is read.
+// Fused workspace: partial records | moments [nv][C][18]; both written by a
+// call before they are read.
 int64_t fvr_tc_sncc_fused_workspace(int64_t C, int64_t R, int64_t nviews) {
   if (C < 1 || R < 1 || nviews < 1) return 0;
-  return fvr_tc_sncc_workspace(C, R, nviews) + 2 * nviews * C * kMomStride * (int64_t)sizeof(double);
+  return fvr_tc_sncc_workspace(C, R, nviews) + nviews * C * kMomStride * (int64_t)sizeof(double);
 }
 
 int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
@@ -1019,9 +1018,7 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
   if (ws_bytes < fvr_tc_sncc_fused_workspace(C, R, nviews)) return FVR_ERR_WORKSPACE;
   char* ws = static_cast<char*>(workspace);
   a.partial = reinterpret_cast<double*>(ws);
-  const int64_t mom_bytes = nviews * C * kMomStride * (int64_t)sizeof(double);
   a.mom = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews));
-  a.jac = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews) + mom_bytes);
   a.loss = loss;
   a.ncc_out = ncc_out;
   a.grad = grad_poses;
@@ -1153,7 +1150,6 @@ int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const floa
   if (rc) return rc;
   a.partial = scratch;
   a.mom = scratch + kStaticPartialDoubles;
-  a.jac = scratch + kStaticPartialDoubles + kStaticMomDoubles;
   a.loss = loss;
   a.ncc_out = ncc_out;
   a.grad = grad_poses;

@@ -34,11 +34,12 @@ def _l2_flush(device):
     return t
 
 
-def choose(kind, key, run, n_variants, reps=5):
+def choose(kind, key, run, n_variants, reps=5, candidates=None):
     """Return the fastest variant of ``run(variant)`` (launches one kernel) for
     ``key``: the median of ``reps`` launches per variant, each after an L2
     rewrite (the flush also keeps the device busy while the launch is
-    enqueued, so the events time the launch alone)."""
+    enqueued, so the events time the launch alone).  ``candidates``
+    restricts the variants tried (default: all)."""
     env = os.environ.get(f"FVR_{kind.upper()}_VARIANT")
     if env is not None:
         return int(env)
@@ -49,7 +50,7 @@ def choose(kind, key, run, n_variants, reps=5):
         return 0
     flush = _l2_flush(torch.cuda.current_device())
     best, best_ms, times = 0, float("inf"), []
-    for v in range(n_variants):
+    for v in (range(n_variants) if candidates is None else candidates):
         try:
             run(v)
         except L.FvrError:  # this shape does not fit the variant (e.g. its shared memory)
@@ -70,7 +71,7 @@ def choose(kind, key, run, n_variants, reps=5):
         if ms < best_ms:
             best, best_ms = v, ms
     _cache[k] = best
-    _timings[k] = times
+    _timings[k] = times  # per candidate, in the order tried
     return best
 
 

@@ -75,6 +75,13 @@ def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
     return mom, loss
 
 
+# Launch variants the value-and-gradient path chooses from: those whose
+# gradient kernel keeps every value in registers (the 3- and 4-CTA-per-SM
+# register budgets spill the 17 moment pairs); the variant table is in
+# csrc/fvr_tc.cu (kSnccVariantTable).
+_FUSED_VARIANTS = (0, 3, 6, 7)
+
+
 def _sncc_fused(eng, p, views, ftargs, hp, R, out=None):
     """Moments kernel + its dependent epilogue: per-candidate finalize and pose
     gradient, view losses.  Returns (loss [nv + 1] f32, grad [C, 6] f32).  The
@@ -106,7 +113,8 @@ def _sncc_fused(eng, p, views, ftargs, hp, R, out=None):
         L.call("fvr_tc_sncc_value_and_grad", *st.args(), L.ptr(p), C, nv, vcodes, fptrs, L.ptr(hp), L.ptr(lin), R, kap,
                int(variant), None, 0, L.ptr(ws), ws_bytes, L.ptr(loss), None, L.ptr(grad), 0, s)
 
-    variant = autotune.choose("sncc_fused", (st.code, C, R, nv, st.dims), run, L.load().fvr_tc_sncc_variants())
+    variant = autotune.choose("sncc_fused", (st.code, C, R, nv, st.dims), run, L.load().fvr_tc_sncc_variants(),
+                              candidates=_FUSED_VARIANTS)
     with profiling.section("tc_sncc_moments"):
         run(variant)
     return loss, grad

@@ -163,7 +163,7 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
                                void* stream);
 /* Allocation-free form of fvr_tc_sncc_value_and_grad (no counterpart in the
  * reference): same arguments and results, but the workspace is a fixed
- * per-device scratch array inside the library (about 426 KB), so the call
+ * per-device scratch array inside the library (about 352 KB), so the call
  * allocates nothing.  For callers that cannot allocate device memory where
  * they call (a host linking only this C ABI, with no device allocator; a
  * loop that must not enter an allocator between steps).
