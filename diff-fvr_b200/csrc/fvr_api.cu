@@ -1,7 +1,34 @@
 // Status strings, version and device checks of the C ABI.
 #include "fvr_common.cuh"
 
+namespace {
+
+// dst[0..n) = src[0..n); 16-byte words when both ends and n allow it.
+__global__ void __launch_bounds__(256) copy_bytes_kernel(unsigned char* __restrict__ dst,
+                                                         const unsigned char* __restrict__ src, int64_t n) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  const bool wide = ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15) == 0;
+  const int64_t nw = wide ? n / 16 : 0;
+  for (int64_t i = t; i < nw; i += stride)
+    reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+  for (int64_t i = nw * 16 + t; i < n; i += stride) dst[i] = src[i];
+}
+
+}  // namespace
+
 extern "C" {
+
+int fvr_copy_bytes(void* dst, const void* src, int64_t n, void* stream) {
+  if (!dst || !src || n < 0) return FVR_ERR_ARG;
+  if (n == 0) return FVR_OK;
+  const int64_t blocks = (n / 16 + 255) / 256;
+  copy_bytes_kernel<<<static_cast<unsigned>(blocks < 1 ? 1 : (blocks > 1184 ? 1184 : blocks)), 256, 0,
+                      static_cast<cudaStream_t>(stream)>>>(static_cast<unsigned char*>(dst),
+                                                           static_cast<const unsigned char*>(src), n);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
 
 const char* fvr_status_string(int status) {
   switch (status) {

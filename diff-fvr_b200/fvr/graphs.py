@@ -17,6 +17,16 @@ import torch
 from . import _lib as L
 
 
+def _copy_kernel(dst, src):
+    """dst <- src (same bytes) by fvr_copy_bytes on the current stream: pinned
+    host buffers are read or written by the kernel itself over the bus, which
+    costs a small kernel node instead of a copy-engine memcpy node."""
+    if dst.numel() * dst.element_size() != src.numel() * src.element_size():
+        raise L.FvrError("copy between buffers of different sizes")
+    L.call("fvr_copy_bytes", L.ptr(dst), L.ptr(src.contiguous()), int(dst.numel() * dst.element_size()),
+           L.stream_ptr())
+
+
 @contextlib.contextmanager
 def no_gc_during_capture():
     """Collect garbage now and keep the cyclic collector off until the block
@@ -41,7 +51,8 @@ class GraphedCallable:
     With ``host_io=True`` the graph also holds the transfers: pinned host
     input buffers (``host_in``) are copied to the device, ``fn`` runs, and its
     outputs are copied into pinned host buffers (``host_out``), so one replay
-    is the whole host-to-host step.  Calling then takes host tensors (or
+    is the whole host-to-host step; the copies are kernels that read or write
+    the pinned buffers directly (``fvr_copy_bytes``).  Calling then takes host tensors (or
     writes nothing when given ``host_in`` itself), replays, and returns
     ``host_out`` after waiting for the stream (``sync=False``: without
     waiting; ``host_out`` is complete once the current stream is)."""
@@ -76,12 +87,12 @@ class GraphedCallable:
             with torch.cuda.graph(self.graph, capture_error_mode="thread_local"):
                 if self.host_io:
                     for s, h in zip(self.static_in, self.host_in):
-                        s.copy_(h, non_blocking=True)
+                        _copy_kernel(s, h)
                 self.static_out = fn(*self.static_in)
                 if self.host_io:
                     outs = self.static_out if isinstance(self.static_out, (tuple, list)) else (self.static_out,)
                     for h, o in zip(self.host_out, outs):
-                        h.copy_(o, non_blocking=True)
+                        _copy_kernel(h, o)
 
     def replay(self):
         self.graph.replay()

@@ -352,6 +352,11 @@ int fvr_hu_to_attenuation(const float* hu, int64_t n, float* out, void* stream);
  * : 0): lets a caller time one kernel inside a captured CUDA graph (no
  * reference counterpart; measurement utility). */
 int fvr_event_record(void* event, void* stream, int external);
+/* dst[0..n) = src[0..n) by a kernel (no reference counterpart): both
+ * pointers may be device memory or pinned host memory (unified addressing),
+ * so a captured step can move its small inputs and outputs between host and
+ * device in kernel nodes instead of copy-engine memcpy nodes. */
+int fvr_copy_bytes(void* dst, const void* src, int64_t n, void* stream);
 /* Gather ceiling of a cell sequence (no reference counterpart; measurement
  * utility): reads the 32-byte entries entries[idx[i]], i < n (an index
  * outside [0, n_entries) reads nothing), three 256-bit loads in flight
