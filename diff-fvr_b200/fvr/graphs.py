@@ -52,12 +52,15 @@ class GraphedCallable:
     input buffers (``host_in``) are copied to the device, ``fn`` runs, and its
     outputs are copied into pinned host buffers (``host_out``), so one replay
     is the whole host-to-host step; the copies are kernels that read or write
-    the pinned buffers directly (``fvr_copy_bytes``).  Calling then takes host tensors (or
+    the pinned buffers directly (``fvr_copy_bytes``).  With
+    ``outputs_on_host=True`` as well, ``fn`` itself returns pinned host tensors
+    that its kernels write, and no output copy is captured.  Calling then takes host tensors (or
     writes nothing when given ``host_in`` itself), replays, and returns
     ``host_out`` after waiting for the stream (``sync=False``: without
     waiting; ``host_out`` is complete once the current stream is)."""
 
-    def __init__(self, fn, *example_inputs, warmup=3, capture_context=None, host_io=False):
+    def __init__(self, fn, *example_inputs, warmup=3, capture_context=None, host_io=False,
+                 outputs_on_host=False):
         for x in example_inputs:
             L.require_cuda(x)
         self.fn = fn
@@ -70,10 +73,12 @@ class GraphedCallable:
                 out = fn(*self.static_in)
         torch.cuda.current_stream().wait_stream(side)
         torch.cuda.synchronize()
+        self.outputs_on_host = bool(host_io and outputs_on_host)
         if self.host_io:
             outs = out if isinstance(out, (tuple, list)) else (out,)
             self.host_in = [torch.empty(x.shape, dtype=x.dtype).pin_memory() for x in self.static_in]
-            self.host_out = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in outs]
+            self.host_out = None if self.outputs_on_host else [torch.empty(o.shape, dtype=o.dtype).pin_memory()
+                                                                for o in outs]
         self.graph = torch.cuda.CUDAGraph()
         n0 = L.launch_count[0]
         with no_gc_during_capture():
@@ -89,8 +94,10 @@ class GraphedCallable:
                     for s, h in zip(self.static_in, self.host_in):
                         _copy_kernel(s, h)
                 self.static_out = fn(*self.static_in)
-                if self.host_io:
-                    outs = self.static_out if isinstance(self.static_out, (tuple, list)) else (self.static_out,)
+                outs = self.static_out if isinstance(self.static_out, (tuple, list)) else (self.static_out,)
+                if self.outputs_on_host:  # fn wrote them into pinned host memory itself
+                    self.host_out = list(outs)
+                elif self.host_io:
                     for h, o in zip(self.host_out, outs):
                         _copy_kernel(h, o)
 
@@ -112,9 +119,9 @@ class GraphedCallable:
         return self.replay()
 
 
-def _biplanar_value_and_grad(engine, f_ap, f_lat, high_pass, sigma, poses):
+def _biplanar_value_and_grad(engine, f_ap, f_lat, high_pass, sigma, poses, out_grad=None, out_loss=None):
     return engine.spectral_ncc_value_and_grad(poses, (f_ap, f_lat), ("ap", "lateral"), high_pass=high_pass,
-                                              cutoff_sigma=sigma)
+                                              cutoff_sigma=sigma, out_grad=out_grad, out_loss=out_loss)
 
 
 class BiplanarSpectralNCCStep:
@@ -129,9 +136,11 @@ class BiplanarSpectralNCCStep:
     keeps that storage alive; capture again after ``to_precision``).
     Returns ``(loss, grad)`` device tensors (scalar, ``[C, 6]``).  With
     ``host_io=True`` (graph only) the step takes host poses and returns pinned
-    host ``(loss, grad)`` tensors: the host-to-device copy, the kernels and the
-    device-to-host copies are one graph replay (``host_poses`` is the pinned
-    input buffer; writing poses there directly skips one host copy).
+    host ``(loss, grad)`` tensors: one graph replay holds a copy kernel that
+    reads the pinned poses and the two kernels of the step, whose epilogue
+    writes the loss and gradient straight into pinned host memory
+    (``host_poses`` is the pinned input buffer; writing poses there directly
+    skips one host copy).
     """
 
     def __init__(self, engine, f_targ_ap, f_targ_lat, n_candidates, high_pass=True, cutoff_sigma=4.0, graph=True,
@@ -146,9 +155,12 @@ class BiplanarSpectralNCCStep:
         # the captured callable holds no reference back to this object (no
         # reference cycle: the step and its graph are freed as soon as dropped)
         fn = functools.partial(_biplanar_value_and_grad, engine, f_targ_ap, f_targ_lat, self.hp, self.sigma)
-        self._g = (GraphedCallable(fn, ex, warmup=warmup, capture_context=capture_context, host_io=host_io)
-                   if graph else None)
         io = graph and host_io
+        if io:  # the epilogue kernel writes loss and gradient straight into pinned host buffers
+            fn = functools.partial(fn, out_grad=torch.empty((int(n_candidates), 6), dtype=torch.float32).pin_memory(),
+                                   out_loss=torch.empty(3, dtype=torch.float32).pin_memory())
+        self._g = (GraphedCallable(fn, ex, warmup=warmup, capture_context=capture_context, host_io=host_io,
+                                   outputs_on_host=io) if graph else None)
         self.host_poses = self._g.host_in[0] if io else None
         self.host_loss, self.host_grad = self._g.host_out if io else (None, None)
 

@@ -82,7 +82,7 @@ def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
 _FUSED_VARIANTS = (0, 3, 6, 7)
 
 
-def _sncc_fused(eng, p, views, ftargs, hp, R, out=None):
+def _sncc_fused(eng, p, views, ftargs, hp, R, out=None, loss_out=None):
     """Moments kernel + its dependent epilogue: per-candidate finalize and pose
     gradient, view losses.  Returns (loss [nv + 1] f32, grad [C, 6] f32).  The
     workspace is cached per shape on the engine, so captured graphs keep a
@@ -97,8 +97,13 @@ def _sncc_fused(eng, p, views, ftargs, hp, R, out=None):
     if ws is None:
         ws = torch.zeros(ws_bytes, dtype=torch.uint8, device=dev)
         eng._fused_ws[key] = ws
-    loss = torch.empty(nv + 1, dtype=torch.float32, device=dev)
+    loss = torch.empty(nv + 1, dtype=torch.float32, device=dev) if loss_out is None else loss_out
     grad = torch.empty((C, 6), dtype=torch.float32, device=dev) if out is None else out
+    for t, shape in ((loss, (nv + 1,)), (grad, (C, 6))):
+        if tuple(t.shape) != shape or t.dtype != torch.float32 or not t.is_contiguous():
+            raise L.FvrError(f"output buffer must be a contiguous float32 tensor of shape {shape}")
+        if not (t.is_cuda or t.is_pinned()):
+            raise L.FvrError("output buffers must be device memory or pinned host memory")
     fts = [f.detach().to(device=dev, dtype=torch.complex64).contiguous() for f in ftargs]
     for f in fts:
         if f.numel() != R * R:
@@ -399,16 +404,19 @@ class TorchDiffFVREngine(nn.Module):
         return _SpectralNCCFn.apply(self._prep_poses(poses), self, codes, hp, R, *f_targs)
 
     def spectral_ncc_value_and_grad(self, poses, f_targs, views=("ap", "lateral"), high_pass=True,
-                                    cutoff_sigma=4.0, out_grad=None):
-        """``(sum_v loss_v, dloss/dposes [C, 6])`` without autograd: one kernel launch
-        gathers every candidate and view, reduces the NCC and pose moments and, in the
-        last CTA of each candidate, forms its fp64 pose gradient (capturable in a CUDA
-        graph).  Launches through one engine must stay on one stream."""
+                                    cutoff_sigma=4.0, out_grad=None, out_loss=None):
+        """``(sum_v loss_v, dloss/dposes [C, 6])`` without autograd: one kernel gathers
+        every candidate and view and reduces the NCC and pose moments; its programmatic
+        dependent forms every candidate's fp64 pose gradient and the view losses
+        (capturable in a CUDA graph).  ``out_grad`` ([C, 6] float32) and ``out_loss``
+        ([len(views) + 1] float32: the view losses, then their sum) receive the results
+        when given; either may be pinned host memory, which the kernel writes directly.
+        Launches through one engine must stay on one stream."""
         p = self._prep_poses(poses).detach().to(torch.float32).contiguous()
         R = int(f_targs[0].shape[-1])
         hp = RT.hp_filter(R, R, cutoff_sigma, self._dev) if high_pass else None
         codes = tuple(_view_code(v) for v in views)
-        loss, grad = _sncc_fused(self, p, codes, f_targs, hp, R, out=out_grad)
+        loss, grad = _sncc_fused(self, p, codes, f_targs, hp, R, out=out_grad, loss_out=out_loss)
         return loss[len(codes)], grad
 
     def spectral_ncc_loss(self, pred_drr: torch.Tensor, target_drr: torch.Tensor, high_pass: bool = True,

@@ -411,8 +411,9 @@ def test_fused_variants_agree_on_ragged_shapes(big, monkeypatch, C, R):
 
 
 def test_host_io_graph_step_matches_device_step(big):
-    """The host-to-host graph (pinned H2D copy, kernels, D2H copies in one
-    replay) returns exactly the device step's loss and gradient."""
+    """The host-to-host graph (pinned-host read of the poses, the kernels, the
+    epilogue writing pinned host outputs, in one replay) returns exactly the
+    device step's loss and gradient."""
     from fvr.graphs import BiplanarSpectralNCCStep
 
     _, eng, _ = big
@@ -426,6 +427,11 @@ def test_host_io_graph_step_matches_device_step(big):
     lh, gh = io_step(torch.from_numpy(poses))
     assert lh.device.type == "cpu" and gh.is_pinned()
     assert float(lh) == float(ld) and torch.equal(gh, gd.cpu())
+    eng.spectral_ncc_value_and_grad(_t(poses), (fa, fl))  # the device step's own loss vector
+    out_loss = torch.empty(3, dtype=torch.float32).pin_memory()
+    eng.spectral_ncc_value_and_grad(_t(poses), (fa, fl), out_loss=out_loss)
+    torch.cuda.synchronize()
+    assert float(out_loss[2]) == float(ld) and float(out_loss[0] + out_loss[1]) == pytest.approx(float(ld), abs=1e-6)
     io_step.host_poses.copy_(torch.from_numpy(tc.make_poses(8, 15)))
     lh2, gh2 = io_step(io_step.host_poses)
     ld2, gd2 = dev_step(_t(tc.make_poses(8, 15)))
