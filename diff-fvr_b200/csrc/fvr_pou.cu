@@ -500,6 +500,26 @@ struct WarpArgs {
   double inv_ds, c_idx;
   int B, N, P, K;
   int64_t ray_stride;
+  int chunk;  // blocks per row-strip round (0: every CTA takes the per-pixel path)
+};
+
+// Row strips.  The pinhole lattice's detector rows share one ray coordinate
+// ry up to the float rounding of the lattice (about 1e-7 relative), so for a
+// CTA whose pixels lie on one row every block is sampled on one image row
+// pair (iy, iy + 1) with one fraction ty.  Such a CTA blends that row pair
+// once per block into a shared-memory strip and interpolates it along x per
+// pixel; the adjoint gathers each pixel's contributions into strips and
+// spreads them onto the two image rows once per block.  A CTA takes this path
+// when its ry spread moves py by at most kWarpRowTolPx image pixels on every
+// block it touches (the row is sampled at the midpoint of its ry range); that
+// shift is far below the fp32 rounding of py in the reference's own kernel.
+constexpr int kWarpStripMax = 16;
+constexpr double kWarpRowTolPx = 1e-4;
+
+struct WarpCull {
+  int nt;      // blocks the CTA samples: tl[0..nt), in increasing order
+  bool rows;   // the row-strip path applies
+  double ry0;  // the row's ray coordinate for that path
 };
 
 // Block culling for a CTA of detector pixels: the box of its live pixels'
@@ -507,11 +527,14 @@ struct WarpArgs {
 // sample inside the block image.  The image coordinate is the same monotone
 // fp64 expression of rx (or ry) that the sampling uses, evaluated at the box
 // corners, so a block is skipped only if no pixel would have sampled it.
+// Surviving blocks are listed in increasing order (touch: per-block flags).
 template <typename OT>
-__device__ __forceinline__ void warp_cull(const WarpArgs<OT>& a, int n, bool live, double rx, double ry,
-                                          unsigned char* touch) {
+__device__ __forceinline__ WarpCull warp_cull(const WarpArgs<OT>& a, int n, bool live, double rx, double ry,
+                                              unsigned char* touch, short* tl) {
   __shared__ double s_box[4][8];
   __shared__ double box[4];
+  __shared__ unsigned s_dbmax;  // max |d_b| over the touched blocks (float bits; non-negative floats order as ints)
+  __shared__ int s_nt;
   const double inf = 1e300;
   double v[4] = {live ? rx : inf, live ? -rx : inf, live ? ry : inf, live ? -ry : inf};  // mins of +-r
 #pragma unroll
@@ -520,6 +543,7 @@ __device__ __forceinline__ void warp_cull(const WarpArgs<OT>& a, int n, bool liv
     for (int o = 16; o > 0; o >>= 1) v[k] = fmin(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
     if ((threadIdx.x & 31) == 0) s_box[k][threadIdx.x >> 5] = v[k];
   }
+  if (threadIdx.x == 0) s_dbmax = 0u;
   __syncthreads();
   if (threadIdx.x < 4) {
     double m = inf;
@@ -535,119 +559,308 @@ __device__ __forceinline__ void warp_cull(const WarpArgs<OT>& a, int n, bool liv
     const double x0 = (db * box[0] - cu) * a.inv_ds + a.c_idx, x1 = (db * -box[1] - cu) * a.inv_ds + a.c_idx;
     const double y0 = (db * box[2] - cv) * a.inv_ds + a.c_idx, y1 = (db * -box[3] - cv) * a.inv_ds + a.c_idx;
     const double P = static_cast<double>(a.P);
-    touch[b] = any && fmax(x0, x1) > -1.0 && fmin(x0, x1) < P && fmax(y0, y1) > -1.0 && fmin(y0, y1) < P;
+    const bool t = any && fmax(x0, x1) > -1.0 && fmin(x0, x1) < P && fmax(y0, y1) > -1.0 && fmin(y0, y1) < P;
+    touch[b] = t;
+    if (t) atomicMax(&s_dbmax, __float_as_uint(static_cast<float>(fabs(db)) * 1.001f));
   }
   __syncthreads();
+  if (threadIdx.x < 32) {  // ordered compaction by warp 0
+    const int lane = threadIdx.x;
+    int base = 0;
+    for (int c0 = 0; c0 < a.B; c0 += 32) {
+      const int b = c0 + lane;
+      const bool f = b < a.B && touch[b];
+      const unsigned m = __ballot_sync(0xffffffffu, f);
+      if (f) tl[base + __popc(m & ((1u << lane) - 1u))] = static_cast<short>(b);
+      base += __popc(m);
+    }
+    if (lane == 0) s_nt = base;
+  }
+  __syncthreads();
+  WarpCull wc;
+  wc.nt = s_nt;
+  const double lo = box[2], hi = -box[3];
+  wc.ry0 = any ? 0.5 * (lo + hi) : 0.0;
+  wc.rows = a.chunk > 0 && any &&
+            0.5 * (hi - lo) * static_cast<double>(__uint_as_float(s_dbmax)) * fabs(a.inv_ds) <= kWarpRowTolPx;
+  return wc;
+}
+
+// Per block of a row-strip round: d_b and cu (for the per-pixel x), the
+// image row iy (-2: the row misses the image) and fraction ty.
+struct WarpRow {
+  double db, cu;
+  int iy;
+  float ty;
+};
+
+template <typename OT>
+__device__ __forceinline__ WarpRow warp_row(const WarpArgs<OT>& a, int64_t bn, double ry0) {
+  WarpRow r;
+  r.db = static_cast<double>(a.db[bn * a.ostride]);
+  r.cu = static_cast<double>(a.cu[bn * a.ostride]);
+  const double cv = static_cast<double>(a.cv[bn * a.ostride]);
+  const double py = (r.db * ry0 - cv) * a.inv_ds + a.c_idx;
+  r.iy = -2;
+  r.ty = 0.f;
+  if (py > -1.0 && py < static_cast<double>(a.P)) {
+    const double fy = floor(py);
+    r.iy = static_cast<int>(fy);
+    r.ty = static_cast<float>(py - fy);
+  }
+  return r;
+}
+
+// Image rows iy and iy + 1 of block image bn at column x (zero outside).
+__device__ __forceinline__ void warp_row_pair(const float* img, int P, int iy, int x, float& r0, float& r1) {
+  const bool xin = x >= 0 && x < P;
+  r0 = xin && iy >= 0 && iy < P ? __ldg(img + static_cast<int64_t>(iy) * P + x) : 0.f;
+  r1 = xin && iy + 1 >= 0 && iy + 1 < P ? __ldg(img + static_cast<int64_t>(iy + 1) * P + x) : 0.f;
+}
+
+// Row-strip forward of one CTA: the pixel's sum over the listed blocks in
+// list order.  Strip k holds the blend rb[x] = (1 - ty) img[iy][x] + ty
+// img[iy + 1][x] at index x + 1 for x in [-1, P] (zero outside the image).
+template <typename OT>
+__device__ float warp_rows_forward(const WarpArgs<OT>& a, int n, bool live, double rx, const WarpCull& wc,
+                                   const short* tl, float* strip) {
+  __shared__ WarpRow s_row[kWarpStripMax];
+  const int P = a.P, W2 = P + 2;
+  float acc = 0.f;
+  for (int c0 = 0; c0 < wc.nt; c0 += a.chunk) {
+    const int cn = min(a.chunk, wc.nt - c0);
+    __syncthreads();  // the previous round's strips are no longer read
+    if (threadIdx.x < cn) s_row[threadIdx.x] = warp_row(a, static_cast<int64_t>(tl[c0 + threadIdx.x]) * a.N + n, wc.ry0);
+    __syncthreads();
+    // element e = k * W2 + xr of the strips, walked without a division per element
+    for (int k = threadIdx.x / W2, xr = threadIdx.x % W2; k < cn;) {
+      float r0, r1;
+      warp_row_pair(a.imgs + (static_cast<int64_t>(tl[c0 + k]) * a.N + n) * P * P, P, s_row[k].iy, xr - 1, r0, r1);
+      strip[k * W2 + xr] = r0 * (1.f - s_row[k].ty) + r1 * s_row[k].ty;
+      for (xr += blockDim.x; xr >= W2; xr -= W2) ++k;
+    }
+    __syncthreads();
+    if (live) {
+      for (int k = 0; k < cn; ++k) {
+        const double px = (s_row[k].db * rx - s_row[k].cu) * a.inv_ds + a.c_idx;
+        if (px > -1.0 && px < static_cast<double>(P)) {
+          const double fx = floor(px);
+          const float tx = static_cast<float>(px - fx);
+          const float* r = strip + k * W2 + static_cast<int>(fx) + 1;
+          acc += r[0] * (1.f - tx) + r[1] * tx;
+        }
+      }
+    }
+  }
+  return acc;
+}
+
+// Row-strip adjoint of one CTA.  Per block k, five strips (index x + 1 for
+// x in [-1, P]): rb (the row blend) and dr = img[iy + 1] - img[iy]; then, per
+// pixel with weight g at column ix, fraction tx:
+//   S[ix] += g (1 - tx), S[ix + 1] += g tx,  Gs[ix] += g,  Gr[ix] += g rx.
+// With dpx = (rb[ix + 1] - rb[ix]) / ds and dpy = (dr[ix] (1 - tx) + dr[ix + 1] tx) / ds
+// (the bilinear image derivatives at the pixel), summing by columns gives
+//   sum g dpx rx = sum_x rb[x] (Gr[x - 1] - Gr[x]) / ds,  sum g dpx = sum_x rb[x] (Gs[x - 1] - Gs[x]) / ds,
+//   sum g dpy = sum_x dr[x] S[x] / ds,
+// and dL/dimg[iy][x] += (1 - ty) S[x], dL/dimg[iy + 1][x] += ty S[x].
+template <typename OT>
+__device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, double rx, float g, const WarpCull& wc,
+                                  const short* tl, float* strip, float* __restrict__ grad_imgs, double* sacc) {
+  __shared__ WarpRow s_row[kWarpStripMax];
+  const int P = a.P, W2 = P + 2;
+  const int plane = a.chunk * W2;
+  float* rb = strip;
+  float* dr = strip + plane;
+  float* S = strip + 2 * plane;
+  float* Gs = strip + 3 * plane;
+  float* Gr = strip + 4 * plane;
+  const float rxf = static_cast<float>(rx), ryf = static_cast<float>(wc.ry0);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c0 = 0; c0 < wc.nt; c0 += a.chunk) {
+    const int cn = min(a.chunk, wc.nt - c0);
+    __syncthreads();  // the previous round's strips are no longer read
+    if (threadIdx.x < cn) s_row[threadIdx.x] = warp_row(a, static_cast<int64_t>(tl[c0 + threadIdx.x]) * a.N + n, wc.ry0);
+    __syncthreads();
+    for (int k = threadIdx.x / W2, xr = threadIdx.x % W2; k < cn;) {
+      float r0, r1;
+      warp_row_pair(a.imgs + (static_cast<int64_t>(tl[c0 + k]) * a.N + n) * P * P, P, s_row[k].iy, xr - 1, r0, r1);
+      const int e = k * W2 + xr;
+      rb[e] = r0 * (1.f - s_row[k].ty) + r1 * s_row[k].ty;
+      dr[e] = r1 - r0;
+      S[e] = 0.f;
+      Gs[e] = 0.f;
+      Gr[e] = 0.f;
+      for (xr += blockDim.x; xr >= W2; xr -= W2) ++k;
+    }
+    __syncthreads();
+    if (live) {
+      for (int k = 0; k < cn; ++k) {
+        const double px = (s_row[k].db * rx - s_row[k].cu) * a.inv_ds + a.c_idx;
+        if (px > -1.0 && px < static_cast<double>(P)) {
+          const double fx = floor(px);
+          const float tx = static_cast<float>(px - fx);
+          const int o = k * W2 + static_cast<int>(fx) + 1;
+          atomicAdd(S + o, g * (1.f - tx));
+          atomicAdd(S + o + 1, g * tx);
+          atomicAdd(Gs + o, g);
+          atomicAdd(Gr + o, g * rxf);
+        }
+      }
+    }
+    __syncthreads();
+    for (int k = wid; k < cn; k += nw) {  // one warp per block
+      const int b = tl[c0 + k];
+      const int iy = s_row[k].iy;
+      const float ty = s_row[k].ty;
+      float* gi = grad_imgs ? grad_imgs + (static_cast<int64_t>(b) * a.N + n) * P * P : nullptr;
+      double sa = 0.0, sb = 0.0, sc = 0.0;
+      for (int x = lane; x < P; x += 32) {
+        const int o = k * W2 + x + 1;
+        const double r = static_cast<double>(rb[o]);
+        sa += r * (static_cast<double>(Gr[o - 1]) - static_cast<double>(Gr[o]));
+        sb += r * (static_cast<double>(Gs[o - 1]) - static_cast<double>(Gs[o]));
+        const float sv = S[o];
+        sc += static_cast<double>(dr[o]) * static_cast<double>(sv);
+        if (gi && sv != 0.f) {
+          if (iy >= 0 && iy < P) atomicAdd(gi + static_cast<int64_t>(iy) * P + x, sv * (1.f - ty));
+          if (iy + 1 >= 0 && iy + 1 < P) atomicAdd(gi + static_cast<int64_t>(iy + 1) * P + x, sv * ty);
+        }
+      }
+      sa = warp_sum(sa);
+      sb = warp_sum(sb);
+      sc = warp_sum(sc);
+      if (lane == 0) {  // the only writer of block b's sums in this CTA
+        sacc[3 * b] += a.inv_ds * (sa + static_cast<double>(ryf) * sc);
+        sacc[3 * b + 1] += -a.inv_ds * sb;
+        sacc[3 * b + 2] += -a.inv_ds * sc;
+      }
+    }
+  }
 }
 
 template <typename OT>
 __global__ void __launch_bounds__(256) pou_warp_kernel(WarpArgs<OT> a, float* __restrict__ out) {
-  extern __shared__ unsigned char touch[];  // [B]
+  extern __shared__ __align__(16) unsigned char wsm[];
+  float* strip = reinterpret_cast<float*>(wsm);  // [chunk][P + 2], then the block list, then flags
+  short* tl = reinterpret_cast<short*>(strip + static_cast<int64_t>(a.chunk) * (a.P + 2));
+  unsigned char* touch = reinterpret_cast<unsigned char*>(tl + a.B);
   const int n = blockIdx.y;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = q < a.K;
   const int64_t rq = n * a.ray_stride + q;
   const double rx = live ? __ldg(a.rx + rq) : 0.0, ry = live ? __ldg(a.ry + rq) : 0.0;
-  warp_cull(a, n, live, rx, ry, touch);
-  if (!live) return;
-  const int P = a.P;
+  const WarpCull wc = warp_cull(a, n, live, rx, ry, touch, tl);
   float acc = 0.f;
-  for (int b = 0; b < a.B; ++b) {
-    if (!touch[b]) continue;
-    const int64_t bn = static_cast<int64_t>(b) * a.N + n;
-    const double db = static_cast<double>(a.db[bn * a.ostride]);
-    const double px = (db * rx - static_cast<double>(a.cu[bn * a.ostride])) * a.inv_ds + a.c_idx;
-    const double py = (db * ry - static_cast<double>(a.cv[bn * a.ostride])) * a.inv_ds + a.c_idx;
-    if (!(px > -1.0 && px < static_cast<double>(P) && py > -1.0 && py < static_cast<double>(P))) continue;
-    const double fx = floor(px), fy = floor(py);
-    const int ix = static_cast<int>(fx), iy = static_cast<int>(fy);
-    const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
-    const float* img = a.imgs + bn * P * P;
-    const bool x0 = ix >= 0, x1 = ix + 1 < P, y0 = iy >= 0, y1 = iy + 1 < P;
-    const float v00 = (x0 && y0) ? __ldg(img + iy * P + ix) : 0.f;
-    const float v01 = (x1 && y0) ? __ldg(img + iy * P + ix + 1) : 0.f;
-    const float v10 = (x0 && y1) ? __ldg(img + (iy + 1) * P + ix) : 0.f;
-    const float v11 = (x1 && y1) ? __ldg(img + (iy + 1) * P + ix + 1) : 0.f;
-    acc += (v00 * (1.f - tx) + v01 * tx) * (1.f - ty) + (v10 * (1.f - tx) + v11 * tx) * ty;
+  if (wc.rows) {
+    acc = warp_rows_forward(a, n, live, rx, wc, tl, strip);
+    if (!live) return;
+  } else {
+    if (!live) return;
+    const int P = a.P;
+    for (int i = 0; i < wc.nt; ++i) {
+      const int64_t bn = static_cast<int64_t>(tl[i]) * a.N + n;
+      const double db = static_cast<double>(a.db[bn * a.ostride]);
+      const double px = (db * rx - static_cast<double>(a.cu[bn * a.ostride])) * a.inv_ds + a.c_idx;
+      const double py = (db * ry - static_cast<double>(a.cv[bn * a.ostride])) * a.inv_ds + a.c_idx;
+      if (!(px > -1.0 && px < static_cast<double>(P) && py > -1.0 && py < static_cast<double>(P))) continue;
+      const double fx = floor(px), fy = floor(py);
+      const int ix = static_cast<int>(fx), iy = static_cast<int>(fy);
+      const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
+      const float* img = a.imgs + bn * P * P;
+      const bool x0 = ix >= 0, x1 = ix + 1 < P, y0 = iy >= 0, y1 = iy + 1 < P;
+      const float v00 = (x0 && y0) ? __ldg(img + iy * P + ix) : 0.f;
+      const float v01 = (x1 && y0) ? __ldg(img + iy * P + ix + 1) : 0.f;
+      const float v10 = (x0 && y1) ? __ldg(img + (iy + 1) * P + ix) : 0.f;
+      const float v11 = (x1 && y1) ? __ldg(img + (iy + 1) * P + ix + 1) : 0.f;
+      acc += (v00 * (1.f - tx) + v01 * tx) * (1.f - ty) + (v10 * (1.f - tx) + v11 * tx) * ty;
+    }
   }
   out[static_cast<int64_t>(n) * a.K + q] = acc * __ldg(a.ic + rq);
 }
 
 // Adjoint: grad_imgs (scatter, red.global.add) and per-(b, n) partial sums of
 // dL/d(d_b, cu, cv) reduced warp -> CTA (fp64 in shared memory) ->
-// partial[n][tile][b][3].
+// partial[n][tile][b][3]; one-row CTAs without ray gradients take the
+// row-strip path.
 template <typename OT>
 __global__ void __launch_bounds__(256) pou_warp_bwd_kernel(WarpArgs<OT> a, const float* __restrict__ gout,
                                                            float* __restrict__ grad_imgs,
                                                            double* __restrict__ partial,
                                                            float* __restrict__ gray) {
-  extern __shared__ double sacc[];  // [B][3], then touch[B]
-  unsigned char* touch = reinterpret_cast<unsigned char*>(sacc + 3 * a.B);
+  extern __shared__ double sacc[];  // [B][3], strips [5][chunk][P + 2], the block list, flags
+  float* strip = reinterpret_cast<float*>(sacc + 3 * a.B);
+  short* tl = reinterpret_cast<short*>(strip + 5 * static_cast<int64_t>(a.chunk) * (a.P + 2));
+  unsigned char* touch = reinterpret_cast<unsigned char*>(tl + a.B);
   const int n = blockIdx.y;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   for (int i = threadIdx.x; i < 3 * a.B; i += blockDim.x) sacc[i] = 0.0;
   const bool live = q < a.K;
   const int64_t rq = n * a.ray_stride + q;
   const double rx = live ? __ldg(a.rx + rq) : 0.0, ry = live ? __ldg(a.ry + rq) : 0.0;
-  warp_cull(a, n, live, rx, ry, touch);
+  const WarpCull wc = warp_cull(a, n, live, rx, ry, touch, tl);
   const float g = live ? __ldg(gout + static_cast<int64_t>(n) * a.K + q) * __ldg(a.ic + rq) : 0.f;
-  const int P = a.P;
-  const float inv_ds = static_cast<float>(a.inv_ds);
-  float grx = 0.f, gry = 0.f, ssum = 0.f;  // explicit rays: dL/drx, dL/dry, sum_b sample
-  for (int b = 0; b < a.B; ++b) {
-    if (!touch[b]) continue;  // no pixel of this CTA samples block b
-    const int64_t bn = static_cast<int64_t>(b) * a.N + n;
-    float gdb = 0.f, gcu = 0.f, gcv = 0.f;
-    bool hit = false;
-    if (live) {
-      const double db = static_cast<double>(a.db[bn * a.ostride]);
-      const double px = (db * rx - static_cast<double>(a.cu[bn * a.ostride])) * a.inv_ds + a.c_idx;
-      const double py = (db * ry - static_cast<double>(a.cv[bn * a.ostride])) * a.inv_ds + a.c_idx;
-      if (px > -1.0 && px < static_cast<double>(P) && py > -1.0 && py < static_cast<double>(P)) {
-        hit = true;
-        const double fx = floor(px), fy = floor(py);
-        const int ix = static_cast<int>(fx), iy = static_cast<int>(fy);
-        const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
-        const float* img = a.imgs + bn * P * P;
-        const bool x0 = ix >= 0, x1 = ix + 1 < P, y0 = iy >= 0, y1 = iy + 1 < P;
-        const float v00 = (x0 && y0) ? __ldg(img + iy * P + ix) : 0.f;
-        const float v01 = (x1 && y0) ? __ldg(img + iy * P + ix + 1) : 0.f;
-        const float v10 = (x0 && y1) ? __ldg(img + (iy + 1) * P + ix) : 0.f;
-        const float v11 = (x1 && y1) ? __ldg(img + (iy + 1) * P + ix + 1) : 0.f;
-        if (grad_imgs) {
-          float* gi = grad_imgs + bn * P * P;
-          if (x0 && y0) atomicAdd(gi + iy * P + ix, g * (1.f - tx) * (1.f - ty));
-          if (x1 && y0) atomicAdd(gi + iy * P + ix + 1, g * tx * (1.f - ty));
-          if (x0 && y1) atomicAdd(gi + (iy + 1) * P + ix, g * (1.f - tx) * ty);
-          if (x1 && y1) atomicAdd(gi + (iy + 1) * P + ix + 1, g * tx * ty);
-        }
-        const float dpx = ((v01 - v00) * (1.f - ty) + (v11 - v10) * ty) * inv_ds;
-        const float dpy = ((v10 - v00) * (1.f - tx) + (v11 - v01) * tx) * inv_ds;
-        gdb = g * (dpx * static_cast<float>(rx) + dpy * static_cast<float>(ry));
-        gcu = -g * dpx;
-        gcv = -g * dpy;
-        if (gray) {
-          const float dbf = static_cast<float>(db);
-          grx += g * dpx * dbf;
-          gry += g * dpy * dbf;
-          ssum += (v00 * (1.f - tx) + v01 * tx) * (1.f - ty) + (v10 * (1.f - tx) + v11 * tx) * ty;
+  if (wc.rows && !gray) {
+    warp_rows_adjoint(a, n, live, rx, g, wc, tl, strip, grad_imgs, sacc);
+  } else {
+    const int P = a.P;
+    const float inv_ds = static_cast<float>(a.inv_ds);
+    float grx = 0.f, gry = 0.f, ssum = 0.f;  // explicit rays: dL/drx, dL/dry, sum_b sample
+    for (int i = 0; i < wc.nt; ++i) {
+      const int b = tl[i];
+      const int64_t bn = static_cast<int64_t>(b) * a.N + n;
+      float gdb = 0.f, gcu = 0.f, gcv = 0.f;
+      bool hit = false;
+      if (live) {
+        const double db = static_cast<double>(a.db[bn * a.ostride]);
+        const double px = (db * rx - static_cast<double>(a.cu[bn * a.ostride])) * a.inv_ds + a.c_idx;
+        const double py = (db * ry - static_cast<double>(a.cv[bn * a.ostride])) * a.inv_ds + a.c_idx;
+        if (px > -1.0 && px < static_cast<double>(P) && py > -1.0 && py < static_cast<double>(P)) {
+          hit = true;
+          const double fx = floor(px), fy = floor(py);
+          const int ix = static_cast<int>(fx), iy = static_cast<int>(fy);
+          const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
+          const float* img = a.imgs + bn * P * P;
+          const bool x0 = ix >= 0, x1 = ix + 1 < P, y0 = iy >= 0, y1 = iy + 1 < P;
+          const float v00 = (x0 && y0) ? __ldg(img + iy * P + ix) : 0.f;
+          const float v01 = (x1 && y0) ? __ldg(img + iy * P + ix + 1) : 0.f;
+          const float v10 = (x0 && y1) ? __ldg(img + (iy + 1) * P + ix) : 0.f;
+          const float v11 = (x1 && y1) ? __ldg(img + (iy + 1) * P + ix + 1) : 0.f;
+          if (grad_imgs) {
+            float* gi = grad_imgs + bn * P * P;
+            if (x0 && y0) atomicAdd(gi + iy * P + ix, g * (1.f - tx) * (1.f - ty));
+            if (x1 && y0) atomicAdd(gi + iy * P + ix + 1, g * tx * (1.f - ty));
+            if (x0 && y1) atomicAdd(gi + (iy + 1) * P + ix, g * (1.f - tx) * ty);
+            if (x1 && y1) atomicAdd(gi + (iy + 1) * P + ix + 1, g * tx * ty);
+          }
+          const float dpx = ((v01 - v00) * (1.f - ty) + (v11 - v10) * ty) * inv_ds;
+          const float dpy = ((v10 - v00) * (1.f - tx) + (v11 - v01) * tx) * inv_ds;
+          gdb = g * (dpx * static_cast<float>(rx) + dpy * static_cast<float>(ry));
+          gcu = -g * dpx;
+          gcv = -g * dpy;
+          if (gray) {
+            const float dbf = static_cast<float>(db);
+            grx += g * dpx * dbf;
+            gry += g * dpy * dbf;
+            ssum += (v00 * (1.f - tx) + v01 * tx) * (1.f - ty) + (v10 * (1.f - tx) + v11 * tx) * ty;
+          }
         }
       }
+      if (!__any_sync(0xffffffffu, hit)) continue;  // nothing to add from this warp
+      const double s0 = warp_sum(static_cast<double>(gdb)), s1 = warp_sum(static_cast<double>(gcu)),
+                   s2 = warp_sum(static_cast<double>(gcv));
+      if ((threadIdx.x & 31) == 0) {
+        atomicAdd(sacc + 3 * b, s0);
+        atomicAdd(sacc + 3 * b + 1, s1);
+        atomicAdd(sacc + 3 * b + 2, s2);
+      }
     }
-    if (!__any_sync(0xffffffffu, hit)) continue;  // nothing to add from this warp
-    const double s0 = warp_sum(static_cast<double>(gdb)), s1 = warp_sum(static_cast<double>(gcu)),
-                 s2 = warp_sum(static_cast<double>(gcv));
-    if ((threadIdx.x & 31) == 0) {
-      atomicAdd(sacc + 3 * b, s0);
-      atomicAdd(sacc + 3 * b + 1, s1);
-      atomicAdd(sacc + 3 * b + 2, s2);
+    if (gray && live) {
+      float* o = gray + (static_cast<int64_t>(n) * a.K + q) * 3;
+      o[0] = grx;
+      o[1] = gry;
+      o[2] = __ldg(gout + static_cast<int64_t>(n) * a.K + q) * ssum;  // direct dL/dic
     }
-  }
-  if (gray && live) {
-    float* o = gray + (static_cast<int64_t>(n) * a.K + q) * 3;
-    o[0] = grx;
-    o[1] = gry;
-    o[2] = __ldg(gout + static_cast<int64_t>(n) * a.K + q) * ssum;  // direct dL/dic
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 3 * a.B; i += blockDim.x)
@@ -878,6 +1091,22 @@ static int pou_image_dispatch(bool adjoint, const PouSliceArgs& a, int B, const 
   return FVR_ERR_UNSUPPORTED;
 }
 
+// Blocks per row-strip round for `planes` strips of P + 2 floats each (about
+// 42 KB of shared memory at most; 0 turns the path off for very wide images).
+static int warp_strip_chunk(int64_t P, int planes) {
+  const int64_t per_block = static_cast<int64_t>(planes) * (P + 2) * static_cast<int64_t>(sizeof(float));
+  const int64_t c = (42 * 1024) / per_block;
+  return static_cast<int>(c < kWarpStripMax ? c : kWarpStripMax);
+}
+
+// Opt a warp kernel in to `sm` bytes of dynamic shared memory when that is
+// above the default 48 KB.
+template <typename K>
+static bool warp_smem_ok(K kernel, size_t sm) {
+  return sm <= 48 * 1024 ||
+         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sm)) == cudaSuccess;
+}
+
 static int pou_image_common(bool adjoint, int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
                             const double* geo, int64_t N, const float* freqs, const float* gimg, float* imgs,
                             double* part, void* stream) {
@@ -1018,20 +1247,25 @@ int fvr_pou_slice_image_adjoint(int dtype, const void* stencil, const float* sca
 int fvr_pou_warp(const float* imgs, int64_t B, int64_t N, int64_t P, const void* db, const void* cu, const void* cv,
                  int offs_f64, int64_t ostride, const float* rx, const float* ry, const float* ic, int64_t K,
                  int64_t ray_stride, double inv_ds, double c_idx, float* out, void* stream) {
-  if (!imgs || !db || !cu || !cv || !rx || !ry || !ic || !out || B < 1 || N < 1 || P < 2 || K < 1 || N > 65535)
+  if (!imgs || !db || !cu || !cv || !rx || !ry || !ic || !out || B < 1 || N < 1 || P < 2 || K < 1 || N > 65535 ||
+      B > 4096)
     return FVR_ERR_ARG;
   dim3 grid(static_cast<unsigned>(cdiv64(K, 256)), static_cast<unsigned>(N));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int chunk = warp_strip_chunk(P, 1);
+  const size_t sm = static_cast<size_t>(chunk) * (P + 2) * sizeof(float) + 3 * static_cast<size_t>(B);
   if (offs_f64) {
     WarpArgs<double> a{imgs, static_cast<const double*>(db), static_cast<const double*>(cu),
                        static_cast<const double*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
-                       (int)P, (int)K, ray_stride};
-    pou_warp_kernel<double><<<grid, 256, static_cast<size_t>(B), s>>>(a, out);
+                       (int)P, (int)K, ray_stride, chunk};
+    if (!warp_smem_ok(pou_warp_kernel<double>, sm)) return FVR_ERR_CUDA;
+    pou_warp_kernel<double><<<grid, 256, sm, s>>>(a, out);
   } else {
     WarpArgs<float> a{imgs, static_cast<const float*>(db), static_cast<const float*>(cu),
                       static_cast<const float*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
-                      (int)P, (int)K, ray_stride};
-    pou_warp_kernel<float><<<grid, 256, static_cast<size_t>(B), s>>>(a, out);
+                      (int)P, (int)K, ray_stride, chunk};
+    if (!warp_smem_ok(pou_warp_kernel<float>, sm)) return FVR_ERR_CUDA;
+    pou_warp_kernel<float><<<grid, 256, sm, s>>>(a, out);
   }
   FVR_LAUNCH_CHECK();
   return FVR_OK;
@@ -1052,25 +1286,20 @@ int fvr_pou_warp_bwd(const float* imgs, int64_t B, int64_t N, int64_t P, const v
   const int tiles = static_cast<int>(cdiv64(K, 256));
   dim3 grid(static_cast<unsigned>(tiles), static_cast<unsigned>(N));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t sm = 3 * B * sizeof(double) + B;
+  const int chunk = gray ? 0 : warp_strip_chunk(P, 5);
+  const size_t sm = 3 * B * sizeof(double) + static_cast<size_t>(5 * chunk) * (P + 2) * sizeof(float) + 3 * B;
   double* part = static_cast<double*>(workspace);
   if (offs_f64) {
     WarpArgs<double> a{imgs, static_cast<const double*>(db), static_cast<const double*>(cu),
                        static_cast<const double*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
-                       (int)P, (int)K, ray_stride};
-    if (sm > 48 * 1024 &&
-        cudaFuncSetAttribute(pou_warp_bwd_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
-            cudaSuccess)
-      return FVR_ERR_CUDA;
+                       (int)P, (int)K, ray_stride, chunk};
+    if (!warp_smem_ok(pou_warp_bwd_kernel<double>, sm)) return FVR_ERR_CUDA;
     pou_warp_bwd_kernel<double><<<grid, 256, sm, s>>>(a, gout, grad_imgs, part, gray);
   } else {
     WarpArgs<float> a{imgs, static_cast<const float*>(db), static_cast<const float*>(cu),
                       static_cast<const float*>(cv), (int)ostride, rx, ry, ic, inv_ds, c_idx, (int)B, (int)N,
-                      (int)P, (int)K, ray_stride};
-    if (sm > 48 * 1024 &&
-        cudaFuncSetAttribute(pou_warp_bwd_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
-            cudaSuccess)
-      return FVR_ERR_CUDA;
+                      (int)P, (int)K, ray_stride, chunk};
+    if (!warp_smem_ok(pou_warp_bwd_kernel<float>, sm)) return FVR_ERR_CUDA;
     pou_warp_bwd_kernel<float><<<grid, 256, sm, s>>>(a, gout, grad_imgs, part, gray);
   }
   FVR_LAUNCH_CHECK();

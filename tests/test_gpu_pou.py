@@ -202,6 +202,45 @@ def test_batched_equals_single_and_bf16_parity():
     assert float(m2.grad.abs().sum()) > 1e-4
 
 
+@pytest.mark.parametrize("W,pinhole", [(256, False), (384, False), (256, True)])
+def test_warp_row_strips_match_oracle(W, pinhole):
+    """Detector rows of 256 pixels (one CTA each) take the row-strip warp:
+    exactly uniform rows, a width whose CTAs alternate between one-row and
+    two-row (per-pixel) paths, and the pinhole lattice whose rows agree only
+    to float rounding.  20 blocks span two strip rounds; positions fall
+    inside, on and beyond every image edge.  Same bounds as the golden
+    warp case: 2e-6 forward, 1e-5 gradients against the float64 oracle."""
+    from fvr.cone_beam_fvr import PerspectiveSlabFVR
+    from fvr.triton_slice import pou_pinhole_warp_sum
+
+    rng = np.random.default_rng(31)
+    B, N, P, H = 20, 2, 24, 6
+    imgs = rng.standard_normal((B, N, P, P)).astype(np.float32)
+    db = rng.uniform(260.0, 320.0, (B, N)).astype(np.float32)
+    cu = rng.uniform(-10.0, 10.0, (B, N)).astype(np.float32)
+    cv = rng.uniform(-10.0, 10.0, (B, N)).astype(np.float32)
+    inv_ds, c_idx = 0.4, 12.0
+    if pinhole:
+        k_inv = torch.tensor([[1 / 2000.0, 0.0, -W / 4000.0], [0.0, 1 / 1500.0, -0.1], [0.0, 0.0, 1.0]])
+        lat = PerspectiveSlabFVR.make_pinhole_lattice(k_inv, 1000.0, H, W)
+        rx, ry, ic = (t.cpu().numpy().astype(np.float32) for t in lat[5:8])
+    else:
+        rx = np.broadcast_to(np.linspace(-0.12, 0.12, W, dtype=np.float32), (H, W)).copy()
+        ry = np.broadcast_to(np.array([-0.1, -0.06, -0.01, 0.03, 0.07, 0.11], np.float32)[:, None], (H, W)).copy()
+        ic = rng.uniform(0.95, 1.0, (H, W)).astype(np.float32)
+    t = [_t(a).requires_grad_(True) for a in (imgs, db, cu, cv)]
+    out = pou_pinhole_warp_sum(t[0], t[1], t[2], t[3], _t(rx), _t(ry), _t(ic), _t(rx).reshape(-1),
+                               _t(ry).reshape(-1), _t(ic).reshape(-1), inv_ds, c_idx)
+    wout = rng.standard_normal((N, H, W)).astype(np.float32)
+    (out * _t(wout)).sum().backward()
+    f64 = [a.astype(np.float64) for a in (imgs, db, cu, cv, rx, ry, ic)]
+    ref = opou.warp_sum(*f64, inv_ds, c_idx)
+    assert rel_l2(out.detach().cpu().numpy(), ref) < 2e-6
+    grads = opou.warp_sum_adjoint(*f64, inv_ds, c_idx, wout.astype(np.float64))
+    for x, r, k in zip(t, grads, ("imgs", "db", "cu", "cv")):
+        assert rel_l2(x.grad.cpu().numpy(), r) < 1e-5, k
+
+
 def test_invariant_matches_explicit_rays():
     from fvr.cone_beam_fvr import PerspectiveSlabFVR
 
