@@ -151,7 +151,9 @@ int fvr_tc_sncc_backward(const double* mom, int nviews, const int* views, const 
  * all ones; accumulate != 0 adds), and loss[nviews + 1] as
  * fvr_tc_sncc_finalize does.  `workspace` (>= fvr_tc_sncc_fused_workspace
  * bytes, 256-byte aligned) needs no initialisation.  Calls sharing one
- * workspace must be stream-ordered.
+ * workspace must be stream-ordered.  loss, ncc_out and grad_poses may be
+ * device memory or page-locked host memory mapped into the device address
+ * space (the epilogue kernel writes them directly).
  * Replaces the forward + autograd backward of TorchDiffFVREngine.
  * forward_spectral_ncc over several views, src/fvr/torch_engine.py:269-307. */
 int64_t fvr_tc_sncc_fused_workspace(int64_t C, int64_t R, int64_t nviews);
