@@ -40,6 +40,15 @@ def test_python_binding_covers_the_header():
     assert sorted(L.SIGNATURES) == _declared()
 
 
+def test_integration_guide_maps_every_entry_point():
+    """INTEGRATION.md's entry-point table names every declared symbol, so a
+    maintainer binding the library finds each one next to the reference
+    interface it replaces."""
+    text = (REPO / "INTEGRATION.md").read_text()
+    missing = [n for n in _declared() if f"`{n}`" not in text]
+    assert not missing, f"not mapped in INTEGRATION.md: {missing}"
+
+
 def test_status_strings_and_queries(lib):
     import fvr._lib as L
 
