@@ -274,7 +274,7 @@ def run_b200(args, torch):
     pou = _pou_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
     npl = _numpy_leg(torch, dev, max(3, min(W, 5)), max(5, min(K, 20)), rank == 0)
     reg = _registration_leg(torch, dev)
-    cfg4 = _cfg4_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
+    large = _large_volume_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
 
     # the memory system's ceiling for this gather: the same 32-byte entries in
     # the moments kernel's sweep order through a load-only kernel, L2 flushed
@@ -288,7 +288,7 @@ def run_b200(args, torch):
         alg_bytes = 2 * CANDIDATES * OUT_RES * OUT_RES * (32 + 8)
         achieved = alg_bytes / (kern_avg_ms * 1e-3) / 1e9
         traffic = None
-        tf = REPO / "profiles" / "tc_sncc_moments_cfg2_traffic.txt"
+        tf = REPO / "profiles" / "tc_sncc_moments_f16_128cube_64cand_traffic.txt"
         if tf.exists():
             for line in tf.read_text().splitlines():
                 if line.startswith("dram_bytes_per_launch:"):
@@ -375,7 +375,7 @@ def run_b200(args, torch):
             "pou_cone_beam": pou,
             "numpy_renderer": npl,
             "registration": reg,
-            "cfg4_512": cfg4,
+            "volume256_spectrum512": large,
         }
     if ws > 1:
         dist.barrier()
@@ -433,7 +433,7 @@ def _pou_leg(torch, dev, flush, warmup, steps):
     return out
 
 
-def _cfg4_leg(torch, dev, flush, warmup, steps):
+def _large_volume_leg(torch, dev, flush, warmup, steps):
     """Secondary line: the large torch-convention case.  Seeded 256^3
     ellipsoid volume (spacing 0.8 x 0.8 x 1.5 mm: voxel-unit spectrum, spacing[0]
     in the phase as the reference uses it) -> 512^3 spectrum, R = 192, 256
@@ -489,8 +489,8 @@ def _cfg4_leg(torch, dev, flush, warmup, steps):
 
 
 def _registration_leg(torch, dev, iters=200, n_cand=CANDIDATES):
-    """Secondary line: multi-start biplanar registration (one volume of
-    BASELINE config 5's kind): seeded 128^3 ellipsoid volume (1 mm), PoU-FVR
+    """Secondary line: multi-start biplanar registration on one volume:
+    seeded 128^3 ellipsoid volume (1 mm), PoU-FVR
     2x2x2 blocks at block_res 64 (P = 128, bf16 spectra), pinhole SDD 1020 /
     SAD 765 mm, 256^2 detector at 1.0 mm, AP and lateral views, references
     rendered at a seeded ground-truth pose; 64 candidates, 200 Adam
