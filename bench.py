@@ -408,6 +408,22 @@ def _f16_from_f32(eng, vol, dev, torch):
     eng.f_vol_5d = fresh.f_vol_5d
 
 
+def _pou_roofline(B, P, K, entry, pose_evals_per_s):
+    """Whole-step bytes per pose-eval as the hot-path scope table counts them
+    for the PoU step: forward = slice gather B P^2 x entry + block-image
+    IFFT B P^2 x 12 B + warp K (B x 16 B of taps + 16 B rays / out);
+    adjoint = warp 2 x B K x 16 B + IFFT B P^2 x 12 B + slice B P^2 x entry
+    (entry: 64 B f32 / 32 B bf16 stencil entry), over the whole step time."""
+    peak, peak_kind = _peak_hbm()
+    fwd = B * P * P * entry + B * P * P * 12 + K * (B * 16 + 16)
+    adj = 2 * B * K * 16 + B * P * P * 12 + B * P * P * entry
+    achieved = (fwd + adj) * pose_evals_per_s / 1e9
+    return {"bound": "hbm", "alg_bytes_per_pose_eval": fwd + adj, "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+            "fallback 6.65 TB/s", "timing": "whole step (all kernels, eager autograd)"}
+
+
 def _pou_leg(torch, dev, flush, warmup, steps):
     """Secondary line: the PoU-FVR cone-beam step (192^3 ellipsoid volume, 4x4x4
     blocks at 50 % overlap, block_res 64 -> P = 128; pinhole SDD 1020 / SAD 765
@@ -435,7 +451,9 @@ def _pou_leg(torch, dev, flush, warmup, steps):
             step()
         t, _ = _time_steps(torch, step, steps, flush)
         ms = statistics.mean(t)
-        out[name] = {"value": CANDIDATES / (ms / 1e3), "ms_per_step": ms, "blocks": int(m.B), "P": int(m.P)}
+        value = CANDIDATES / (ms / 1e3)
+        out[name] = {"value": value, "ms_per_step": ms, "blocks": int(m.B), "P": int(m.P),
+                     "roofline": _pou_roofline(int(m.B), int(m.P), 256 * 256, 64 if name == "f32" else 32, value)}
         del m, lattice
         torch.cuda.empty_cache()
     out["unit"] = UNIT
