@@ -501,7 +501,8 @@ def _large_volume_leg(torch, dev, flush, warmup, steps):
         st, _ = _time_steps(torch, step._g.replay, steps, flush)
         ms = statistics.mean(st)
         entry = {"value": C / (ms / 1e3), "ms_per_step": ms, "ms_per_step_min_median_max":
-                 [min(st), statistics.median(st), max(st)]}
+                 [min(st), statistics.median(st), max(st)],
+                 "roofline": _sncc_step_roofline(name, C, R, ms)}
         if ref is None:
             ref = res
         else:
@@ -517,6 +518,23 @@ def _large_volume_leg(torch, dev, flush, warmup, steps):
                         "R = 192, 256 candidates x 2 views, loss + 6-DOF gradient per step (CUDA-graph replay, "
                         "L2 flushed before each step)",
             "error_reference": "this run's f32 path (the f32 path is pinned to the fp64 oracle at 128^3 -> 256^3)"}
+
+
+def _sncc_step_roofline(storage, C, R, ms):
+    """Whole-step bytes as the hot-path scope table counts them for the
+    batched spectral-NCC step: per view and sample the 8-corner gather of
+    the forward pass and again of the adjoint (8 B a corner in f32, 4 B in
+    16-bit storage), the 8 B target and, for f16, a 4 B brick scale; over the
+    step's CUDA-event time."""
+    peak, peak_kind = _peak_hbm()
+    corner = 8 if storage == "f32" else 4
+    per_sample = 2 * 8 * corner + 8 + (4 if storage == "f16" else 0)
+    alg = 2 * C * R * R * per_sample
+    achieved = alg / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "alg_bytes_per_step": alg, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak,
+            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+            "fallback 6.65 TB/s", "timing": "whole step (graph replay)"}
 
 
 REG_VOLUMES = ((128, 128, 128), (192, 192, 192), (160, 256, 256))  # (Z, Y, X) voxels at 1 mm
