@@ -1,0 +1,49 @@
+"""bench.py's multi-rank plumbing on CPU: the slowest rank's time through a
+world_size-2 gloo group, and the reference arm's non-zero ranks exiting
+without work (no GPU needed)."""
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+def _rank_main(rank, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, str(REPO))
+    import bench
+
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    try:
+        got = bench._max_over_ranks(torch, dist, 2, torch.device("cpu"), 10.0 + 5.0 * rank)
+        out[rank] = got
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo():
+    port = 29500 + os.getpid() % 2000
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_rank_main, args=(port, out), nprocs=2, start_method="spawn", join=True)
+        assert dict(out) == {0: 15.0, 1: 15.0}
+
+
+def test_max_over_ranks_single_rank_is_local():
+    sys.path.insert(0, str(REPO))
+    import bench
+
+    assert bench._max_over_ranks(torch, None, 1, torch.device("cpu"), 3.5) == 3.5
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    env = dict(os.environ, WORLD_SIZE="2", RANK="1", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+                        "--warmup", "1"], cwd=REPO, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
