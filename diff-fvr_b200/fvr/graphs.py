@@ -54,10 +54,11 @@ class GraphedCallable:
     is the whole host-to-host step; the copies are kernels that read or write
     the pinned buffers directly (``fvr_copy_bytes``).  With
     ``outputs_on_host=True`` as well, ``fn`` itself returns pinned host tensors
-    that its kernels write, and no output copy is captured.  Calling then takes host tensors (or
-    writes nothing when given ``host_in`` itself), replays, and returns
-    ``host_out`` after waiting for the stream (``sync=False``: without
-    waiting; ``host_out`` is complete once the current stream is)."""
+    that its kernels write, and no output copy is captured.  Calling then
+    takes host tensors (or writes nothing when given ``host_in`` itself),
+    replays, and returns ``host_out`` after waiting for the stream
+    (``sync=False``: without waiting; ``host_out`` is complete once the
+    current stream is)."""
 
     def __init__(self, fn, *example_inputs, warmup=3, capture_context=None, host_io=False,
                  outputs_on_host=False):
