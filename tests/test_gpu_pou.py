@@ -202,12 +202,13 @@ def test_batched_equals_single_and_bf16_parity():
     assert float(m2.grad.abs().sum()) > 1e-4
 
 
-@pytest.mark.parametrize("W,pinhole", [(256, False), (384, False), (256, True)])
+@pytest.mark.parametrize("W,pinhole", [(256, False), (384, False), (512, False), (320, False), (256, True)])
 def test_warp_row_strips_match_oracle(W, pinhole):
     """Detector rows of 256 pixels (one CTA each) take the row-strip warp:
-    exactly uniform rows, a width whose CTAs alternate between one-row and
-    two-row (per-pixel) paths, and the pinhole lattice whose rows agree only
-    to float rounding.  20 blocks span two strip rounds; positions fall
+    exactly uniform rows, widths whose CTAs alternate between one-row and
+    two-row (per-pixel) paths (384), cover half a row each (512) or end in a
+    partly filled one-row CTA (320: the last CTA holds 192 pixels), and the
+    pinhole lattice whose rows agree only to float rounding.  20 blocks span two strip rounds; positions fall
     inside, on and beyond every image edge.  Same bounds as the golden
     warp case: 2e-6 forward, 1e-5 gradients against the float64 oracle."""
     from fvr.cone_beam_fvr import PerspectiveSlabFVR
