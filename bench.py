@@ -279,6 +279,7 @@ def run_b200(args, torch):
     t_eager, _ = _time_steps(torch, e2e_eager, K, flush)
 
     pou = _pou_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
+    pou8 = _pou_eight_block_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
     npl = _numpy_leg(torch, dev, max(3, min(W, 5)), max(5, min(K, 20)), rank == 0)
     reg = _registration_leg(torch, dev)
     large = _large_volume_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
@@ -393,6 +394,7 @@ def run_b200(args, torch):
             "kernels_per_step": int(f16["kernels_per_step"]),
             "clocks": f16["clocks"],
             "pou_cone_beam": pou,
+            "pou_cone_beam_8_blocks": pou8,
             "numpy_renderer": npl,
             "registration": reg,
             "volume256_spectrum512": large,
@@ -467,6 +469,51 @@ def _pou_leg(torch, dev, flush, warmup, steps):
     out["workload"] = ("PoU-FVR cone-beam: seeded 192^3 ellipsoid volume (1 mm), 4x4x4 blocks, 50% overlap, "
                        "block_res 64 (P = 128), SDD 1020 / SAD 765 mm, 256x256 detector at 0.8 mm, 64 poses, "
                        "forward + pose gradient (eager autograd through forward_pinhole)")
+    out["l2"] = "flushed before every timed step (256 MiB write)"
+    return out
+
+
+def _pou_eight_block_leg(torch, dev, flush, warmup, steps):
+    """Secondary line in the block configuration the reference publishes its
+    PoU-FVR GPU timings for (2x2x2 blocks at block_res 64 -> P = 128, SDD
+    1020 mm, 256^2 detector at 1.0 mm, 64 poses): forward only and forward +
+    pose gradient, eager, on the seeded 192^3 ellipsoid volume (the
+    reference's own numbers are on a CT volume and another GPU)."""
+    from fvr import synthetic
+    from fvr.cone_beam_fvr import PerspectiveSlabFVR
+
+    out = {}
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+        vol = synthetic.make_ellipsoid_volume(192, SEED)
+        m = PerspectiveSlabFVR.from_volume(vol, vox_mm=1.0, grid_blocks=(2, 2, 2), block_res=64, overlap=0.5,
+                                           dtype=dt, device=dev)
+        f = 1020.0 / 1.0
+        k_inv = torch.tensor([[1.0 / f, 0.0, -128.0 / f], [0.0, 1.0 / f, -128.0 / f], [0.0, 0.0, 1.0]], device=dev)
+        lattice = m.make_pinhole_lattice(k_inv, 1020.0, 256, 256)
+        mats = synthetic.make_pinhole_mats(CANDIDATES, SEED + 1, sad_mm=765.0, device=dev)
+
+        def fwd():
+            with torch.no_grad():
+                return m.forward_pinhole(mats, lattice)
+
+        def fwd_bwd():
+            mm = mats.detach().requires_grad_(True)
+            m.forward_pinhole(mm, lattice).sum().backward()
+            return mm.grad
+
+        res = {"blocks": int(m.B), "P": int(m.P)}
+        for key, fn in (("forward", fwd), ("forward_backward", fwd_bwd)):
+            for _ in range(warmup):
+                fn()
+            t, _ = _time_steps(torch, fn, steps, flush)
+            ms = statistics.mean(t)
+            res[key] = {"ms_per_step": ms, "pose_evals_per_s": CANDIDATES / (ms / 1e3)}
+        out[name] = res
+        del m, lattice
+        torch.cuda.empty_cache()
+    out["workload"] = ("PoU-FVR cone-beam: seeded 192^3 ellipsoid volume (1 mm), 2x2x2 blocks, 50% overlap, "
+                       "block_res 64 (P = 128), SDD 1020 / SAD 765 mm, 256x256 detector at 1.0 mm, 64 poses; "
+                       "forward (no grad) and forward + pose gradient, eager")
     out["l2"] = "flushed before every timed step (256 MiB write)"
     return out
 
