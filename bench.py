@@ -280,6 +280,7 @@ def run_b200(args, torch):
 
     pou = _pou_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
     pou8 = _pou_eight_block_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
+    fwd_only = _sncc_forward_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
     npl = _numpy_leg(torch, dev, max(3, min(W, 5)), max(5, min(K, 20)), rank == 0)
     reg = _registration_leg(torch, dev)
     large = _large_volume_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
@@ -395,6 +396,7 @@ def run_b200(args, torch):
             "clocks": f16["clocks"],
             "pou_cone_beam": pou,
             "pou_cone_beam_8_blocks": pou8,
+            "spectral_ncc_forward_one_view": fwd_only,
             "numpy_renderer": npl,
             "registration": reg,
             "volume256_spectrum512": large,
@@ -470,6 +472,50 @@ def _pou_leg(torch, dev, flush, warmup, steps):
                        "block_res 64 (P = 128), SDD 1020 / SAD 765 mm, 256x256 detector at 0.8 mm, 64 poses, "
                        "forward + pose gradient (eager autograd through forward_pinhole)")
     out["l2"] = "flushed before every timed step (256 MiB write)"
+    return out
+
+
+def _sncc_forward_leg(torch, dev, flush, warmup, steps):
+    """Secondary line in the configuration the reference publishes its
+    TorchDiffFVREngine zero-IFFT spectral-NCC GPU timings for: 128^3 volume,
+    pad 2 (256^3 spectrum), 16-bit spectrum, one view, 64 candidates,
+    out_res 128 / 256 / 512, forward only through forward_spectral_ncc
+    (eager, no grad), on the seeded ellipsoid volume."""
+    import fvr
+    from fvr import synthetic
+
+    vol = synthetic.make_ellipsoid_volume(VOL_N, SEED)
+    poses = torch.from_numpy(synthetic.make_poses(CANDIDATES, SEED + 1)).to(dev)
+    tp = torch.from_numpy(synthetic.make_poses(1, SEED + 2)).to(dev)
+    eng = fvr.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0, device=dev)
+    targets = {}
+    with torch.no_grad():
+        for R in (128, 256, 512):
+            targets[R] = eng.prepare_spectral_target(eng(tp, view="ap", out_res=R))
+    out = {}
+    for name, dt in (("bf16", torch.bfloat16), ("f16", torch.float16)):
+        if name == "bf16":
+            eng.to_precision(dt)
+        else:
+            eng = fvr.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0, device=dev)
+            eng.to_precision(dt)
+        res = {}
+        for R, ft in targets.items():
+            def fn():
+                with torch.no_grad():
+                    return eng.forward_spectral_ncc(poses, ft, view="ap")
+
+            for _ in range(warmup):
+                fn()
+            t, _ = _time_steps(torch, fn, steps, flush)
+            ms = statistics.mean(t)
+            res[str(R)] = {"ms_per_call": ms, "poses_per_s": CANDIDATES / (ms / 1e3)}
+        out[name] = res
+    del eng
+    torch.cuda.empty_cache()
+    out["workload"] = ("TorchDiffFVREngine.forward_spectral_ncc, one view (AP), 64 candidates, seeded 128^3 "
+                       "ellipsoid volume -> 256^3 spectrum, out_res 128 / 256 / 512, forward only, eager")
+    out["l2"] = "flushed before every timed call (256 MiB write)"
     return out
 
 
