@@ -664,18 +664,25 @@ __device__ float warp_rows_forward(const WarpArgs<OT>& a, int n, bool live, doub
 //   sum g dpx rx = sum_x rb[x] (Gr[x - 1] - Gr[x]) / ds,  sum g dpx = sum_x rb[x] (Gs[x - 1] - Gs[x]) / ds,
 //   sum g dpy = sum_x dr[x] S[x] / ds,
 // and dL/dimg[iy][x] += (1 - ty) S[x], dL/dimg[iy + 1][x] += ty S[x].
+// S, Gs and Gr are accumulated as 32-bit fixed point with one power-of-two
+// scale per CTA (2^22 / the largest |g| or |g rx| of its pixels, so an
+// entry's at most 256 contributions cannot overflow): integer shared-memory
+// atomics are several times faster than float ones, and each contribution is
+// rounded once, to 2^-22 of that largest weight.
 template <typename OT>
-__device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, double rx, float g, const WarpCull& wc,
-                                  const short* tl, float* strip, float* __restrict__ grad_imgs, double* sacc) {
+__device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, double rx, float g, int scale_exp,
+                                  const WarpCull& wc, const short* tl, float* strip, float* __restrict__ grad_imgs,
+                                  double* sacc) {
   __shared__ WarpRow s_row[kWarpStripMax];
   const int P = a.P, W2 = P + 2;
   const int plane = a.chunk * W2;
   float* rb = strip;
   float* dr = strip + plane;
-  float* S = strip + 2 * plane;
-  float* Gs = strip + 3 * plane;
-  float* Gr = strip + 4 * plane;
+  int* S = reinterpret_cast<int*>(strip + 2 * plane);
+  int* Gs = reinterpret_cast<int*>(strip + 3 * plane);
+  int* Gr = reinterpret_cast<int*>(strip + 4 * plane);
   const float rxf = static_cast<float>(rx), ryf = static_cast<float>(wc.ry0);
+  const float fix = ldexpf(1.f, scale_exp), unfix = ldexpf(1.f, -scale_exp);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int c0 = 0; c0 < wc.nt; c0 += a.chunk) {
     const int cn = min(a.chunk, wc.nt - c0);
@@ -688,9 +695,9 @@ __device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, doubl
       const int e = k * W2 + xr;
       rb[e] = r0 * (1.f - s_row[k].ty) + r1 * s_row[k].ty;
       dr[e] = r1 - r0;
-      S[e] = 0.f;
-      Gs[e] = 0.f;
-      Gr[e] = 0.f;
+      S[e] = 0;
+      Gs[e] = 0;
+      Gr[e] = 0;
       for (xr += blockDim.x; xr >= W2; xr -= W2) ++k;
     }
     __syncthreads();
@@ -701,10 +708,10 @@ __device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, doubl
           const double fx = floor(px);
           const float tx = static_cast<float>(px - fx);
           const int o = k * W2 + static_cast<int>(fx) + 1;
-          atomicAdd(S + o, g * (1.f - tx));
-          atomicAdd(S + o + 1, g * tx);
-          atomicAdd(Gs + o, g);
-          atomicAdd(Gr + o, g * rxf);
+          atomicAdd(S + o, __float2int_rn(g * (1.f - tx) * fix));
+          atomicAdd(S + o + 1, __float2int_rn(g * tx * fix));
+          atomicAdd(Gs + o, __float2int_rn(g * fix));
+          atomicAdd(Gr + o, __float2int_rn(g * rxf * fix));
         }
       }
     }
@@ -718,9 +725,9 @@ __device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, doubl
       for (int x = lane; x < P; x += 32) {
         const int o = k * W2 + x + 1;
         const double r = static_cast<double>(rb[o]);
-        sa += r * (static_cast<double>(Gr[o - 1]) - static_cast<double>(Gr[o]));
-        sb += r * (static_cast<double>(Gs[o - 1]) - static_cast<double>(Gs[o]));
-        const float sv = S[o];
+        sa += r * (static_cast<double>(Gr[o - 1] - Gr[o]) * unfix);
+        sb += r * (static_cast<double>(Gs[o - 1] - Gs[o]) * unfix);
+        const float sv = static_cast<float>(S[o]) * unfix;
         sc += static_cast<double>(dr[o]) * static_cast<double>(sv);
         if (gi && sv != 0.f) {
           if (iy >= 0 && iy < P) atomicAdd(gi + static_cast<int64_t>(iy) * P + x, sv * (1.f - ty));
@@ -800,8 +807,20 @@ __global__ void __launch_bounds__(256) pou_warp_bwd_kernel(WarpArgs<OT> a, const
   const double rx = live ? __ldg(a.rx + rq) : 0.0, ry = live ? __ldg(a.ry + rq) : 0.0;
   const WarpCull wc = warp_cull(a, n, live, rx, ry, touch, tl);
   const float g = live ? __ldg(gout + static_cast<int64_t>(n) * a.K + q) * __ldg(a.ic + rq) : 0.f;
-  if (wc.rows && !gray) {
-    warp_rows_adjoint(a, n, live, rx, g, wc, tl, strip, grad_imgs, sacc);
+  // the row-strip path's fixed-point scale: the CTA's largest weight (float
+  // bits of non-negative values order as integers; NaN and inf sort above)
+  __shared__ unsigned s_wmax;
+  if (threadIdx.x == 0) s_wmax = 0u;
+  __syncthreads();
+  const unsigned wbits = __reduce_max_sync(
+      0xffffffffu, __float_as_uint(live ? fmaxf(fabsf(g), fabsf(g * static_cast<float>(rx))) : 0.f));
+  if ((threadIdx.x & 31) == 0) atomicMax(&s_wmax, wbits);
+  __syncthreads();
+  const bool finite = s_wmax < 0x7f800000u;
+  const int wexp = static_cast<int>((s_wmax >> 23) & 0xffu) - 126;  // largest weight < 2^wexp (normal values)
+  const int scale_exp = max(-126, min(126, 22 - wexp));
+  if (wc.rows && !gray && finite) {
+    warp_rows_adjoint(a, n, live, rx, g, scale_exp, wc, tl, strip, grad_imgs, sacc);
   } else {
     const int P = a.P;
     const float inv_ds = static_cast<float>(a.inv_ds);
