@@ -586,10 +586,11 @@ __device__ __forceinline__ WarpCull warp_cull(const WarpArgs<OT>& a, int n, bool
   return wc;
 }
 
-// Per block of a row-strip round: d_b and cu (for the per-pixel x), the
+// Per block of a row-strip round: the affine map from a pixel's rx to its
+// image column, (d_b / ds) rx + (c - cu / ds) (one fp64 FMA per pixel), the
 // image row iy (-2: the row misses the image) and fraction ty.
 struct WarpRow {
-  double db, cu;
+  double sx, ox;  // the pixel's image column is sx * rx + ox
   int iy;
   float ty;
 };
@@ -597,10 +598,12 @@ struct WarpRow {
 template <typename OT>
 __device__ __forceinline__ WarpRow warp_row(const WarpArgs<OT>& a, int64_t bn, double ry0) {
   WarpRow r;
-  r.db = static_cast<double>(a.db[bn * a.ostride]);
-  r.cu = static_cast<double>(a.cu[bn * a.ostride]);
+  const double db = static_cast<double>(a.db[bn * a.ostride]);
+  const double cu = static_cast<double>(a.cu[bn * a.ostride]);
   const double cv = static_cast<double>(a.cv[bn * a.ostride]);
-  const double py = (r.db * ry0 - cv) * a.inv_ds + a.c_idx;
+  r.sx = db * a.inv_ds;
+  r.ox = a.c_idx - cu * a.inv_ds;
+  const double py = (db * ry0 - cv) * a.inv_ds + a.c_idx;
   r.iy = -2;
   r.ty = 0.f;
   if (py > -1.0 && py < static_cast<double>(a.P)) {
@@ -642,7 +645,7 @@ __device__ float warp_rows_forward(const WarpArgs<OT>& a, int n, bool live, doub
     __syncthreads();
     if (live) {
       for (int k = 0; k < cn; ++k) {
-        const double px = (s_row[k].db * rx - s_row[k].cu) * a.inv_ds + a.c_idx;
+        const double px = fma(s_row[k].sx, rx, s_row[k].ox);
         if (px > -1.0 && px < static_cast<double>(P)) {
           const double fx = floor(px);
           const float tx = static_cast<float>(px - fx);
@@ -703,7 +706,7 @@ __device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, doubl
     __syncthreads();
     if (live) {
       for (int k = 0; k < cn; ++k) {
-        const double px = (s_row[k].db * rx - s_row[k].cu) * a.inv_ds + a.c_idx;
+        const double px = fma(s_row[k].sx, rx, s_row[k].ox);
         if (px > -1.0 && px < static_cast<double>(P)) {
           const double fx = floor(px);
           const float tx = static_cast<float>(px - fx);
