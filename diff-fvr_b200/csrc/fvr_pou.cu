@@ -614,6 +614,15 @@ __device__ __forceinline__ WarpRow warp_row(const WarpArgs<OT>& a, int64_t bn, d
   return r;
 }
 
+// Image rows iy and iy + 1 of a block image at columns 4 xq .. 4 xq + 3 (P a
+// multiple of 4, so each row starts on a 16-byte boundary); zero outside.
+__device__ __forceinline__ void warp_row_quads(const float* img, int P, int iy, int xq, float4& r0, float4& r1) {
+  const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+  r0 = iy >= 0 && iy < P ? __ldg(reinterpret_cast<const float4*>(img + static_cast<int64_t>(iy) * P) + xq) : z;
+  r1 = iy + 1 >= 0 && iy + 1 < P ? __ldg(reinterpret_cast<const float4*>(img + static_cast<int64_t>(iy + 1) * P) + xq)
+                                 : z;
+}
+
 // Image rows iy and iy + 1 of block image bn at column x (zero outside).
 __device__ __forceinline__ void warp_row_pair(const float* img, int P, int iy, int x, float& r0, float& r1) {
   const bool xin = x >= 0 && x < P;
@@ -636,11 +645,28 @@ __device__ float warp_rows_forward(const WarpArgs<OT>& a, int n, bool live, doub
     if (threadIdx.x < cn) s_row[threadIdx.x] = warp_row(a, static_cast<int64_t>(tl[c0 + threadIdx.x]) * a.N + n, wc.ry0);
     __syncthreads();
     // element e = k * W2 + xr of the strips, walked without a division per element
-    for (int k = threadIdx.x / W2, xr = threadIdx.x % W2; k < cn;) {
-      float r0, r1;
-      warp_row_pair(a.imgs + (static_cast<int64_t>(tl[c0 + k]) * a.N + n) * P * P, P, s_row[k].iy, xr - 1, r0, r1);
-      strip[k * W2 + xr] = r0 * (1.f - s_row[k].ty) + r1 * s_row[k].ty;
-      for (xr += blockDim.x; xr >= W2; xr -= W2) ++k;
+    if ((P & 3) == 0) {  // four columns per thread, 16-byte loads
+      const int Q = P >> 2;
+      for (int k = threadIdx.x / Q, xq = threadIdx.x % Q; k < cn;) {
+        float4 r0, r1;
+        warp_row_quads(a.imgs + (static_cast<int64_t>(tl[c0 + k]) * a.N + n) * P * P, P, s_row[k].iy, xq, r0, r1);
+        const float ty = s_row[k].ty, uy = 1.f - ty;
+        float* d = strip + k * W2 + 1 + 4 * xq;
+        d[0] = r0.x * uy + r1.x * ty;
+        d[1] = r0.y * uy + r1.y * ty;
+        d[2] = r0.z * uy + r1.z * ty;
+        d[3] = r0.w * uy + r1.w * ty;
+        for (xq += blockDim.x; xq >= Q; xq -= Q) ++k;
+      }
+      for (int k = threadIdx.x; k < cn; k += blockDim.x) strip[k * W2] = strip[k * W2 + P + 1] = 0.f;
+    } else {
+      for (int k = threadIdx.x / W2, xr = threadIdx.x % W2; k < cn;) {
+        float r0, r1;
+        warp_row_pair(a.imgs + (static_cast<int64_t>(tl[c0 + k]) * a.N + n) * P * P, P, s_row[k].iy, xr - 1, r0,
+                      r1);
+        strip[k * W2 + xr] = r0 * (1.f - s_row[k].ty) + r1 * s_row[k].ty;
+        for (xr += blockDim.x; xr >= W2; xr -= W2) ++k;
+      }
     }
     __syncthreads();
     if (live) {
@@ -692,16 +718,41 @@ __device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, doubl
     __syncthreads();  // the previous round's strips are no longer read
     if (threadIdx.x < cn) s_row[threadIdx.x] = warp_row(a, static_cast<int64_t>(tl[c0 + threadIdx.x]) * a.N + n, wc.ry0);
     __syncthreads();
-    for (int k = threadIdx.x / W2, xr = threadIdx.x % W2; k < cn;) {
-      float r0, r1;
-      warp_row_pair(a.imgs + (static_cast<int64_t>(tl[c0 + k]) * a.N + n) * P * P, P, s_row[k].iy, xr - 1, r0, r1);
-      const int e = k * W2 + xr;
-      rb[e] = r0 * (1.f - s_row[k].ty) + r1 * s_row[k].ty;
-      dr[e] = r1 - r0;
-      S[e] = 0;
-      Gs[e] = 0;
-      Gr[e] = 0;
-      for (xr += blockDim.x; xr >= W2; xr -= W2) ++k;
+    if ((P & 3) == 0) {  // four columns per thread, 16-byte loads
+      const int Q = P >> 2;
+      for (int k = threadIdx.x / Q, xq = threadIdx.x % Q; k < cn;) {
+        float4 r0, r1;
+        warp_row_quads(a.imgs + (static_cast<int64_t>(tl[c0 + k]) * a.N + n) * P * P, P, s_row[k].iy, xq, r0, r1);
+        const float ty = s_row[k].ty, uy = 1.f - ty;
+        const int e = k * W2 + 1 + 4 * xq;
+        rb[e] = r0.x * uy + r1.x * ty;
+        rb[e + 1] = r0.y * uy + r1.y * ty;
+        rb[e + 2] = r0.z * uy + r1.z * ty;
+        rb[e + 3] = r0.w * uy + r1.w * ty;
+        dr[e] = r1.x - r0.x;
+        dr[e + 1] = r1.y - r0.y;
+        dr[e + 2] = r1.z - r0.z;
+        dr[e + 3] = r1.w - r0.w;
+        for (xq += blockDim.x; xq >= Q; xq -= Q) ++k;
+      }
+      for (int k = threadIdx.x; k < cn; k += blockDim.x) {
+        rb[k * W2] = rb[k * W2 + P + 1] = 0.f;
+        dr[k * W2] = dr[k * W2 + P + 1] = 0.f;
+      }
+      for (int e = threadIdx.x; e < cn * W2; e += blockDim.x) S[e] = Gs[e] = Gr[e] = 0;
+    } else {
+      for (int k = threadIdx.x / W2, xr = threadIdx.x % W2; k < cn;) {
+        float r0, r1;
+        warp_row_pair(a.imgs + (static_cast<int64_t>(tl[c0 + k]) * a.N + n) * P * P, P, s_row[k].iy, xr - 1, r0,
+                      r1);
+        const int e = k * W2 + xr;
+        rb[e] = r0 * (1.f - s_row[k].ty) + r1 * s_row[k].ty;
+        dr[e] = r1 - r0;
+        S[e] = 0;
+        Gs[e] = 0;
+        Gr[e] = 0;
+        for (xr += blockDim.x; xr >= W2; xr -= W2) ++k;
+      }
     }
     __syncthreads();
     if (live) {
