@@ -285,17 +285,12 @@ def run_b200(args, torch):
     reg = _registration_leg(torch, dev)
     large = _large_volume_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
 
-    # the memory system's ceiling for this gather: the same 32-byte entries in
-    # the moments kernel's sweep order through a load-only kernel, L2 flushed
-    cells = profiling.sncc_cell_sequence(eng, poses, ("ap", "lateral"), OUT_RES)
-    gather_ms = profiling.gather_ceiling_ms(eng, cells, flush=flush, reps=7)
-
     res = None
     if rank == 0:
         peak, peak_kind = _peak_hbm()
         kern_avg_ms = statistics.mean(f16["kern_ms"])
-        # algorithmic bytes per pose-eval as the hot-path scope table counts
-        # them for 16-bit storage with brick scales: per view and sample the
+        # algorithmic bytes per pose-eval, counted for 16-bit storage with
+        # brick scales as the logical work of the path: per view and sample the
         # 8-corner gather of the forward pass and again of the adjoint (4 B a
         # corner), the 8 B target and a 4 B brick scale.  The kernel fuses the
         # adjoint into the forward pass and reads each 32 B entry once, so it
@@ -370,15 +365,6 @@ def run_b200(args, torch):
                 "min_bytes_note": "what the fused kernel must read: one 32 B stencil entry + 8 B target per sample",
                 "kernel_ms": kern_avg_ms,
                 "kernel_launches_timed": len(f16["kern_ms"]),
-                "gather_ceiling": {
-                    "ms": gather_ms,
-                    "entries": int(cells.numel()),
-                    "achieved_gbs_of_entries": int(cells.numel()) * 32 / (gather_ms * 1e-3) / 1e9,
-                    "kernel_frac": gather_ms / kern_avg_ms,
-                    "note": "fvr_bench_gather32 over the same 32-byte stencil entries in the moments kernel's "
-                            "sweep order, no arithmetic, L2 flushed (python -m fvr.kernel_bench gather); "
-                            "kernel_frac = ceiling time / kernel time",
-                },
             },
             "cpu_baseline": cpu["baseline"],
             "e2e": {"value": CANDIDATES * ws / (e2e_ms / 1e3), "unit": UNIT,
@@ -420,8 +406,7 @@ def _f16_from_f32(eng, vol, dev, torch):
 
 
 def _pou_roofline(B, P, K, entry, pose_evals_per_s):
-    """Whole-step bytes per pose-eval as the hot-path scope table counts them
-    for the PoU step: forward = slice gather B P^2 x entry + block-image
+    """Whole-step logical bytes per pose-eval of the PoU step: forward = slice gather B P^2 x entry + block-image
     IFFT B P^2 x 12 B + warp K (B x 16 B of taps + 16 B rays / out);
     adjoint = warp 2 x B K x 16 B + IFFT B P^2 x 12 B + slice B P^2 x entry
     (entry: 64 B f32 / 32 B bf16 stencil entry), over the whole step time."""
@@ -621,8 +606,7 @@ def _large_volume_leg(torch, dev, flush, warmup, steps):
 
 
 def _sncc_step_roofline(storage, C, R, ms):
-    """Whole-step bytes as the hot-path scope table counts them for the
-    batched spectral-NCC step: per view and sample the 8-corner gather of
+    """Whole-step logical bytes of the batched spectral-NCC step: per view and sample the 8-corner gather of
     the forward pass and again of the adjoint (8 B a corner in f32, 4 B in
     16-bit storage), the 8 B target and, for f16, a 4 B brick scale; over the
     step's CUDA-event time."""
@@ -853,14 +837,95 @@ def run_reference(args):
     }
 
 
+PRECISION_NAMES = ("f32", "bf16", "f16")
+
+
+def run_profile_case(args, torch):
+    """One small hot-path case for a profiler: builds the workload, lets the
+    autotuner settle, then runs ``--steps`` steps inside an NVTX range named
+    ``fvr_profile`` and prints the mean step time (CUDA events).
+
+    ``sncc``: the batched spectral-NCC graph step (``--volume``^3 ellipsoid
+    volume, ``--candidates`` poses x AP + lateral, ``--out-res``^2) in the
+    ``--precision`` storage.  ``pou``: the PoU-FVR forward + pose gradient
+    (``--volume``^3, ``--grid``^3 blocks at ``--block-res``, 50 % overlap,
+    SDD 1020 / SAD 765 mm, ``--det``^2 at 0.8 mm, ``--candidates`` poses)."""
+    from fvr import synthetic
+
+    dt = {"f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}[args.precision]
+    dev = torch.device("cuda", 0)
+    vol = synthetic.make_ellipsoid_volume(args.volume, SEED)
+    if args.profile_case == "sncc":
+        from fvr.graphs import BiplanarSpectralNCCStep
+        from fvr.torch_engine import TorchDiffFVREngine
+
+        poses = torch.from_numpy(synthetic.make_poses(args.candidates, SEED + 1)).to(dev)
+        tp = torch.from_numpy(synthetic.make_poses(1, SEED + 2)).to(dev)
+        eng = TorchDiffFVREngine(torch.from_numpy(vol), device=dev)
+        with torch.no_grad():
+            fa = eng.prepare_spectral_target(eng(tp, view="ap", out_res=args.out_res))
+            fl = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=args.out_res))
+        eng.to_precision(dt)
+        st = BiplanarSpectralNCCStep(eng, fa, fl, args.candidates, graph=False)
+
+        def step():
+            st(poses)
+    else:
+        from fvr.cone_beam_fvr import PerspectiveSlabFVR
+
+        g = args.grid
+        m = PerspectiveSlabFVR.from_volume(vol, vox_mm=1.0, grid_blocks=(g, g, g), block_res=args.block_res,
+                                           overlap=0.5, dtype=dt, device=dev)
+        H = args.det
+        f = 1020.0 / 0.8
+        k_inv = torch.tensor([[1.0 / f, 0.0, -0.5 * H / f], [0.0, 1.0 / f, -0.5 * H / f], [0.0, 0.0, 1.0]],
+                             device=dev)
+        lattice = m.make_pinhole_lattice(k_inv, 1020.0, H, H)
+        mats = synthetic.make_pinhole_mats(args.candidates, SEED + 1, sad_mm=765.0, device=dev)
+
+        def step():
+            mm = mats.detach().requires_grad_(True)
+            m.forward_pinhole(mm, lattice).sum().backward()
+
+    # backward on this thread, so the NVTX range also covers the adjoint kernels
+    torch.autograd.set_multithreading_enabled(False)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("fvr_profile")
+    a.record()
+    for _ in range(args.steps):
+        step()
+    b.record()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    return {"profile_case": args.profile_case, "precision": args.precision,
+            "ms_per_step": a.elapsed_time(b) / args.steps}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--profile-case", choices=["sncc", "pou"], default=None,
+                    help="run one small case for a profiler instead of the benchmark")
+    ap.add_argument("--precision", choices=PRECISION_NAMES, default="f16")
+    ap.add_argument("--volume", type=int, default=128)
+    ap.add_argument("--candidates", type=int, default=64)
+    ap.add_argument("--out-res", type=int, default=128)
+    ap.add_argument("--grid", type=int, default=4)
+    ap.add_argument("--block-res", type=int, default=64)
+    ap.add_argument("--det", type=int, default=256)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.profile_case is not None:
+        import torch
+
+        print(json.dumps(run_profile_case(args, torch)), flush=True)
+        return
     if args.impl == "reference":
         res = run_reference(args)
     else:

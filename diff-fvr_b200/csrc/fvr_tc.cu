@@ -905,7 +905,19 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
 //
 // Set-up: the first call on each device, made with that device current,
 // resolves the array's device address with cudaGetSymbolAddress and caches
-// it; make that first call before any stream capture begins.
+// it; make that first call before any stream capture begins.  The cached
+// address belongs to the device's primary context of that moment: a process
+// that calls cudaDeviceReset (or otherwise destroys that context) while the
+// library is loaded must not call this entry point on that device again,
+// since the module is loaded anew into the next context and the cached
+// address no longer names the array.
+//
+// Record bound: sncc_plan gives each (candidate, view) item
+// max(1, floor(min_blocks * SMs / items)) tiles, so one call needs at most
+// max(items, min_blocks * SMs) partial records; with items <= 512 and the
+// largest min_blocks of the variant table on a 148-SM B200 that stays within
+// kStaticRecords (static_assert below; the run-time check refuses anything
+// else before launching).
 //
 // Races: one array per device is shared by every caller in the process.
 // Calls on the same device must be ordered (one stream, or explicit
@@ -920,6 +932,14 @@ constexpr int64_t kStaticDoubles = kStaticPartialDoubles + kStaticMomDoubles;
 constexpr int kStaticMaxDevices = 64;
 
 static __device__ __align__(256) double g_sncc_static_scratch[kStaticDoubles];
+
+constexpr int max_min_blocks() {
+  int m = 0;
+  for (const SnccVariant& v : kSnccVariantTable) m = v.min_blocks > m ? v.min_blocks : m;
+  return m;
+}
+static_assert(kStaticItems <= kStaticRecords && max_min_blocks() * 148 <= kStaticRecords,
+              "static scratch holds the partial records of every launch variant on a 148-SM device");
 
 static std::mutex g_static_mu;
 static double* g_static_ptr[kStaticMaxDevices] = {};

@@ -61,7 +61,6 @@ SIGNATURES = {
                                          I64, P, P, P, I32, P]),
     "fvr_event_record": (I32, [P, P, I32]),
     "fvr_copy_bytes": (I32, [P, P, I64, P]),
-    "fvr_bench_gather32": (I32, [P, I64, P, I64, P, I64, I32, P]),
     "fvr_tc_sncc_backward": (I32, [P, I32, P, P, I64, P, I64, I64, I64, I64, F64, P, I32, P]),
     "fvr_tc_slice": (I32, [I32, P, P, I64, I64, I64, P, I64, P, I64, F64, I32, P, P]),
     "fvr_tc_slice_adjoint_workspace": (I64, [I64, I64]),

@@ -169,12 +169,14 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
  * allocates nothing.  For callers that cannot allocate device memory where
  * they call (a host linking only this C ABI, with no device allocator; a
  * loop that must not enter an allocator between steps).
- * Limits: C * nviews <= 512 and at most 2048 partial records (tile grid:
- * C * nviews * tiles; one range per CTA: CTAs + C * nviews - 1, as the launch
- * variant sizes them); larger calls return FVR_ERR_WORKSPACE without
- * launching.
+ * Limits: C * nviews <= 512 and at most 2048 partial records (partial
+ * records = C * nviews * tiles, tiles chosen by the launch variant; on a
+ * 148-SM B200 every variant stays within the limit when C * nviews <= 512);
+ * larger calls return FVR_ERR_WORKSPACE without launching.
  * The first call on a device (that device current) resolves the scratch
- * address once; make it before any stream capture begins.  Nothing has to be
+ * address once; make it before any stream capture begins.  The cached address
+ * is tied to that device's context: after cudaDeviceReset on a device, do not
+ * call this entry point on it again in the same process.  Nothing has to be
  * zeroed by the caller: every call writes the scratch before reading it.
  * All callers in the process share one
  * scratch per device, so calls on one device must not overlap in time (use
@@ -359,13 +361,6 @@ int fvr_event_record(void* event, void* stream, int external);
  * so a captured step can move its small inputs and outputs between host and
  * device in kernel nodes instead of copy-engine memcpy nodes. */
 int fvr_copy_bytes(void* dst, const void* src, int64_t n, void* stream);
-/* Gather ceiling of a cell sequence (no reference counterpart; measurement
- * utility): reads the 32-byte entries entries[idx[i]], i < n (an index
- * outside [0, n_entries) reads nothing), three 256-bit loads in flight
- * per thread on `blocks` CTAs of 256 threads, and writes one folded word per
- * thread to out[blocks * 256] (out_len elements available). */
-int fvr_bench_gather32(const void* entries, int64_t n_entries, const int* idx, int64_t n, unsigned* out,
-                       int64_t out_len, int blocks, void* stream);
 
 /* ------------------------------------------- image-domain spectral NCC -- */
 /* Between centred spectra Fp[B][n] and Ft[Bt][n] (Bt = 1 or B, complex), both

@@ -2,7 +2,7 @@
 
 Usage (needs the reference checkout; run from the repository root):
 
-    python tests/golden/make_golden.py /root/reference [name,name,...]
+    python tests/golden/make_golden.py <reference checkout> [name,name,...]
 
 (names: slice_warp, torch_engine, pou, numpy_renderer, articulated,
 ingest_targets; all of them when none is given)
@@ -325,7 +325,9 @@ def gen_ingest_and_targets(ref_root: Path):
 
 
 def main():
-    ref_root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference checkout> [name,name,...]")
+    ref_root = Path(sys.argv[1])
     only = set(sys.argv[2].split(",")) if len(sys.argv) > 2 else None
     import torch
 

@@ -1,4 +1,4 @@
-"""GPU parity of the §8(f) rows around the NumPy-convention path:
+"""GPU parity of the callers and data formats around the NumPy-convention path:
 articulated multi-segment spectra (``ArticulatedSpineModel``,
 src/fvr/articulated_spine.py), volume ingest (``resample_isotropic_cube`` /
 ``hu_to_attenuation``, src/fvr/dicom_loader.py) and the target-spectrum

@@ -43,11 +43,13 @@ def _outputs(C, dev):
     return loss, grad
 
 
-@pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
-def test_static_scratch_matches_workspace_entry(dtype):
+@pytest.mark.parametrize("C", [24, 256])
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.bfloat16])
+def test_static_scratch_matches_workspace_entry(dtype, C):
+    """C = 256 with two views is the scratch's limit (512 items: every item
+    record row and four 128-item chunks of the epilogue are used)."""
     from fvr import _lib as L
 
-    C = 24
     eng, fts, poses, head, dev = _problem(C, dtype=dtype)
     lib = L.load()
     s = L.stream_ptr(dev)
