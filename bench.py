@@ -284,6 +284,13 @@ def run_b200(args, torch):
     npl = _numpy_leg(torch, dev, max(3, min(W, 5)), max(5, min(K, 20)), rank == 0)
     reg = _registration_leg(torch, dev)
     large = _large_volume_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)))
+    mine = {"screening": {"graph_f16": value / ws, "eager_api_f16": CANDIDATES / (statistics.mean(t_eager) / 1e3)},
+            "forward_one_view": {R: v["ms_per_call"] for R, v in fwd_only["bf16"].items()},
+            "pou": {"grid4_P128_det0.8mm": {k: pou[k]["ms_per_step"] for k in ("f32", "bf16")},
+                    "grid2_P128_det1.0mm": {k: pou8[k]["forward_backward"]["ms_per_step"] for k in ("f32", "bf16")}}}
+    # the reference's own GPU path, single-GPU runs only (its set-up takes longer than the
+    # process group's timeout would allow the other ranks to wait)
+    ref_gpu = _reference_gpu_leg(torch, dev, flush, max(3, min(W, 5)), max(5, min(K, 20)), mine) if ws == 1 else None
 
     res = None
     if rank == 0:
@@ -386,6 +393,7 @@ def run_b200(args, torch):
             "numpy_renderer": npl,
             "registration": reg,
             "volume256_spectrum512": large,
+            "reference_gpu": ref_gpu,
         }
     if ws > 1:
         dist.barrier()
@@ -621,6 +629,127 @@ def _sncc_step_roofline(storage, C, R, ms):
             "fallback 6.65 TB/s", "timing": "whole step (graph replay)"}
 
 
+def _reference_modules():
+    """The unmodified reference package installed in baseline/_ref, imported
+    under the package name ``fvr_reference`` (its modules import one another
+    relatively; this package already owns the name ``fvr``).  Only the two
+    modules on the rendering path are imported, so its DICOM reader's
+    third-party dependencies are not needed.  None when it is not installed."""
+    import importlib
+    import types
+
+    root = REPO / "baseline" / "_ref" / "fvr"
+    if not (root / "torch_engine.py").exists():
+        return None
+    if "fvr_reference" not in sys.modules:
+        pkg = types.ModuleType("fvr_reference")
+        pkg.__path__ = [str(root)]
+        sys.modules["fvr_reference"] = pkg
+    return (importlib.import_module("fvr_reference.torch_engine"),
+            importlib.import_module("fvr_reference.cone_beam_fvr"))
+
+
+def _reference_gpu_leg(torch, dev, flush, warmup, steps, mine):
+    """The reference's own GPU path (its Triton slice and warp kernels, cuFFT
+    through torch.fft, eager autograd) on this B200, through its public API,
+    on the same seeded workloads, L2 flush and timing as this build's lines:
+    the batched spectral-NCC step (forward_spectral_ncc(ap) +
+    forward_spectral_ncc(lateral) + backward, 64 candidates, f32 and bf16
+    storage), the PoU cone-beam forward + gradient in the 4x4x4 and 2x2x2
+    block configurations, and the forward-only spectral NCC at out_res 128 /
+    256 / 512.  ``mine`` holds this build's numbers for the same workloads;
+    each entry carries both and their ratio."""
+    from fvr import synthetic
+
+    mods = _reference_modules()
+    if mods is None:
+        return {"unavailable": "the reference is not installed in baseline/_ref"}
+    te, cb = mods
+    out = {"source": "baseline/_ref (pip install --no-deps of the reference checkout), imported as fvr_reference",
+           "l2": "flushed before every timed step (256 MiB write)"}
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        t, _ = _time_steps(torch, fn, steps, flush)
+        return statistics.mean(t)
+
+    vol = synthetic.make_ellipsoid_volume(VOL_N, SEED)
+    poses = torch.from_numpy(synthetic.make_poses(CANDIDATES, SEED + 1)).to(dev)
+    tp = torch.from_numpy(synthetic.make_poses(1, SEED + 2)).to(dev)
+    eng = te.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0, device=dev,
+                                use_triton=True)
+    with torch.no_grad():
+        f_ap = eng.prepare_spectral_target(eng(tp, view="ap", out_res=OUT_RES))
+        f_lat = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=OUT_RES))
+        fts = {R: eng.prepare_spectral_target(eng(tp, view="ap", out_res=R)) for R in (128, 256, 512)}
+
+    def sncc_step():
+        pp = poses.detach().requires_grad_(True)
+        (eng.forward_spectral_ncc(pp, f_ap, view="ap") + eng.forward_spectral_ncc(pp, f_lat, view="lateral")).backward()
+
+    screening = {}
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+        if name == "bf16":
+            eng.to_precision(dt)
+        ms = timed(sncc_step)
+        screening[name] = {"ms_per_step": ms, "pose_evals_per_s": CANDIDATES / (ms / 1e3)}
+    screening["workload"] = WORKLOAD
+    screening["api"] = "forward_spectral_ncc(ap) + forward_spectral_ncc(lateral) + backward(), eager, use_triton=True"
+    for k, v in mine["screening"].items():
+        screening[f"this_build_{k}"] = v
+        screening[f"ratio_{k}_over_reference_bf16"] = v / screening["bf16"]["pose_evals_per_s"]
+    out["screening"] = screening
+
+    fwd = {}
+    for R, ft in fts.items():
+        def fn():
+            with torch.no_grad():
+                return eng.forward_spectral_ncc(poses, ft, view="ap")
+
+        ms = timed(fn)
+        entry = {"ms_per_call": ms, "poses_per_s": CANDIDATES / (ms / 1e3)}
+        got = mine.get("forward_one_view", {}).get(str(R))
+        if got is not None:
+            entry["this_build_ms_per_call"] = got
+            entry["ratio_time_reference_over_this_build"] = ms / got
+        fwd[str(R)] = entry
+    fwd["storage"] = "bf16 (reference to_precision); this build: bf16 stencil"
+    out["spectral_ncc_forward_one_view"] = fwd
+    del eng, fts, f_ap, f_lat
+    torch.cuda.empty_cache()
+
+    pou = {}
+    for label, grid, pitch in (("grid4_P128_det0.8mm", 4, 0.8), ("grid2_P128_det1.0mm", 2, 1.0)):
+        pv = synthetic.make_ellipsoid_volume(192, SEED)
+        f = 1020.0 / pitch
+        k_inv = torch.tensor([[1.0 / f, 0.0, -128.0 / f], [0.0, 1.0 / f, -128.0 / f], [0.0, 0.0, 1.0]], device=dev)
+        mats = synthetic.make_pinhole_mats(CANDIDATES, SEED + 1, sad_mm=765.0, device=dev)
+        res = {}
+        for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+            m = cb.PerspectiveSlabFVR.from_volume(pv, vox_mm=1.0, grid_blocks=(grid,) * 3, block_res=64, overlap=0.5,
+                                                  dtype=dt).to(dev)
+            lattice = m.make_pinhole_lattice(k_inv, 1020.0, 256, 256)
+
+            def step():
+                mm = mats.detach().requires_grad_(True)
+                m.forward_pinhole(mm, lattice).sum().backward()
+
+            ms = timed(step)
+            res[name] = {"ms_per_step": ms, "pose_evals_per_s": CANDIDATES / (ms / 1e3), "blocks": int(m.B)}
+            got = mine.get("pou", {}).get(label, {}).get(name)
+            if got is not None:
+                res[name]["this_build_ms_per_step"] = got
+                res[name]["ratio_time_reference_over_this_build"] = ms / got
+            del m, lattice
+            torch.cuda.empty_cache()
+        pou[label] = res
+    pou["workload"] = ("forward_pinhole(mats).sum().backward(), 64 poses, seeded 192^3 volume, block_res 64 at 50% "
+                       "overlap (P = 128), SDD 1020 / SAD 765 mm, 256^2 detector")
+    out["pou_cone_beam"] = pou
+    return out
+
+
 REG_VOLUMES = ((128, 128, 128), (192, 192, 192), (160, 256, 256))  # (Z, Y, X) voxels at 1 mm
 REG_INITS = 4
 
@@ -826,6 +955,7 @@ def run_reference(args):
         step()
     dt = time.perf_counter() - t0
     value = CANDIDATES * args.steps / dt
+    torch_cpu = _reference_torch_cpu_sample(vol, poses, tpose, ncores)
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -834,7 +964,44 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "port",
                          "sample": "every step is one full workload step (64 candidates x 2 views, loss + gradient)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_pytorch_cpu": torch_cpu,
     }
+
+
+def _reference_torch_cpu_sample(vol, poses_np, tpose_np, ncores):
+    """The reference's own PyTorch-CPU implementation (baseline/_ref,
+    TorchDiffFVREngine with use_triton=False: grid_sample gather, torch.fft,
+    autograd) on the same workload step, timed over 3 steps after one warm-up
+    step, all host threads: reported beside the float64 C port, which is the
+    line's value."""
+    import torch
+
+    mods = _reference_modules()
+    if mods is None:
+        return {"unavailable": "the reference is not installed in baseline/_ref"}
+    te = mods[0]
+    torch.set_num_threads(ncores)
+    eng = te.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0, device="cpu",
+                                use_triton=False)
+    tp = torch.from_numpy(tpose_np)
+    with torch.no_grad():
+        f_ap = eng.prepare_spectral_target(eng(tp, view="ap", out_res=OUT_RES))
+        f_lat = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=OUT_RES))
+    poses = torch.from_numpy(poses_np)
+
+    def step():
+        pp = poses.detach().requires_grad_(True)
+        (eng.forward_spectral_ncc(pp, f_ap, view="ap") + eng.forward_spectral_ncc(pp, f_lat, view="lateral")).backward()
+
+    step()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        step()
+    dt = (time.perf_counter() - t0) / 3
+    return {"value": CANDIDATES / dt, "unit": UNIT, "cores": ncores, "ms_per_step": dt * 1e3,
+            "sample": "3 full workload steps (64 candidates x 2 views, loss + gradient) after 1 warm-up step",
+            "api": "baseline/_ref TorchDiffFVREngine(use_triton=False, device='cpu'): forward_spectral_ncc(ap) + "
+                   "forward_spectral_ncc(lateral) + backward()"}
 
 
 PRECISION_NAMES = ("f32", "bf16", "f16")

@@ -73,6 +73,8 @@ SIGNATURES = {
     "fvr_pou_build_blocks": (I32, [P, I64, I64, I64, P, P, I64, P, P, I64, P, P, I64, P, I64, P, I64, I64, I64, F64,
                                    P, P]),
     "fvr_pou_geo_stride": (I64, []),
+    "fvr_pou_pinhole_lattice": (I32, [P, F64, I64, I64, P, P, P, P, P, P]),
+    "fvr_spine_phantom": (I32, [I64, P, P]),
     "fvr_pou_pose": (I32, [P, P, I64, P, F64, P, I64, P, P, P]),
     "fvr_pou_rays_prep": (I32, [P, P, I64, I64, P, P, P, P]),
     "fvr_pou_rays_bwd_workspace": (I64, [I64, I64]),

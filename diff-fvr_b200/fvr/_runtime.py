@@ -18,12 +18,24 @@ _one_cache = {}
 
 
 def device_of(device):
+    if not torch.cuda.is_available():
+        raise L.FvrError("fvr_b200 computes on a CUDA (B200, sm_100a) device only and none is available; "
+                         "there is no CPU fallback")
     d = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     if d.type != "cuda":
         raise L.FvrError(f"fvr_b200 runs on CUDA devices only (requested {d}); there is no CPU path")
     if d.index is None:
         d = torch.device("cuda", torch.cuda.current_device())
     return d
+
+
+def compute_device(*tensors):
+    """The CUDA device a call computes on: that of its first CUDA tensor, else
+    the current CUDA device (inputs on the CPU are moved there by the caller)."""
+    for t in tensors:
+        if isinstance(t, torch.Tensor) and t.is_cuda:
+            return t.device
+    return device_of(None)
 
 
 def twiddles(n, prec, device):

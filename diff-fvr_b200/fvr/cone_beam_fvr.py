@@ -7,9 +7,11 @@ inverse-transformed and pinhole-warped onto the detector, and the blocks are
 summed with the 1/cos obliquity factor.  Block extraction, the block spectra
 (batched shared-memory FFT), the per-pose slices (stencil layout), the
 batched 2D IFFT, the warp-sum and the whole adjoint chain back to the pose
-matrices run in ``libfvr_b200.so``.  The one-time geometry tables (1D
-windows, supports, the pinhole lattice) are small host / tensor glue exactly
-as in the reference.
+matrices run in ``libfvr_b200.so``, and so does the FP64 pinhole lattice.
+The one-time block layout (1D windows and their supports, block centres) is
+small host arithmetic.  Inputs on the CPU are moved to the model's CUDA
+device and results come back on the device of the pose inputs; there is no
+CPU compute path.
 """
 from __future__ import annotations
 
@@ -32,31 +34,36 @@ SLAB_PRESETS: Dict[str, Dict[str, object]] = {
 }
 
 
-def _pou_1d_np(length: int, n_blocks: int, overlap: float):
+def _pou_windows(length: int, n_blocks: int, overlap: float):
+    """Partition-of-unity weights along one axis as an fp64 array
+    ``[n_blocks, length]`` and the block pitch (cone_beam_fvr.py:42-61).
+
+    The axis is cut at the ``n_blocks - 1`` interior boundaries ``j * step``.
+    Around each boundary the two neighbouring blocks cross-fade over a band of
+    half-width ``h = max(2, step * overlap)`` voxels: with ``s`` the voxel
+    centre's progress through the band (0 before it, 1 after it), the block
+    above takes ``sin^2(pi s / 2)`` and the block below ``cos^2(pi s / 2)``,
+    so the weights at every voxel sum to one."""
     if n_blocks <= 1:
-        return [np.ones(length)], float(length)
+        return np.ones((1, length)), float(length)
     step = length / float(n_blocks)
-    ov = max(2.0, step * overlap)
-    coords = np.arange(length) + 0.5
-    ws = []
-    for i in range(n_blocks):
-        w = np.ones(length)
-        if i > 0:
-            x0, x1 = i * step - ov, i * step + ov
-            t = np.clip((coords - x0) / (x1 - x0), 0.0, 1.0)
-            w = w * 0.5 * (1.0 - np.cos(np.pi * t))
-        if i < n_blocks - 1:
-            x0, x1 = (i + 1) * step - ov, (i + 1) * step + ov
-            t = np.clip((coords - x0) / (x1 - x0), 0.0, 1.0)
-            w = w * 0.5 * (1.0 + np.cos(np.pi * t))
-        ws.append(w)
-    return ws, step
+    h = max(2.0, step * overlap)
+    centres = np.arange(length) + 0.5
+    bounds = step * np.arange(1, n_blocks)
+    s = np.clip((centres[None, :] - (bounds[:, None] - h)) / (2.0 * h), 0.0, 1.0)
+    fade_in = np.sin(0.5 * np.pi * s) ** 2
+    fade_out = np.cos(0.5 * np.pi * s) ** 2
+    w = np.ones((n_blocks, length))
+    w[1:] *= fade_in
+    w[:-1] *= fade_out
+    return w, step
 
 
 def _make_pou_1d(length: int, n_blocks: int, overlap: float):
-    """Raised-cosine partition-of-unity windows summing to 1 (cone_beam_fvr.py:42-61)."""
-    ws, step = _pou_1d_np(length, n_blocks, overlap)
-    return [torch.from_numpy(w.astype(np.float32)) for w in ws], float(step)
+    """Raised-cosine partition-of-unity windows summing to 1, as a list of
+    float32 tensors (cone_beam_fvr.py:42-61)."""
+    w, step = _pou_windows(length, n_blocks, overlap)
+    return [torch.from_numpy(row.astype(np.float32)) for row in w], float(step)
 
 
 def _sinc2_precomp_1d(n: int, p: int) -> torch.Tensor:
@@ -135,7 +142,10 @@ def edge_dominant_ncc(pred, target, border_crop=None, multiscale_weight=0.25, re
     else the per-item values [B]."""
     W = int(pred.shape[-1])
     crop = max(4, W // 8) if border_crop is None else int(border_crop)
-    return _EdgeNCCFn.apply(pred, target, crop, float(multiscale_weight), reduction == "mean")
+    home = pred.device
+    dev = RT.compute_device(pred, target)
+    out = _EdgeNCCFn.apply(pred.to(dev), target.to(dev), crop, float(multiscale_weight), reduction == "mean")
+    return out if out.device == home else out.to(home)
 
 
 _LATTICE_CACHE: Dict[Tuple, Tuple] = {}
@@ -296,7 +306,7 @@ class PerspectiveSlabFVR(nn.Module):
         self.pad_mult = int(pad_mult)
         self.P = self.block_res * self.pad_mult
         ks = tuple(int(k) for k in grid_blocks)
-        wl, steps = zip(*[_pou_1d_np(n, k, overlap) for n, k in zip((n0, n1, n2), ks)])
+        wl, steps = zip(*[_pou_windows(n, k, overlap) for n, k in zip((n0, n1, n2), ks)])
         ov = [max(2, int(round(s * overlap))) if k > 1 else 0 for s, k in zip(steps, ks)]
         M = max(int(np.ceil(s + 2 * o)) for s, o in zip(steps, ov)) + (1 if max(ks) > 1 else 0)
         self.M = M
@@ -415,59 +425,58 @@ class PerspectiveSlabFVR(nn.Module):
 
     @staticmethod
     def _extract_detector_basis(srcs, trg_pts, u_det=None, v_det=None, n_0=None):
-        """Orthonormal detector axes (cone_beam_fvr.py:575-596)."""
-        c_det = trg_pts.mean(dim=(1, 2))
-        if u_det is None:
-            u_raw = trg_pts[:, 0, -1] - trg_pts[:, 0, 0]
-            u_det = u_raw / (u_raw.norm(dim=-1, keepdim=True) + 1e-12)
-        if v_det is None:
-            v_raw = trg_pts[:, -1, 0] - trg_pts[:, 0, 0]
-            v_det = v_raw / (v_raw.norm(dim=-1, keepdim=True) + 1e-12)
+        """Unit detector axes ``(N, 3)`` of explicit lattices ``trg_pts (N, H, W, 3)``
+        (cone_beam_fvr.py:575-596): u along each lattice's first row, v along its
+        first column, n the unit ``v x u`` turned to face away from the source
+        (towards the lattice's centroid).  Axes that are given are kept;
+        differentiable in the lattice and the sources."""
+        first = trg_pts[:, 0, 0]
+        edges = torch.stack([trg_pts[:, 0, -1] - first, trg_pts[:, -1, 0] - first], dim=1)
+        edges = edges / (edges.norm(dim=-1, keepdim=True) + 1e-12)
+        u = edges[:, 0] if u_det is None else u_det
+        v = edges[:, 1] if v_det is None else v_det
         if n_0 is None:
-            n_raw = torch.cross(v_det, u_det, dim=-1)
-            n_0 = n_raw / (n_raw.norm(dim=-1, keepdim=True) + 1e-12)
-            flip = ((c_det - srcs) * n_0).sum(dim=-1, keepdim=True) < 0
-            n_0 = torch.where(flip, -n_0, n_0)
-        return u_det, v_det, n_0
-
-    @staticmethod
-    def _make_ray_cache(src0, trg0, u0, v0, n0):
-        """SE(3)-invariant camera-frame ray coefficients (cone_beam_fvr.py:523-545)."""
-        rays0 = (trg0 - src0.view(1, 1, 3)).float()
-        r0_hat = rays0 * torch.rsqrt((rays0 * rays0).sum(dim=-1, keepdim=True).clamp(min=1e-12))
-        cos0 = (r0_hat * n0.float().view(1, 1, 3)).sum(dim=-1).clamp(min=0.1)
-        inv_cos_hw = (1.0 / cos0).contiguous()
-        rx_hw = ((r0_hat * u0.float().view(1, 1, 3)).sum(dim=-1) * inv_cos_hw).contiguous()
-        ry_hw = ((r0_hat * v0.float().view(1, 1, 3)).sum(dim=-1) * inv_cos_hw).contiguous()
-        return (rx_hw, ry_hw, inv_cos_hw, rx_hw.reshape(-1).contiguous(), ry_hw.reshape(-1).contiguous(),
-                inv_cos_hw.reshape(-1).contiguous())
+            normal = torch.linalg.cross(v, u, dim=-1)
+            normal = normal / (normal.norm(dim=-1, keepdim=True) + 1e-12)
+            facing = ((trg_pts.mean(dim=(1, 2)) - srcs) * normal).sum(dim=-1, keepdim=True)
+            n_0 = torch.where(facing < 0, -normal, normal)
+        return u, v, n_0
 
     @staticmethod
     def make_pinhole_lattice(k_inv, sdd_mm, height, width):
-        """Camera-space pinhole lattice + ray cache, an 11-tuple (cone_beam_fvr.py:705-728)."""
+        """Camera-frame pinhole lattice and SE(3)-invariant ray cache as the
+        reference's 11-tuple ``(src0, trg0, u0, v0, n0, rx_hw, ry_hw, ic_hw,
+        rx_flat, ry_flat, ic_flat)`` (cone_beam_fvr.py:705-728), formed in FP64
+        by ``fvr_pou_pinhole_lattice`` and stored as float32 on ``k_inv``'s
+        device (pixel centres at +1/2, source at the camera origin)."""
         k0 = k_inv.squeeze(0) if k_inv.ndim == 3 else k_inv
-        device, dtype = k0.device, torch.float32
-        cols = torch.arange(width, device=device, dtype=dtype) + 0.5
-        rows = torch.arange(height, device=device, dtype=dtype) + 0.5
-        rr, cc = torch.meshgrid(rows, cols, indexing="ij")
-        pix = torch.stack([cc, rr, torch.ones_like(cc)], dim=-1)
-        cam_dirs = torch.einsum("ij,hwj->hwi", k0.to(dtype=dtype), pix)
-        trg0 = cam_dirs * (float(sdd_mm) / cam_dirs[..., 2:3].clamp(min=1e-6))
-        src0 = torch.zeros(3, device=device, dtype=dtype)
-        u0, v0, n0 = PerspectiveSlabFVR._extract_detector_basis(src0.unsqueeze(0), trg0.unsqueeze(0))
-        u0s, v0s, n0s = u0.squeeze(0), v0.squeeze(0), n0.squeeze(0)
-        ray_cache = PerspectiveSlabFVR._make_ray_cache(src0, trg0, u0s, v0s, n0s)
-        return (src0, trg0, u0s, v0s, n0s, *ray_cache)
+        home = k0.device
+        dev = RT.device_of(home if home.type == "cuda" else None)
+        H, W = int(height), int(width)
+        kk = (_ct.c_double * 9)(*[float(x) for x in k0.detach().double().cpu().reshape(9)])
+        trg0 = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+        rays = torch.empty((3, H, W), dtype=torch.float32, device=dev)
+        basis = torch.empty(9, dtype=torch.float64, device=dev)
+        L.call("fvr_pou_pinhole_lattice", kk, float(sdd_mm), H, W, L.ptr(trg0), L.ptr(rays[0]), L.ptr(rays[1]),
+               L.ptr(rays[2]), L.ptr(basis), L.stream_ptr(dev))
+        trg0, rays, basis = trg0.to(home), rays.to(home), basis.float().to(home)
+        rx, ry, ic = rays[0], rays[1], rays[2]
+        src0 = torch.zeros(3, dtype=torch.float32, device=home)
+        return (src0, trg0, basis[0:3], basis[3:6], basis[6:9], rx, ry, ic, rx.reshape(-1), ry.reshape(-1),
+                ic.reshape(-1))
 
     # ---------------------------------------------------------------- rendering
 
     def _forward_from_lattice(self, pose_mats, lattice):
         """Camera-frame lattice moved by pose matrices (cone_beam_fvr.py:670-688)."""
+        home = pose_mats.device
         if len(lattice) >= 11:
             key, _, (rx, ry, ic) = _prepared_lattice(lattice, self._dev)
-            mats = pose_mats if pose_mats.device == self._dev else pose_mats.to(self._dev)
-            return _PinholeFn.apply(mats, self, rx, ry, ic, key)
-        return self._forward_explicit(pose_mats, lattice)
+            mats = pose_mats if home == self._dev else pose_mats.to(self._dev)
+            out = _PinholeFn.apply(mats, self, rx, ry, ic, key)
+        else:
+            out = self._forward_explicit(pose_mats, lattice)
+        return out if out.device == home else out.to(home)
 
     def _forward_explicit(self, pose_mats, lattice):
         from .cone_beam_rays import forward_explicit
@@ -496,8 +505,12 @@ class PerspectiveSlabFVR(nn.Module):
         lattices ``(N, H, W, 3)`` (cone_beam_fvr.py:598-612)."""
         from .cone_beam_rays import project_rays_batched
 
+        home, dev = trg_pts.device, self._dev
+        srcs, trg_pts = srcs.to(dev), trg_pts.to(dev)
+        u_det, v_det, n_0 = (None if a is None else a.to(dev) for a in (u_det, v_det, n_0))
         u_det, v_det, n_0 = self._extract_detector_basis(srcs, trg_pts, u_det, v_det, n_0)
-        return project_rays_batched(self, srcs, trg_pts, u_det, v_det, n_0)
+        out = project_rays_batched(self, srcs, trg_pts, u_det, v_det, n_0)
+        return out if out.device == home else out.to(home)
 
     def project_rays(self, src, trg_pts, u_det=None, v_det=None, n_0=None):
         """Single-pose form of :meth:`project_rays_batched` (cone_beam_fvr.py:614-632)."""
@@ -505,42 +518,48 @@ class PerspectiveSlabFVR(nn.Module):
             src.unsqueeze(0), trg_pts.unsqueeze(0), None if u_det is None else u_det.unsqueeze(0),
             None if v_det is None else v_det.unsqueeze(0), None if n_0 is None else n_0.unsqueeze(0)).squeeze(0)
 
+    # Detector frames of the two C-arm views in the volume's (z, y, x) axes:
+    # (u0, v0, n0) = detector columns, detector rows, beam direction.  The
+    # source sits at -SAD along n0 and the detector plane at SDD - SAD.
+    _CARM_AXES = {"ap": ((0.0, 0.0, 1.0), (1.0, 0.0, 0.0), (0.0, 1.0, 0.0)),
+                  "lateral": ((0.0, 1.0, 0.0), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0))}
+
+    @staticmethod
+    def _axis_rotation(angle_rad, axis):
+        """Rotation by ``angle_rad`` (0-d tensor) about coordinate axis ``axis``
+        (differentiable): the plane of the two following axes turns."""
+        i, j = (axis + 1) % 3, (axis + 2) % 3
+        c, s = torch.cos(angle_rad), torch.sin(angle_rad)
+        one, zero = torch.ones_like(c), torch.zeros_like(c)
+        rows = [[one if r == k else zero for k in range(3)] for r in range(3)]
+        rows[i][i], rows[i][j], rows[j][i], rows[j][j] = c, -s, s, c
+        return torch.stack([torch.stack(r) for r in rows])
+
     def forward_carm_view(self, yaw_deg, pitch_deg, roll_deg, tx_vox, ty_vox, tz_vox, sad_mm, sdd_mm, det_px,
                           det_fov_mm, view="ap"):
-        """C-arm AP / lateral projection ``(det_px, det_px)`` (cone_beam_fvr.py:761-832)."""
-        device = self._dev
-        args = [torch.as_tensor(a, dtype=torch.float32).to(device) for a in
-                (yaw_deg, pitch_deg, roll_deg, tx_vox, ty_vox, tz_vox)]
-        y_r, p_r, r_r = (torch.deg2rad(a) for a in args[:3])
-        cy, sy = torch.cos(y_r), torch.sin(y_r)
-        cp, sp = torch.cos(p_r), torch.sin(p_r)
-        cr, sr = torch.cos(r_r), torch.sin(r_r)
-        zero = torch.zeros((), device=device, dtype=torch.float32)
-        one = torch.ones((), device=device, dtype=torch.float32)
-        rz = torch.stack([torch.stack([one, zero, zero]), torch.stack([zero, cy, -sy]), torch.stack([zero, sy, cy])])
-        ry = torch.stack([torch.stack([cr, zero, sr]), torch.stack([zero, one, zero]), torch.stack([-sr, zero, cr])])
-        rx = torch.stack([torch.stack([cp, -sp, zero]), torch.stack([sp, cp, zero]), torch.stack([zero, zero, one])])
-        rot = rz @ ry @ rx
-        u_lin = torch.linspace(-0.5, 0.5, det_px, device=device) * float(det_fov_mm)
-        v_lin = torch.linspace(-0.5, 0.5, det_px, device=device) * float(det_fov_mm)
-        vv, uu = torch.meshgrid(v_lin, u_lin, indexing="ij")
-        det_d = float(sdd_mm - sad_mm)
-        if view == "ap":
-            src0 = torch.tensor([0.0, -float(sad_mm), 0.0], device=device)
-            trg0 = torch.stack([vv, torch.full_like(uu, det_d), uu], dim=-1)
-            u_det0 = torch.tensor([0.0, 0.0, 1.0], device=device)
-            v_det0 = torch.tensor([1.0, 0.0, 0.0], device=device)
-            n0 = torch.tensor([0.0, 1.0, 0.0], device=device)
-        else:
-            src0 = torch.tensor([0.0, 0.0, -float(sad_mm)], device=device)
-            trg0 = torch.stack([vv, uu, torch.full_like(uu, det_d)], dim=-1)
-            u_det0 = torch.tensor([0.0, 1.0, 0.0], device=device)
-            v_det0 = torch.tensor([1.0, 0.0, 0.0], device=device)
-            n0 = torch.tensor([0.0, 0.0, 1.0], device=device)
-        t_shift = torch.stack([args[5], args[4], args[3]]) * self.vox_mm
-        src = rot @ src0 - t_shift
-        trg_pts = torch.einsum("ij,hwj->hwi", rot, trg0) - t_shift
-        return self.project_rays(src, trg_pts, u_det=rot @ u_det0, v_det=rot @ v_det0, n_0=rot @ n0)
+        """C-arm AP / lateral projection ``(det_px, det_px)`` (cone_beam_fvr.py:761-832).
+
+        The pose turns the C-arm about the volume's z axis by yaw, then its y
+        axis by roll, then its x axis by pitch (``R = R_z R_y R_x`` on (z, y, x)
+        coordinates, degrees) and shifts it by ``-(tz, ty, tx)`` voxels.
+        Detector pixels span ``det_fov_mm`` on a ``det_px``-point grid from
+        edge to edge.  Rendered by the explicit-ray path; differentiable in
+        the six pose scalars, returned on their device."""
+        home = torch.as_tensor(yaw_deg).device
+        dev = self._dev
+        ang = [torch.deg2rad(torch.as_tensor(a, dtype=torch.float32).to(dev)) for a in (yaw_deg, roll_deg, pitch_deg)]
+        rot = (self._axis_rotation(ang[0], 0) @ self._axis_rotation(ang[1], 1)) @ self._axis_rotation(ang[2], 2)
+        shift = torch.stack([torch.as_tensor(t, dtype=torch.float32).to(dev) for t in (tz_vox, ty_vox, tx_vox)])
+        shift = shift * self.vox_mm
+        axes = self._CARM_AXES["ap" if view == "ap" else "lateral"]
+        u0, v0, n0 = (torch.tensor(a, dtype=torch.float32, device=dev) for a in axes)
+        grid = torch.linspace(-0.5, 0.5, int(det_px), device=dev) * float(det_fov_mm)
+        plane = float(sdd_mm - sad_mm) * n0
+        trg0 = grid[:, None, None] * v0 + grid[None, :, None] * u0 + plane
+        src = rot @ (-float(sad_mm) * n0) - shift
+        trg_pts = trg0 @ rot.T - shift
+        img = self.project_rays(src, trg_pts, u_det=rot @ u0, v_det=rot @ v0, n_0=rot @ n0)
+        return img if img.device == home else img.to(home)
 
     def cache_diffdrr_geometry(self, drr_mod, out_res):
         raise ImportError("cache_diffdrr_geometry needs the third-party diffdrr package, which this build does "

@@ -1,9 +1,9 @@
 """Volume ingest on B200: the array side of ``src/fvr/dicom_loader.py``.
 
-``resample_isotropic_cube`` and ``hu_to_attenuation`` keep the reference's
-signatures, checks and NumPy-in / NumPy-out contract (dicom_loader.py:11-30,
-179-188) and run on the GPU (``fvr_ingest_resample``,
-``fvr_hu_to_attenuation``).  ``attenuation_cube`` fuses the two into one pass
+``resample_isotropic_cube``, ``hu_to_attenuation`` and ``create_spine_phantom``
+keep the reference's signatures, checks and NumPy-in / NumPy-out contract
+(dicom_loader.py:11-30, 114-188) and run on the GPU (``fvr_ingest_resample``,
+``fvr_hu_to_attenuation``, ``fvr_spine_phantom``).  ``attenuation_cube`` fuses the two into one pass
 and returns the device tensor, which a :class:`fvr.TorchDiffFVREngine` or a
 :class:`fvr.cone_beam_fvr.PerspectiveSlabFVR` takes directly, so a CT goes
 from HU to the spectrum precompute without a host round trip.  Reading DICOM
@@ -62,6 +62,19 @@ def hu_to_attenuation(volume_hu: np.ndarray, device: Optional[torch.device] = No
     out = torch.empty_like(hu)
     L.call("fvr_hu_to_attenuation", L.ptr(hu), int(hu.numel()), L.ptr(out), L.stream_ptr(dev))
     return out.cpu().numpy()
+
+
+def create_spine_phantom(size: int = 128, device: Optional[torch.device] = None):
+    """Synthetic CT of a torso with five vertebrae in HU (dicom_loader.py:114-176):
+    ``(volume [size]^3 float32 (Z, Y, X), spacing (1.0, 1.0, 1.0) mm)``.
+    Air is -1000 HU, the torso 40, cortical bone 1100, trabecular bone 400,
+    the spinal canal 15, spinous processes 900 and transverse processes 850;
+    the labels equal the reference's float32 construction voxel for voxel."""
+    dev = RT.device_of(device)
+    n = int(size)
+    out = torch.empty((n, n, n), dtype=torch.float32, device=dev)
+    L.call("fvr_spine_phantom", n, L.ptr(out), L.stream_ptr(dev))
+    return out.cpu().numpy(), (1.0, 1.0, 1.0)
 
 
 def attenuation_cube(volume_hu, spacing, target_res,

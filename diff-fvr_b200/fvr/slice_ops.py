@@ -3,7 +3,8 @@ public functions of src/fvr/triton_slice.py), computed by libfvr_b200.so.
 
 ``fourier_slice_3d(vol_ri, u_xyz, v_xyz, fx, fy, center_xyz)`` returns
 ``(B_vol, N_pose, 2, K)`` in the volume dtype with zero-padding partial
-interpolation, differentiable in ``u_xyz`` and ``v_xyz`` (the reference never
+interpolation on the volume's device (CPU inputs are computed on the current
+CUDA device and copied back), differentiable in ``u_xyz`` and ``v_xyz`` (the reference never
 returns a volume gradient from its fused path, triton_slice.py:339; a volume
 that requires grad raises here instead of silently routing elsewhere).
 
@@ -20,6 +21,7 @@ from typing import Tuple
 import torch
 
 from . import _lib as L
+from . import _runtime as RT
 
 
 class _Slice3DFn(torch.autograd.Function):
@@ -72,7 +74,10 @@ def fourier_slice_3d(
         raise L.FvrError("fourier_slice_3d: gradients with respect to the volume are not provided "
                          "(the reference's fused path does not return them either)")
     cx, cy, cz = center_xyz
-    return _Slice3DFn.apply(vol_ri, u_xyz, v_xyz, fx, fy, cx, cy, cz)
+    home = vol_ri.device
+    dev = RT.compute_device(vol_ri, u_xyz, v_xyz)
+    out = _Slice3DFn.apply(vol_ri.to(dev), u_xyz.to(dev), v_xyz.to(dev), fx.to(dev), fy.to(dev), cx, cy, cz)
+    return out if out.device == home else out.to(home)
 
 
 def fourier_slice_3d_torch(vol_ri, u_xyz, v_xyz, fx, fy, center_xyz):
@@ -139,8 +144,12 @@ def pou_pinhole_warp_sum(imgs, d_b, cu, cv, rx_hw, ry_hw, inv_cos_hw, rx_flat, r
     """Batched PoU pinhole bilinear warp + obliquity sum ``(N, H, W)``
     (triton_slice.py:787-808); differentiable in imgs, d_b, cu, cv."""
     H, W = int(rx_hw.shape[0]), int(rx_hw.shape[1])
-    out = _WarpSumFn.apply(imgs, d_b, cu, cv, rx_flat, ry_flat, ic_flat, inv_ds, c_idx)
-    return out.view(out.shape[0], H, W)
+    home = imgs.device
+    dev = RT.compute_device(imgs, d_b, cu, cv)
+    out = _WarpSumFn.apply(imgs.to(dev), d_b.to(dev), cu.to(dev), cv.to(dev), rx_flat.to(dev), ry_flat.to(dev),
+                           ic_flat.to(dev), inv_ds, c_idx)
+    out = out.view(out.shape[0], H, W)
+    return out if out.device == home else out.to(home)
 
 
 def pou_pinhole_warp_sum_torch(imgs, d_b, cu, cv, rx_hw, ry_hw, inv_cos_hw, inv_ds, c_idx):

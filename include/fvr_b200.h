@@ -232,6 +232,17 @@ int fvr_pou_build_blocks(const float* vol, int64_t n0, int64_t n1, int64_t n2, c
  * vecs[N][12] = (s, u, v, n) when mats is NULL), slice axes flip(u)*vscale,
  * flip(v)*vscale; offs[B][N][3] (fp64) = (d_b, cu, cv) = (c_b - s).(n, u, v)
  * for the block centres [B][3].  cone_beam_fvr.py:485-488, 507-521, 676-682. */
+/* Pinhole lattice of an H x W detector from k_inv[9] (row-major K^-1, host
+ * memory) and the source-to-detector distance, all in FP64: per pixel the
+ * detector point trg0[H][W][3] = d sdd / max(d_z, 1e-6) with
+ * d = K^-1 (c + 1/2, r + 1/2, 1), the ray numbers rx, ry, ic [H][W]
+ * (ic = 1 / max(r.n0, 0.1), rx = (r.u0) ic, ry = (r.v0) ic for the unit ray r
+ * to the point), and basis[9] (device) = u0, v0, n0: unit vectors along the
+ * first row and first column and the unit normal facing the lattice.
+ * Replaces PerspectiveSlabFVR.make_pinhole_lattice with _make_ray_cache and
+ * _extract_detector_basis, src/fvr/cone_beam_fvr.py:523-545, 575-596, 705-728. */
+int fvr_pou_pinhole_lattice(const double* k_inv, double sdd_mm, int64_t H, int64_t W, float* trg0, float* rx,
+                            float* ry, float* ic, double* basis, void* stream);
 int64_t fvr_pou_geo_stride(void);
 int fvr_pou_pose(const float* mats, const float* vecs, int64_t N, const double* base12, double vscale,
                  const float* centers, int64_t B, double* geo, double* offs, void* stream);
@@ -350,6 +361,11 @@ int fvr_ingest_resample(const float* hu, int64_t Z, int64_t Y, int64_t X, double
 /* out[i] = max(0, (hu[i] + 1000) / 1000) in float32 (hu_to_attenuation,
  * src/fvr/dicom_loader.py:179-188). */
 int fvr_hu_to_attenuation(const float* hu, int64_t n, float* out, void* stream);
+/* Spine phantom out[n][n][n] (Z, Y, X) in HU: air, a soft-tissue torso and
+ * five vertebrae (cortical and trabecular body, canal, spinous and transverse
+ * processes), evaluated in float32 exactly as the NumPy construction of
+ * create_spine_phantom, src/fvr/dicom_loader.py:114-176.  n <= 2048. */
+int fvr_spine_phantom(int64_t n, float* out, void* stream);
 
 /* ----------------------------------------------------------- timing ---- */
 /* cudaEventRecordWithFlags(event, stream, external ? cudaEventRecordExternal

@@ -5,7 +5,7 @@ Usage (needs the reference checkout; run from the repository root):
     python tests/golden/make_golden.py <reference checkout> [name,name,...]
 
 (names: slice_warp, torch_engine, pou, numpy_renderer, articulated,
-ingest_targets; all of them when none is given)
+ingest_targets, phantom; all of them when none is given)
 
 It imports the reference's ``fvr`` package (``src/fvr``) with empty stand-ins
 for ``pydicom`` / ``SimpleITK`` (only ``dicom_loader`` needs them, and nothing
@@ -324,6 +324,21 @@ def gen_ingest_and_targets(ref_root: Path):
     np.savez_compressed(HERE / "ingest_targets.npz", **out)
 
 
+def gen_phantom(ref_root: Path):
+    """create_spine_phantom (dicom_loader.py:114-176) at the size the
+    reference's engine test uses (64) and at odd and non-power-of-two sizes;
+    stored as int16 HU (every label is an integer)."""
+    from fvr import dicom_loader
+
+    out = {}
+    for n in (64, 37, 50, 96):
+        vol, sp = dicom_loader.create_spine_phantom(n)
+        assert vol.dtype == np.float32 and np.array_equal(vol, np.round(vol))
+        out[f"hu_{n}"] = vol.astype(np.int16)
+        out[f"spacing_{n}"] = np.array(sp)
+    np.savez_compressed(HERE / "phantom.npz", **out)
+
+
 def main():
     if len(sys.argv) < 2:
         sys.exit("usage: make_golden.py <reference checkout> [name,name,...]")
@@ -336,7 +351,8 @@ def main():
     gens = {"slice_warp": lambda: gen_slice_and_warp(ts), "torch_engine": lambda: gen_torch_engine(te),
             "pou": lambda: gen_pou(cb), "numpy_renderer": lambda: gen_numpy(df, gr),
             "articulated": lambda: gen_articulated(ref_root),
-            "ingest_targets": lambda: gen_ingest_and_targets(ref_root)}
+            "ingest_targets": lambda: gen_ingest_and_targets(ref_root),
+            "phantom": lambda: gen_phantom(ref_root)}
     for name, gen in gens.items():
         if only is None or name in only:
             gen()

@@ -62,8 +62,13 @@ def test_status_strings_and_queries(lib):
     assert L.query("fvr_stencil_bytes", 3, 3, 3, 1) == 4 * 4 * 4 * 32
 
 
-def test_product_path_refuses_cpu_tensors():
+def test_product_path_fails_loudly_without_a_gpu():
+    """CPU inputs are moved to the CUDA device; with none present the call
+    raises FvrError instead of computing on the CPU."""
     import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
 
     import fvr._lib as L
     from fvr.slice_ops import fourier_slice_3d

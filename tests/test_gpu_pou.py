@@ -90,7 +90,8 @@ def test_carm_view_and_grads(model, golden, view):
     g = golden("pou")
     params = [torch.tensor(v, requires_grad=True) for v in (3.0, -2.0, 1.5, 1.0, -1.0, 0.5)]
     img = model.forward_carm_view(*params, sad_mm=300.0, sdd_mm=600.0, det_px=20, det_fov_mm=70.0, view=view)
-    (img * _t(g[f"carm_{view}_w"])).sum().backward()
+    assert img.device == params[0].device  # results come back on the pose scalars' device
+    (img * torch.as_tensor(g[f"carm_{view}_w"], dtype=torch.float32)).sum().backward()
     assert rel_l2(img.detach().cpu().numpy(), g[f"carm_{view}_out"]) < 2e-5
     grads = np.array([float(p.grad) for p in params])
     assert rel_l2(grads, g[f"carm_{view}_grad"]) < 1e-4
