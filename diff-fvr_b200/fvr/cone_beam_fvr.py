@@ -154,7 +154,9 @@ _LATTICE_CACHE: Dict[Tuple, Tuple] = {}
 def _prepared_lattice(lattice, device):
     """Device copies of an 11-tuple lattice's ray tables and its basis
     (src0, u0, v0, n0) as 12 host doubles, cached per (storage, device): the
-    lattice is a per-geometry constant, moved once."""
+    lattice is a per-geometry constant, moved once.  The entry holds the
+    lattice's own tensors, so their storage cannot be freed and reused by
+    another lattice while the entry exists."""
     key = tuple(int(t.data_ptr()) for t in lattice[:8]) + (str(device),)
     hit = _LATTICE_CACHE.get(key)
     if hit is None:
@@ -163,7 +165,7 @@ def _prepared_lattice(lattice, device):
         basis = torch.cat([lattice[i].reshape(3) for i in (0, 2, 3, 4)]).detach().double().cpu()
         base = (_ct.c_double * 12)(*[float(x) for x in basis])
         rays = tuple(t.detach().to(device=device, dtype=torch.float32).contiguous() for t in lattice[5:8])
-        hit = (key, base, rays)
+        hit = (key, base, rays, tuple(lattice[:8]))
         _LATTICE_CACHE[key] = hit
     return hit
 
@@ -234,13 +236,13 @@ class _PinholeFn(torch.autograd.Function):
                    _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), H * W, 0,
                    1.0 / model.ds_block, float(P // 2), L.ptr(out), s)
         ctx.save_for_backward(geo, offs, imgs, rx, ry, ic)
-        ctx.meta = (model, base_key, mats.dtype)
+        ctx.meta = (model, base, mats.dtype)
         return out
 
     @staticmethod
     def backward(ctx, g_out):
         geo, offs, imgs, rx, ry, ic = ctx.saved_tensors
-        model, base_key, mdt = ctx.meta
+        model, base, mdt = ctx.meta
         dev = geo.device
         B, N, P = model.B, int(geo.shape[0]), model.P
         H, W = int(rx.shape[0]), int(rx.shape[1])
@@ -257,7 +259,7 @@ class _PinholeFn(torch.autograd.Function):
         del grad_imgs
         gm = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
         L.call("fvr_pou_pose_backward", L.ptr(ws2), tiles, L.ptr(goffs), None, 0, L.ptr(geo), L.ptr(model.centers), B,
-               N, _LATTICE_CACHE[base_key][1], float(P) * model.ds_block, L.ptr(gm), None, s)
+               N, base, float(P) * model.ds_block, L.ptr(gm), None, s)
         return gm.to(mdt), None, None, None, None, None
 
 
@@ -471,7 +473,7 @@ class PerspectiveSlabFVR(nn.Module):
         """Camera-frame lattice moved by pose matrices (cone_beam_fvr.py:670-688)."""
         home = pose_mats.device
         if len(lattice) >= 11:
-            key, _, (rx, ry, ic) = _prepared_lattice(lattice, self._dev)
+            key, _, (rx, ry, ic), _ = _prepared_lattice(lattice, self._dev)
             mats = pose_mats if home == self._dev else pose_mats.to(self._dev)
             out = _PinholeFn.apply(mats, self, rx, ry, ic, key)
         else:
