@@ -17,7 +17,33 @@ __global__ void __launch_bounds__(256) copy_bytes_kernel(unsigned char* __restri
 
 }  // namespace
 
+#ifdef FVR_CHECK
+namespace fvr {
+int check_word_tc(unsigned long long* out, int clear);
+int check_word_pou(unsigned long long* out, int clear);
+int check_word_slice3d(unsigned long long* out, int clear);
+int check_word_np(unsigned long long* out, int clear);
+}  // namespace fvr
+#endif
+
 extern "C" {
+
+int fvr_check_words(unsigned long long* out, int n, int clear) {
+#ifdef FVR_CHECK
+  using Reader = int (*)(unsigned long long*, int);
+  const Reader readers[] = {fvr::check_word_tc, fvr::check_word_pou, fvr::check_word_slice3d, fvr::check_word_np};
+  constexpr int kUnits = sizeof(readers) / sizeof(readers[0]);
+  if (!out || n < kUnits) return FVR_ERR_ARG;
+  for (int i = 0; i < kUnits; ++i)
+    if (readers[i](out + i, clear)) return FVR_ERR_CUDA;
+  return FVR_OK;
+#else
+  (void)out;
+  (void)n;
+  (void)clear;
+  return FVR_ERR_UNSUPPORTED;
+#endif
+}
 
 int fvr_copy_bytes(void* dst, const void* src, int64_t n, void* stream) {
   if (!dst || !src || n < 0) return FVR_ERR_ARG;

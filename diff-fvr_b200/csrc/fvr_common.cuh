@@ -23,6 +23,63 @@ namespace fvr {
 
 constexpr int kWarp = 32;
 
+// ---- bounds-checked debug build --------------------------------------------
+// Built with -DFVR_CHECK (libfvr_b200_check.so), every global or shared
+// access guarded by fvr_checked(index, extent, site) whose index falls
+// outside [0, extent) is skipped (the guarded load reads zero, the guarded
+// store or atomic does nothing), and the first such event of each
+// translation unit is recorded in that unit's check word: the site code in
+// bits 40-63, the low 40 bits of the index below.  fvr_check_words reads and
+// clears the words.  The normal build compiles every guard to `true`.
+#ifdef FVR_CHECK
+static __device__ unsigned long long g_fvr_check_word;
+
+__device__ __forceinline__ bool fvr_checked(long long i, long long n, unsigned site) {
+  if (i >= 0 && i < n) return true;
+  atomicCAS(&g_fvr_check_word, 0ull,
+            (static_cast<unsigned long long>(site) << 40) | (static_cast<unsigned long long>(i) & 0xffffffffffull));
+  return false;
+}
+
+// Host side of one translation unit's check word (read, then optionally clear).
+#define FVR_CHECK_ACCESSOR(name)                                                              \
+  namespace fvr {                                                                             \
+  int name(unsigned long long* out, int clear) {                                              \
+    if (cudaMemcpyFromSymbol(out, g_fvr_check_word, sizeof(*out)) != cudaSuccess) return 1;   \
+    if (clear) {                                                                              \
+      const unsigned long long zero = 0ull;                                                   \
+      if (cudaMemcpyToSymbol(g_fvr_check_word, &zero, sizeof(zero)) != cudaSuccess) return 1; \
+    }                                                                                         \
+    return 0;                                                                                 \
+  }                                                                                           \
+  }
+#else
+__device__ __forceinline__ constexpr bool fvr_checked(long long, long long, unsigned) { return true; }
+#define FVR_CHECK_ACCESSOR(name)
+#endif
+
+// Checked read-only load / atomic add of element i of an n-element buffer.
+__device__ __forceinline__ float ldg_in(const float* p, long long i, long long n, unsigned site) {
+  return fvr_checked(i, n, site) ? __ldg(p + i) : 0.f;
+}
+__device__ __forceinline__ void atomic_add_in(float* p, long long i, long long n, unsigned site, float v) {
+  if (fvr_checked(i, n, site)) atomicAdd(p + i, v);
+}
+
+// Site codes of the checked accesses.
+enum : unsigned {
+  kSiteStencilEntry = 1,  // stencil entry gather
+  kSiteStencilScale,      // f16 brick scale
+  kSiteSnccTarget,        // spectral-NCC target / high-pass sample
+  kSitePlanar,            // planar drop-in gather
+  kSiteNpGather,          // NumPy-convention fp64 gather
+  kSiteWarpTap,           // PoU warp image tap (per-pixel paths)
+  kSiteWarpGrad,          // PoU warp adjoint image-gradient atomic
+  kSiteWarpStrip,         // PoU warp row-strip shared-memory access
+  kSiteWarpStripRow,      // PoU warp row-strip image row read
+  kSiteHalfImage,         // PoU half-spectrum image shared-memory access
+};
+
 template <typename T>
 struct Cx {
   T x, y;

@@ -59,7 +59,9 @@ __device__ __forceinline__ double2 np_sample(const double2* __restrict__ f, int 
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         const double w = wz[a] * wy[b] * wx[c];
-        const double2 v = __ldg(f + (static_cast<int64_t>(zs[a]) * H + ys[b]) * W + xs[c]);
+        const int64_t e = (static_cast<int64_t>(zs[a]) * H + ys[b]) * W + xs[c];
+        const double2 v = fvr_checked(e, static_cast<int64_t>(D) * H * W, kSiteNpGather) ? __ldg(f + e)
+                                                                                          : make_double2(0.0, 0.0);
         re += w * v.x;
         im += w * v.y;
       }
@@ -289,3 +291,5 @@ int fvr_np_pair_moments(const void* a, const void* b, int64_t sh, int64_t sw, vo
 }
 
 }  // extern "C"
+
+FVR_CHECK_ACCESSOR(check_word_np)

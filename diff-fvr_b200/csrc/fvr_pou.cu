@@ -486,6 +486,244 @@ __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kerne
 
 
 // ----------------------------------------------------------------------------
+// Half-spectrum block images.  Only the real part of each block image is
+// used, and Re IFFT2(X) is the (real) inverse transform of the Hermitian part
+// X_h[a][b] = (X[a][b] + conj X[-a][-b]) / 2 of the transform input X =
+// ifftshift(S).  X_h is determined by its P/2 + 1 columns b = 0 .. P/2, so a
+// CTA keeps a P x (P/2 + 1) complex array in shared memory (half of the full
+// image): complex inverse FFTs down those columns, then the rows are real
+// transforms of Hermitian row spectra, done two at a time (row y1 + i row y2
+// through one complex FFT: the real part is y1's image row, the imaginary
+// part y2's).  The adjoint mirrors it: the FFT of the real image gradient is
+// Hermitian, so two real rows share one complex FFT (separated as
+// (Z[k] + conj Z[-k]) / 2 and (Z[k] - conj Z[-k]) / 2i), half the columns are
+// transformed, and the other half of G is read as conj G[-a][-b].  Every
+// slice sample is still gathered (X_h needs both S(k) and S(-k); the
+// zero-padded interpolation is not exactly Hermitian near the edges).  Half
+// the shared memory lets two CTAs share an SM, one gathering while the other
+// transforms.
+// ----------------------------------------------------------------------------
+constexpr int kPouHalfThreads = 256;
+
+__host__ __device__ constexpr int pou_half_cols(int P) { return P / 2 + 1; }
+
+// Half image (P x (P/2 + 1) complex, pitch P/2 + 1: odd, so a warp's column
+// accesses fall in distinct 64-bit banks), the 2P-entry tables, and one
+// P-complex scratch row per warp.
+__host__ __device__ constexpr int64_t pou_half_smem(int P) {
+  return static_cast<int64_t>(P) * pou_half_cols(P) * 8 + 40 * 2 * static_cast<int64_t>(P) +
+         static_cast<int64_t>(kPouHalfThreads / 32) * P * 8 + 32;
+}
+
+template <int M>
+__device__ __forceinline__ int pou_half_tab_offset() {
+  constexpr int P = 32 * M;
+  return ((P * pou_half_cols(P) * 8 + 15) / 16) * 16;
+}
+
+// One slice sample (row entry P + i, column entry j) of block stencil st.
+template <int DT>
+__device__ __forceinline__ void pou_tab_gather(const Stencil& st, const AxisTables& tab, int P, int i, int j,
+                                               Raw<DT>& raw) {
+  const TabCell cell = tab_cell(st, tab.idx[P + i], tab.frac[P + i], tab.idx[j], tab.frac[j]);
+  tab_load<DT>(st, cell, raw);
+}
+
+template <int DT, int M>
+__global__ void __launch_bounds__(kPouHalfThreads, 2) pou_slice_c2r_kernel(PouSliceArgs a, float* __restrict__ imgs) {
+  constexpr int P = 32 * M, H = P / 2, NC = pou_half_cols(P), PITCH = NC, NW = kPouHalfThreads / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem);
+  const AxisTables tab = axis_tables(smem + pou_half_tab_offset<M>(), 2 * P);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  float* scratch = reinterpret_cast<float*>(smem + pou_half_tab_offset<M>() + 40 * 2 * P) + wid * 2 * P;
+  const int n = blockIdx.x, b = blockIdx.y;
+  const Stencil st = pou_block_stencil(a, b);
+  pou_image_tables(tab, a, a.geo + n * kGeo);
+  WarpFft<M, true> fft;
+  fft.init(lane);
+  __syncthreads();
+  // columns kb = 0 .. H of X_h, each an inverse FFT along the rows
+  for (int kb = wid; kb < NC; kb += NW) {
+    const int j = kb + H < P ? kb + H : kb - H;          // S column of X[., kb]
+    const int jm = H - kb >= 0 ? H - kb : H - kb + P;    // S column of X[., -kb]
+    Cx<float> x[M];
+    {
+      Raw<DT> raw[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int ka = lane + 32 * m;
+        pou_tab_gather<DT>(st, tab, P, ka + H < P ? ka + H : ka - H, j, raw[m]);
+      }
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int ka = lane + 32 * m, i = ka + H < P ? ka + H : ka - H;
+        Interp o;
+        pou_table_sample<DT, false>(st, raw[m], tab.frac[P + i], tab.frac[j], o);
+        x[m] = Cx<float>{0.5f * o.sr, 0.5f * o.si};
+      }
+    }
+    {
+      Raw<DT> raw[M];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int ka = lane + 32 * m;
+        pou_tab_gather<DT>(st, tab, P, H - ka >= 0 ? H - ka : H - ka + P, jm, raw[m]);
+      }
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int ka = lane + 32 * m, im = H - ka >= 0 ? H - ka : H - ka + P;
+        Interp o;
+        pou_table_sample<DT, false>(st, raw[m], tab.frac[P + im], tab.frac[jm], o);
+        x[m].x = fmaf(0.5f, o.sr, x[m].x);
+        x[m].y = fmaf(-0.5f, o.si, x[m].y);
+      }
+    }
+    fft.run(x, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + kb] = x[k];
+  }
+  __syncthreads();
+  // rows two at a time: row y1 + i row y2 (Hermitian row spectra, the upper
+  // half read as conj of the lower), one inverse FFT, real part -> y1, imaginary -> y2
+  const float scale = 1.f / static_cast<float>(P * P);
+  float* out = imgs + (static_cast<int64_t>(b) * a.N + n) * P * P;
+  for (int t = wid; t < H; t += NW) {
+    const int y1 = 2 * t, y2 = 2 * t + 1;
+    const Cx<float>* r1 = buf + wfft_pos<M>(y1) * PITCH;
+    const Cx<float>* r2 = buf + wfft_pos<M>(y2) * PITCH;
+    Cx<float> z[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int kc = lane + 32 * m;
+      const bool lo = kc <= H;
+      const int src = lo ? kc : P - kc;
+      const Cx<float> c1 = r1[src], c2 = r2[src];
+      const float s = lo ? 1.f : -1.f;  // conjugate the mirrored half
+      z[m] = Cx<float>{c1.x - s * c2.y, s * c1.y + c2.x};
+    }
+    fft.run(z, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+      const int xi = k + M * brev5(lane);
+      scratch[xi] = z[k].x * scale;
+      scratch[P + xi] = z[k].y * scale;
+    }
+    __syncwarp();
+    const int oy1 = y1 + H < P ? y1 + H : y1 - H, oy2 = y2 + H < P ? y2 + H : y2 - H;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int xo = lane + 32 * m, xs = xo + H < P ? xo + H : xo - H;  // fftshift of the row
+      out[oy1 * P + xo] = scratch[xs];
+      out[oy2 * P + xo] = scratch[P + xs];
+    }
+    __syncwarp();
+  }
+}
+
+// Adjoint of pou_slice_c2r_kernel: G = fftshift(fft2(ifftshift(g))) / P^2 kept
+// as its columns kb = 0 .. P/2, then the per-sample products with the
+// spectrum derivatives as in pou_fft_slice_adjoint_kernel.
+template <int DT, int M>
+__global__ void __launch_bounds__(kPouHalfThreads, 2) pou_r2c_slice_adjoint_kernel(PouSliceArgs a,
+                                                                                  const float* __restrict__ gimg,
+                                                                                  double* __restrict__ partial) {
+  constexpr int P = 32 * M, H = P / 2, NC = pou_half_cols(P), PITCH = NC, NW = kPouHalfThreads / 32, GROUP = 4;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ double red[6 * NW];
+  Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem);
+  const AxisTables tab = axis_tables(smem + pou_half_tab_offset<M>(), 2 * P);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Cx<float>* zrow = reinterpret_cast<Cx<float>*>(smem + pou_half_tab_offset<M>() + 40 * 2 * P) + wid * P;
+  const int n = blockIdx.x, b = blockIdx.y;
+  const Stencil st = pou_block_stencil(a, b);
+  pou_image_tables(tab, a, a.geo + n * kGeo);
+  WarpFft<M, false> fft;
+  fft.init(lane);
+  const float* g = gimg + (static_cast<int64_t>(b) * a.N + n) * P * P;
+  // rows of ifftshift(g) two at a time through one complex FFT, separated
+  // into the two Hermitian row spectra; columns 0 .. H kept (natural row order)
+  for (int t = wid; t < H; t += NW) {
+    const int a1 = 2 * t, a2 = 2 * t + 1;
+    const int y1 = a1 + H < P ? a1 + H : a1 - H, y2 = a2 + H < P ? a2 + H : a2 - H;
+    Cx<float> z[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int c = lane + 32 * m, xs = c + H < P ? c + H : c - H;
+      z[m] = Cx<float>{__ldg(g + y1 * P + xs), __ldg(g + y2 * P + xs)};
+    }
+    fft.run(z, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) zrow[k + M * brev5(lane)] = z[k];
+    __syncwarp();
+    for (int kb = lane; kb < NC; kb += 32) {
+      const Cx<float> p = zrow[kb], q = zrow[kb == 0 ? 0 : P - kb];  // Z[k], Z[-k]
+      // G1 = (Z[k] + conj Z[-k]) / 2, G2 = (Z[k] - conj Z[-k]) / 2i
+      buf[a1 * PITCH + kb] = Cx<float>{0.5f * (p.x + q.x), 0.5f * (p.y - q.y)};
+      buf[a2 * PITCH + kb] = Cx<float>{0.5f * (p.y + q.y), 0.5f * (q.x - p.x)};
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int kb = wid; kb < NC; kb += NW) {
+    Cx<float> x[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) x[m] = buf[(lane + 32 * m) * PITCH + kb];
+    fft.run(x, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + kb] = x[k];
+  }
+  __syncthreads();
+  const float scale = 1.f / static_cast<float>(P * P);
+  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int q0 = threadIdx.x; q0 < P * P; q0 += kPouHalfThreads * GROUP) {
+    Raw<DT> raw[GROUP];
+#pragma unroll
+    for (int u = 0; u < GROUP; ++u) {
+      const int q = q0 + u * kPouHalfThreads;
+      const int i = q < P * P ? q / P : 0, j = q < P * P ? q - (q / P) * P : 0;
+      TabCell cell = tab_cell(st, tab.idx[P + i], tab.frac[P + i], tab.idx[j], tab.frac[j]);
+      if (q >= P * P) cell.e = -1;
+      tab_load<DT>(st, cell, raw[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < GROUP; ++u) {
+      const int q = q0 + u * kPouHalfThreads;
+      if (q >= P * P) continue;
+      const int i = q / P, j = q - i * P;
+      const float4 fa = tab.frac[P + i], fb = tab.frac[j];
+      Interp o;
+      pou_table_sample<DT, true>(st, raw[u], fa, fb, o);
+      const int ka = i + H < P ? i + H : i - H, kb = j + H < P ? j + H : j - H;
+      const bool lo = kb <= H;
+      const int gpos = lo ? wfft_pos<M>(ka) * PITCH + kb : wfft_pos<M>(ka == 0 ? 0 : P - ka) * PITCH + (P - kb);
+      Cx<float> G = fvr_checked(gpos, P * PITCH, kSiteHalfImage) ? buf[gpos] : Cx<float>{0.f, 0.f};
+      if (!lo) G.y = -G.y;
+      const float gx = G.x * scale, gy = G.y * scale;
+      const float e0 = gx * o.dxr + gy * o.dxi, e1 = gx * o.dyr + gy * o.dyi, e2 = gx * o.dzr + gy * o.dzi;
+      const float fx = fb.w, fy = fa.w;
+      acc[0] = fmaf(fx, e0, acc[0]);
+      acc[1] = fmaf(fx, e1, acc[1]);
+      acc[2] = fmaf(fx, e2, acc[2]);
+      acc[3] = fmaf(fy, e0, acc[3]);
+      acc[4] = fmaf(fy, e1, acc[4]);
+      acc[5] = fmaf(fy, e2, acc[5]);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const double v = warp_sum(static_cast<double>(acc[m]));
+    if (lane == 0) red[m * NW + wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double sum = 0.0;
+    for (int w = 0; w < NW; ++w) sum += red[threadIdx.x * NW + w];
+    partial[(static_cast<int64_t>(n) * gridDim.y + b) * 6 + threadIdx.x] = sum;
+  }
+}
+
+// ----------------------------------------------------------------------------
 // pinhole warp + sum  (triton_slice.py:348-407 / 409-496)
 // ----------------------------------------------------------------------------
 
@@ -618,16 +856,19 @@ __device__ __forceinline__ WarpRow warp_row(const WarpArgs<OT>& a, int64_t bn, d
 // multiple of 4, so each row starts on a 16-byte boundary); zero outside.
 __device__ __forceinline__ void warp_row_quads(const float* img, int P, int iy, int xq, float4& r0, float4& r1) {
   const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-  r0 = iy >= 0 && iy < P ? __ldg(reinterpret_cast<const float4*>(img + static_cast<int64_t>(iy) * P) + xq) : z;
-  r1 = iy + 1 >= 0 && iy + 1 < P ? __ldg(reinterpret_cast<const float4*>(img + static_cast<int64_t>(iy + 1) * P) + xq)
-                                 : z;
+  const bool q_in = fvr_checked(4 * xq + 3, P, kSiteWarpStripRow);
+  r0 = q_in && iy >= 0 && iy < P ? __ldg(reinterpret_cast<const float4*>(img + static_cast<int64_t>(iy) * P) + xq) : z;
+  r1 = q_in && iy + 1 >= 0 && iy + 1 < P
+           ? __ldg(reinterpret_cast<const float4*>(img + static_cast<int64_t>(iy + 1) * P) + xq)
+           : z;
 }
 
 // Image rows iy and iy + 1 of block image bn at column x (zero outside).
 __device__ __forceinline__ void warp_row_pair(const float* img, int P, int iy, int x, float& r0, float& r1) {
   const bool xin = x >= 0 && x < P;
-  r0 = xin && iy >= 0 && iy < P ? __ldg(img + static_cast<int64_t>(iy) * P + x) : 0.f;
-  r1 = xin && iy + 1 >= 0 && iy + 1 < P ? __ldg(img + static_cast<int64_t>(iy + 1) * P + x) : 0.f;
+  r0 = xin && iy >= 0 && iy < P ? ldg_in(img, static_cast<int64_t>(iy) * P + x, P * P, kSiteWarpStripRow) : 0.f;
+  r1 = xin && iy + 1 >= 0 && iy + 1 < P ? ldg_in(img, static_cast<int64_t>(iy + 1) * P + x, P * P, kSiteWarpStripRow)
+                                        : 0.f;
 }
 
 // Row-strip forward of one CTA: the pixel's sum over the listed blocks in
@@ -762,6 +1003,7 @@ __device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, doubl
           const double fx = floor(px);
           const float tx = static_cast<float>(px - fx);
           const int o = k * W2 + static_cast<int>(fx) + 1;
+          if (!fvr_checked(o + 1, static_cast<long long>(cn) * W2, kSiteWarpStrip)) continue;
           atomicAdd(S + o, __float2int_rn(g * (1.f - tx) * fix));
           atomicAdd(S + o + 1, __float2int_rn(g * tx * fix));
           atomicAdd(Gs + o, __float2int_rn(g * fix));
@@ -784,8 +1026,9 @@ __device__ void warp_rows_adjoint(const WarpArgs<OT>& a, int n, bool live, doubl
         const float sv = static_cast<float>(S[o]) * unfix;
         sc += static_cast<double>(dr[o]) * static_cast<double>(sv);
         if (gi && sv != 0.f) {
-          if (iy >= 0 && iy < P) atomicAdd(gi + static_cast<int64_t>(iy) * P + x, sv * (1.f - ty));
-          if (iy + 1 >= 0 && iy + 1 < P) atomicAdd(gi + static_cast<int64_t>(iy + 1) * P + x, sv * ty);
+          if (iy >= 0 && iy < P) atomic_add_in(gi, static_cast<int64_t>(iy) * P + x, P * P, kSiteWarpGrad, sv * (1.f - ty));
+          if (iy + 1 >= 0 && iy + 1 < P)
+            atomic_add_in(gi, static_cast<int64_t>(iy + 1) * P + x, P * P, kSiteWarpGrad, sv * ty);
         }
       }
       sa = warp_sum(sa);
@@ -830,10 +1073,10 @@ __global__ void __launch_bounds__(256) pou_warp_kernel(WarpArgs<OT> a, float* __
       const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
       const float* img = a.imgs + bn * P * P;
       const bool x0 = ix >= 0, x1 = ix + 1 < P, y0 = iy >= 0, y1 = iy + 1 < P;
-      const float v00 = (x0 && y0) ? __ldg(img + iy * P + ix) : 0.f;
-      const float v01 = (x1 && y0) ? __ldg(img + iy * P + ix + 1) : 0.f;
-      const float v10 = (x0 && y1) ? __ldg(img + (iy + 1) * P + ix) : 0.f;
-      const float v11 = (x1 && y1) ? __ldg(img + (iy + 1) * P + ix + 1) : 0.f;
+      const float v00 = (x0 && y0) ? ldg_in(img, iy * P + ix, P * P, kSiteWarpTap) : 0.f;
+      const float v01 = (x1 && y0) ? ldg_in(img, iy * P + ix + 1, P * P, kSiteWarpTap) : 0.f;
+      const float v10 = (x0 && y1) ? ldg_in(img, (iy + 1) * P + ix, P * P, kSiteWarpTap) : 0.f;
+      const float v11 = (x1 && y1) ? ldg_in(img, (iy + 1) * P + ix + 1, P * P, kSiteWarpTap) : 0.f;
       acc += (v00 * (1.f - tx) + v01 * tx) * (1.f - ty) + (v10 * (1.f - tx) + v11 * tx) * ty;
     }
   }
@@ -895,16 +1138,16 @@ __global__ void __launch_bounds__(256) pou_warp_bwd_kernel(WarpArgs<OT> a, const
           const float tx = static_cast<float>(px - fx), ty = static_cast<float>(py - fy);
           const float* img = a.imgs + bn * P * P;
           const bool x0 = ix >= 0, x1 = ix + 1 < P, y0 = iy >= 0, y1 = iy + 1 < P;
-          const float v00 = (x0 && y0) ? __ldg(img + iy * P + ix) : 0.f;
-          const float v01 = (x1 && y0) ? __ldg(img + iy * P + ix + 1) : 0.f;
-          const float v10 = (x0 && y1) ? __ldg(img + (iy + 1) * P + ix) : 0.f;
-          const float v11 = (x1 && y1) ? __ldg(img + (iy + 1) * P + ix + 1) : 0.f;
+          const float v00 = (x0 && y0) ? ldg_in(img, iy * P + ix, P * P, kSiteWarpTap) : 0.f;
+          const float v01 = (x1 && y0) ? ldg_in(img, iy * P + ix + 1, P * P, kSiteWarpTap) : 0.f;
+          const float v10 = (x0 && y1) ? ldg_in(img, (iy + 1) * P + ix, P * P, kSiteWarpTap) : 0.f;
+          const float v11 = (x1 && y1) ? ldg_in(img, (iy + 1) * P + ix + 1, P * P, kSiteWarpTap) : 0.f;
           if (grad_imgs) {
             float* gi = grad_imgs + bn * P * P;
-            if (x0 && y0) atomicAdd(gi + iy * P + ix, g * (1.f - tx) * (1.f - ty));
-            if (x1 && y0) atomicAdd(gi + iy * P + ix + 1, g * tx * (1.f - ty));
-            if (x0 && y1) atomicAdd(gi + (iy + 1) * P + ix, g * (1.f - tx) * ty);
-            if (x1 && y1) atomicAdd(gi + (iy + 1) * P + ix + 1, g * tx * ty);
+            if (x0 && y0) atomic_add_in(gi, iy * P + ix, P * P, kSiteWarpGrad, g * (1.f - tx) * (1.f - ty));
+            if (x1 && y0) atomic_add_in(gi, iy * P + ix + 1, P * P, kSiteWarpGrad, g * tx * (1.f - ty));
+            if (x0 && y1) atomic_add_in(gi, (iy + 1) * P + ix, P * P, kSiteWarpGrad, g * (1.f - tx) * ty);
+            if (x1 && y1) atomic_add_in(gi, (iy + 1) * P + ix + 1, P * P, kSiteWarpGrad, g * tx * ty);
           }
           const float dpx = ((v01 - v00) * (1.f - ty) + (v11 - v10) * ty) * inv_ds;
           const float dpy = ((v10 - v00) * (1.f - tx) + (v11 - v01) * tx) * inv_ds;
@@ -1124,29 +1367,28 @@ static PouBase make_base(const double* base12) {
 
 using namespace fvr;
 
+// Opt a half-spectrum image kernel in to its dynamic shared memory (above the
+// default 48 KB) with the largest shared-memory carve-out, so two CTAs fit.
+template <typename K>
+static bool pou_half_attr(K kernel, int64_t smem) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) ==
+             cudaSuccess &&
+         cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
+}
+
 template <int DT, int M>
 static int pou_image_launch(bool adjoint, const PouSliceArgs& a, int B, const float* gimg, float* imgs,
                             double* part, cudaStream_t s) {
-  const int64_t smem = pou_image_smem(32 * M);
+  const int64_t smem = pou_half_smem(32 * M);
   dim3 grid(static_cast<unsigned>(a.N), static_cast<unsigned>(B));
   if (adjoint) {
-    static bool attr = false;
-    if (!attr) {
-      if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem)) != cudaSuccess)
-        return FVR_ERR_CUDA;
-      attr = true;
-    }
-    pou_fft_slice_adjoint_kernel<DT, M><<<grid, kPouImgThreads, smem, s>>>(a, gimg, part);
+    static const bool attr = pou_half_attr(pou_r2c_slice_adjoint_kernel<DT, M>, smem);
+    if (!attr) return FVR_ERR_CUDA;
+    pou_r2c_slice_adjoint_kernel<DT, M><<<grid, kPouHalfThreads, smem, s>>>(a, gimg, part);
   } else {
-    static bool attr = false;
-    if (!attr) {
-      if (cudaFuncSetAttribute(pou_slice_ifft_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem)) != cudaSuccess)
-        return FVR_ERR_CUDA;
-      attr = true;
-    }
-    pou_slice_ifft_kernel<DT, M><<<grid, kPouImgThreads, smem, s>>>(a, imgs);
+    static const bool attr = pou_half_attr(pou_slice_c2r_kernel<DT, M>, smem);
+    if (!attr) return FVR_ERR_CUDA;
+    pou_slice_c2r_kernel<DT, M><<<grid, kPouHalfThreads, smem, s>>>(a, imgs);
   }
   FVR_LAUNCH_CHECK();
   return FVR_OK;
@@ -1418,3 +1660,5 @@ int fvr_pou_rays_bwd(const float* trg, const double* geo, int64_t N, int64_t K, 
 }
 
 }  // extern "C"
+
+FVR_CHECK_ACCESSOR(check_word_pou)

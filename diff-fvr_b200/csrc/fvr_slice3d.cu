@@ -12,7 +12,8 @@ namespace fvr {
 template <typename VT>
 __device__ __forceinline__ float planar_at(const VT* ch, int D, int H, int W, int z, int y, int x) {
   if (z < 0 || z >= D || y < 0 || y >= H || x < 0 || x >= W) return 0.f;
-  return ldf(ch + (static_cast<int64_t>(z) * H + y) * W + x);
+  const int64_t i = (static_cast<int64_t>(z) * H + y) * W + x;
+  return fvr_checked(i, static_cast<int64_t>(D) * H * W, kSitePlanar) ? ldf(ch + i) : 0.f;
 }
 
 template <typename VT>
@@ -189,3 +190,5 @@ int fvr_slice3d_bwd(const void* vol, int dtype, int64_t B, int64_t D, int64_t H,
 }
 
 }  // extern "C"
+
+FVR_CHECK_ACCESSOR(check_word_slice3d)

@@ -180,10 +180,17 @@ __device__ __forceinline__ Cell stencil_cell(const Stencil& s, double px, double
   return c;
 }
 
+__device__ __forceinline__ int64_t stencil_entries(const Stencil& s) {
+  return static_cast<int64_t>(s.D + 1) * (s.H + 1) * (s.W + 1);
+}
+__device__ __forceinline__ int64_t stencil_scales(const Stencil& s) {
+  return static_cast<int64_t>((s.D + kBrick) / kBrick) * ((s.H + kBrick) / kBrick) * ((s.W + kBrick) / kBrick);
+}
+
 template <int DT>
 __device__ __forceinline__ void raw_load(const Stencil& s, const Cell& c, Raw<DT>& r) {
   if constexpr (DT == FVR_F32) {
-    if (c.e < 0) {
+    if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
       return;
@@ -192,7 +199,7 @@ __device__ __forceinline__ void raw_load(const Stencil& s, const Cell& c, Raw<DT
     ldg256(p, r.q[0], r.q[1]);
     ldg256(p + 2, r.q[2], r.q[3]);
   } else {
-    if (c.e < 0) {
+    if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
       r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
       if constexpr (DT == FVR_F16) r.sc = 0.f;
       return;
@@ -201,7 +208,8 @@ __device__ __forceinline__ void raw_load(const Stencil& s, const Cell& c, Raw<DT
     ldg256(p, r.q[0], r.q[1]);
     if constexpr (DT == FVR_F16) {
       const int bx = (s.W + 1 + kBrick - 1) / kBrick, by = (s.H + 1 + kBrick - 1) / kBrick;
-      r.sc = __ldg(s.scales + (static_cast<int64_t>(c.ez / kBrick) * by + c.ey / kBrick) * bx + c.ex / kBrick);
+      const int64_t si = (static_cast<int64_t>(c.ez / kBrick) * by + c.ey / kBrick) * bx + c.ex / kBrick;
+      r.sc = fvr_checked(si, stencil_scales(s), kSiteStencilScale) ? __ldg(s.scales + si) : 0.f;
     }
   }
 }
@@ -304,7 +312,7 @@ __device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa
 template <int DT>
 __device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw<DT>& r) {
   if constexpr (DT == FVR_F32) {
-    if (c.e < 0) {
+    if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
       return;
@@ -313,7 +321,7 @@ __device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw
     ldg256(p, r.q[0], r.q[1]);
     ldg256(p + 2, r.q[2], r.q[3]);
   } else {
-    if (c.e < 0) {
+    if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
       r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
       if constexpr (DT == FVR_F16) r.sc = 0.f;
       return;
@@ -321,7 +329,8 @@ __device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw
     ldg256(static_cast<const uint4*>(s.data) + static_cast<int64_t>(c.e) * 2, r.q[0], r.q[1]);
     if constexpr (DT == FVR_F16) {
       const int bx = (s.W + kBrick) / kBrick, by = (s.H + kBrick) / kBrick;
-      r.sc = __ldg(s.scales + ((c.ez / kBrick) * by + c.ey / kBrick) * bx + c.ex / kBrick);
+      const int si = ((c.ez / kBrick) * by + c.ey / kBrick) * bx + c.ex / kBrick;
+      r.sc = fvr_checked(si, stencil_scales(s), kSiteStencilScale) ? __ldg(s.scales + si) : 0.f;
     }
   }
 }

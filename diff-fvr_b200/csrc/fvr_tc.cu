@@ -300,7 +300,7 @@ __device__ __forceinline__ SCell sncc_cell(const Stencil& s, int4 ia, float4 fa,
 template <int DT>
 __device__ __forceinline__ void sncc_load(const Stencil& s, const SCell& c, Raw<DT>& r) {
   if constexpr (DT == FVR_F32) {
-    if (c.e < 0) {
+    if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
       return;
@@ -309,7 +309,7 @@ __device__ __forceinline__ void sncc_load(const Stencil& s, const SCell& c, Raw<
     ldg256(p, r.q[0], r.q[1]);
     ldg256(p + 2, r.q[2], r.q[3]);
   } else {
-    if (c.e < 0) {
+    if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
       r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
       if constexpr (DT == FVR_F16) r.sc = 0.f;
       return;
@@ -319,7 +319,8 @@ __device__ __forceinline__ void sncc_load(const Stencil& s, const SCell& c, Raw<
       const unsigned bx = static_cast<unsigned>(s.W + kBrick) / kBrick, by = static_cast<unsigned>(s.H + kBrick) / kBrick;
       const unsigned ex = static_cast<unsigned>(c.ex) / kBrick, ey = static_cast<unsigned>(c.ey) / kBrick,
                      ez = static_cast<unsigned>(c.ez) / kBrick;
-      r.sc = __ldg(s.scales + (ez * by + ey) * bx + ex);
+      const unsigned si = (ez * by + ey) * bx + ex;
+      r.sc = fvr_checked(si, stencil_scales(s), kSiteStencilScale) ? __ldg(s.scales + si) : 0.f;
     }
   }
 }
@@ -392,8 +393,9 @@ __device__ __forceinline__ void sncc_run(const SnccArgs& a, const SnccTab& tab, 
         if (!ok) cell.e = -1;
         sncc_load<DT>(a.st, cell, raw[g]);
         const int q = ig * R + j;
-        Ts[g] = ok ? __ldg(ft + q) : make_float2(0.f, 0.f);
-        hs[g] = ok ? (a.hp ? __ldg(a.hp + q) : 1.f) : 0.f;
+        const bool inq = ok && fvr_checked(q, static_cast<long long>(R) * R, kSiteSnccTarget);
+        Ts[g] = inq ? __ldg(ft + q) : make_float2(0.f, 0.f);
+        hs[g] = inq ? (a.hp ? __ldg(a.hp + q) : 1.f) : 0.f;
       }
 #pragma unroll
       for (int g = 0; g < GROUP; ++g) {
@@ -1189,3 +1191,5 @@ int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const floa
 }
 
 }  // extern "C"
+
+FVR_CHECK_ACCESSOR(check_word_tc)

@@ -23,6 +23,10 @@ _OPTIONAL = [
     ("cone_beam_fvr", ("PerspectiveSlabFVR", "SLAB_PRESETS", "sample_isocenter_parity_offsets")),
     ("diff_fvr", ("DifferentiableFourierVolumeRenderer",)),
     ("gradients", ("SpectralGradientEngine",)),
+    ("core_engine", ("RobustDiffFVREngine", "detect_radio_opaque_metal")),
+    ("gradient_optimizer", ("GradientRegistrationOptimizer",)),
+    ("dicom_loader", ("create_spine_phantom", "hu_to_attenuation", "resample_isotropic_cube")),
+    ("articulated_spine", ("ArticulatedSpineModel", "VertebralSegment")),
 ]
 for _mod, _names in _OPTIONAL:
     try:

@@ -30,6 +30,7 @@ F64_ = 3
 SIGNATURES = {
     "fvr_status_string": (ctypes.c_char_p, [I32]),
     "fvr_version": (I32, []),
+    "fvr_check_words": (I32, [P, I32, I32]),
     "fvr_device_supported": (I32, [I32]),
     "fvr_fft_supported": (I32, [I64]),
     "fvr_fft_twiddles": (I32, [I64, I32, P, P]),

@@ -122,18 +122,27 @@ class DifferentiableFourierVolumeRenderer:
         """Spatial DRR: fftshift(ifft2(ifftshift(slice))) * scale, ReLU, centre crop (diff_fvr.py:152-182)."""
         if interp_order != 1:
             raise L.FvrError("only linear interpolation (interp_order=1) is implemented on the GPU path")
-        sl = self._slices_device([(yaw_deg, pitch_deg, roll_deg, tx, ty, view)])[0]
-        sh, sw = sl.shape
-        scale = (self.pz * self.py * self.px) / (sh * sw)
-        crop = (0, sh, 0, sw)
-        if crop_to_roi:
-            nz, ny, nx = self.orig_shape
-            th = nz if view in ("lateral", "ap") else ny
-            tw = ny if view == "lateral" else nx
-            crop = ((sh - th) // 2, th, (sw - tw) // 2, tw)
-        img = RT.fft2d(sl.contiguous(), inverse=True, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT,
-                       scale=scale / (sh * sw), out_mode=RT.OUT_RELU, crop=crop)
-        return img.cpu().numpy()
+        return self._drrs_device([(yaw_deg, pitch_deg, roll_deg, tx, ty, view)], crop_to_roi)[0].cpu().numpy()
+
+    def _drrs_device(self, specs, crop_to_roi=True):
+        """render_drr for several (yaw, pitch, roll, tx, ty, view) specs: every
+        slice in one gather launch, then one inverse FFT per view; device
+        float64 images."""
+        slices = self._slices_device(specs)
+        out = []
+        for sl, spec in zip(slices, specs):
+            view = spec[5]
+            sh, sw = sl.shape
+            scale = (self.pz * self.py * self.px) / (sh * sw)
+            crop = (0, sh, 0, sw)
+            if crop_to_roi:
+                nz, ny, nx = self.orig_shape
+                th = nz if view in ("lateral", "ap") else ny
+                tw = ny if view == "lateral" else nx
+                crop = ((sh - th) // 2, th, (sw - tw) // 2, tw)
+            out.append(RT.fft2d(sl.contiguous(), inverse=True, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT,
+                                scale=scale / (sh * sw), out_mode=RT.OUT_RELU, crop=crop))
+        return out
 
     def _ncc_moments(self, specs, targets):
         """mom[item][5] for specs against device targets (list of complex128 [sh, sw])."""

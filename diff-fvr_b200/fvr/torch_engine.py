@@ -125,37 +125,33 @@ def _sncc_fused(eng, p, views, ftargs, hp, R, out=None, loss_out=None):
     return loss, grad
 
 
-def _sncc_backward(eng, p, views, mom, g, g_stride, R, out=None):
-    dev = p.device
-    C = int(p.shape[0])
-    D, H, W = eng._stencil.dims
-    grad = torch.empty((C, 6), dtype=torch.float32, device=dev) if out is None else out
-    nv = len(views)
-    L.call("fvr_tc_sncc_backward", L.ptr(mom), nv, (ctypes.c_int * nv)(*views), L.ptr(g), int(g_stride), L.ptr(p),
-           C, D, H, W, RT.kappa(R, eng.spacing[0]), L.ptr(grad), 0, L.stream_ptr(dev))
-    return grad
-
-
 class _SpectralNCCFn(torch.autograd.Function):
     """Zero-IFFT spectral NCC (torch_engine.py:269-307), summed over the given
-    views, with a moment-based adjoint."""
+    views.  When the poses need a gradient, the forward pass already runs the
+    fused loss-and-gradient launch (moments kernel + its dependent epilogue)
+    and keeps dL/dposes; backward only scales it by the upstream gradient (the
+    loss is a scalar, so its pose gradient is linear in that factor).
+    Without a gradient the cheaper value-only moments (3 instead of 17) run."""
 
     @staticmethod
     def forward(ctx, poses, eng, views, hp, R, *ftargs):
         p = poses.detach().to(device=eng._dev, dtype=torch.float32).contiguous()
-        with_grad = bool(ctx.needs_input_grad[0])
-        mom, loss = _sncc_forward(eng, p, views, ftargs, hp, R, with_grad)
-        ctx.save_for_backward(p, mom)
-        ctx.meta = (eng, views, R, poses.dtype)
-        return loss[len(views)]
+        nv = len(views)
+        ctx.meta = (views, poses.dtype)
+        if ctx.needs_input_grad[0]:
+            grad = torch.empty((int(p.shape[0]), 6), dtype=torch.float32, device=eng._dev)
+            loss = torch.empty(nv + 1, dtype=torch.float32, device=eng._dev)
+            _sncc_fused(eng, p, views, ftargs, hp, R, out=grad, loss_out=loss)
+            ctx.save_for_backward(grad)
+            return loss[nv]
+        _, loss = _sncc_forward(eng, p, views, ftargs, hp, R, False)
+        return loss[nv]
 
     @staticmethod
     def backward(ctx, g):
-        p, mom = ctx.saved_tensors
-        eng, views, R, pdt = ctx.meta
-        gg = g.detach().to(device=p.device, dtype=torch.float32).reshape(1).contiguous()
-        grad = _sncc_backward(eng, p, views, mom, gg, 0, R)
-        return (grad.to(pdt), None, None, None, None) + (None,) * len(views)
+        (grad,) = ctx.saved_tensors
+        views, pdt = ctx.meta
+        return ((grad * g.to(grad.dtype)).to(pdt), None, None, None, None) + (None,) * len(views)
 
 
 class _SliceFn(torch.autograd.Function):

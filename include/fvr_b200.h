@@ -39,6 +39,14 @@ typedef enum { FVR_F32 = 0, FVR_BF16 = 1, FVR_F16 = 2, FVR_F64 = 3 } fvr_dtype;
 
 const char* fvr_status_string(int status);
 int fvr_version(void);
+/* Check words of the bounds-checked debug build (libfvr_b200_check.so, built
+ * with -DFVR_CHECK; no reference counterpart): out[0..4) receive one word per
+ * kernel family (parallel-beam, PoU, planar drop-in gather, NumPy
+ * convention), 0 when every checked access stayed in bounds, else the first
+ * out-of-bounds access (site code << 40 | low 40 bits of its index), which
+ * the kernel skipped; clear != 0 resets them.  n >= 4.  The normal build
+ * returns FVR_ERR_UNSUPPORTED. */
+int fvr_check_words(unsigned long long* out, int n, int clear);
 /* 1 if the device (ordinal) is sm_100 (B200 family), 0 otherwise. */
 int fvr_device_supported(int device);
 

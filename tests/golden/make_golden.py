@@ -5,7 +5,7 @@ Usage (needs the reference checkout; run from the repository root):
     python tests/golden/make_golden.py <reference checkout> [name,name,...]
 
 (names: slice_warp, torch_engine, pou, numpy_renderer, articulated,
-ingest_targets, phantom; all of them when none is given)
+ingest_targets, phantom, registration; all of them when none is given)
 
 It imports the reference's ``fvr`` package (``src/fvr``) with empty stand-ins
 for ``pydicom`` / ``SimpleITK`` (only ``dicom_loader`` needs them, and nothing
@@ -324,6 +324,45 @@ def gen_ingest_and_targets(ref_root: Path):
     np.savez_compressed(HERE / "ingest_targets.npz", **out)
 
 
+def gen_registration(ref_root: Path):
+    """GradientRegistrationOptimizer.register_adam (gradient_optimizer.py:24-90)
+    and RobustDiffFVREngine.register_biplanar_robust (core_engine.py:109-224,
+    clean and metal branches) on a seeded 32^3 ellipsoid cube: trajectories,
+    final poses, losses and evaluation counts."""
+    from fvr import core_engine, diff_fvr, gradient_optimizer
+
+    out = {}
+    vol = _ellipsoids(32, 21).astype(np.float64)
+    out["vol"] = vol
+    truth = np.array([1.5, -1.0, 0.8, 0.6, -0.4, 0.5])
+    out["truth"] = truth
+    ren = diff_fvr.DifferentiableFourierVolumeRenderer(vol, pad_factor=2.0)
+    f_ap = ren.extract_frequency_slice(*truth[:3], tx=truth[3], ty=truth[5], view="ap")
+    f_lat = ren.extract_frequency_slice(*truth[:3], tx=truth[4], ty=truth[5], view="lateral")
+    opt = gradient_optimizer.GradientRegistrationOptimizer(ren)
+    r = opt.register_adam(f_ap, f_lat, np.zeros(6), max_iter=12)
+    out["adam_losses"] = np.array([t[1] for t in r["trajectory"]])
+    out["adam_poses"] = np.stack([t[2] for t in r["trajectory"]])
+    out["adam_final_pose"] = r["final_pose"]
+    out["adam_final_loss"] = np.array(r["final_loss"])
+    out["adam_iterations"] = np.array(r["iterations"])
+    eng = core_engine.RobustDiffFVREngine(vol, spacing=(1.0, 1.0, 1.0))
+    t_ap = eng.render_calibrated_drr(*truth[:3], tx=truth[3], ty=truth[5], view="ap")
+    t_lat = eng.render_calibrated_drr(*truth[:3], tx=truth[4], ty=truth[5], view="lateral")
+    out["target_ap"], out["target_lat"] = t_ap, t_lat
+    for tag, (a, b) in (("clean", (t_ap, t_lat)), ("metal", (t_ap.copy(), t_lat.copy()))):
+        if tag == "metal":
+            a[3:10, 20:27] = a.max() * 3.0
+            b[22:29, 4:11] = b.max() * 3.0
+            out["metal_target_ap"], out["metal_target_lat"] = a, b
+        res = eng.register_biplanar_robust(a, b, initial_pose=(0.5, 0.0, -0.3, 0.0, 0.2, 0.0), max_iter=2)
+        out[f"robust_{tag}_pose"] = np.asarray(res["final_pose"])
+        out[f"robust_{tag}_loss"] = np.array(res["final_loss"])
+        out[f"robust_{tag}_evals"] = np.array(res["evaluations"])
+        out[f"robust_{tag}_metal"] = np.array(res["metal_detected"])
+    np.savez_compressed(HERE / "registration.npz", **out)
+
+
 def gen_phantom(ref_root: Path):
     """create_spine_phantom (dicom_loader.py:114-176) at the size the
     reference's engine test uses (64) and at odd and non-power-of-two sizes;
@@ -352,7 +391,8 @@ def main():
             "pou": lambda: gen_pou(cb), "numpy_renderer": lambda: gen_numpy(df, gr),
             "articulated": lambda: gen_articulated(ref_root),
             "ingest_targets": lambda: gen_ingest_and_targets(ref_root),
-            "phantom": lambda: gen_phantom(ref_root)}
+            "phantom": lambda: gen_phantom(ref_root),
+            "registration": lambda: gen_registration(ref_root)}
     for name, gen in gens.items():
         if only is None or name in only:
             gen()

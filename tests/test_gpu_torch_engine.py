@@ -436,3 +436,49 @@ def test_host_io_graph_step_matches_device_step(big):
     lh2, gh2 = io_step(io_step.host_poses)
     ld2, gd2 = dev_step(_t(tc.make_poses(8, 15)))
     assert float(lh2) == float(ld2) and torch.equal(gh2, gd2.cpu())
+
+
+@pytest.mark.parametrize("g", [(1.0, 1.0), (0.5, -2.0)])
+def test_three_kernel_abi_path_matches_fused(big, g):
+    """fvr_tc_sncc_moments (with gradient moments) + fvr_tc_sncc_finalize +
+    fvr_tc_sncc_backward, called through the C ABI, give the losses and the
+    pose gradient of the fused fvr_tc_sncc_value_and_grad for upstream
+    gradients g per view."""
+    import ctypes
+
+    from fvr import _lib as L
+    from fvr import _runtime as RT
+
+    _, eng, _ = big
+    C, R, nv = 8, 128, 2
+    poses = _t(tc.make_poses(C, 9)).contiguous()
+    tp = _t(tc.make_poses(1, 10))
+    fts = [eng.prepare_spectral_target(eng(tp, view=v, out_res=R)).reshape(R, R).contiguous()
+           for v in ("ap", "lateral")]
+    st = eng._stencil
+    views = (ctypes.c_int * nv)(0, 1)
+    fptrs = (ctypes.c_void_p * nv)(*[f.data_ptr() for f in fts])
+    hp, lin = RT.hp_filter(R, R, 4.0, poses.device), RT.linspace(R, poses.device)
+    kap = RT.kappa(R, eng.spacing[0])
+    s = L.stream_ptr(poses.device)
+    gt = _t(np.array(g, np.float32))
+    ws_b = int(L.query("fvr_tc_sncc_workspace", C, R, nv))
+    ws = torch.empty(ws_b, dtype=torch.uint8, device=DEV)
+    mom = torch.empty((nv, C, int(L.query("fvr_tc_sncc_mom_stride"))), dtype=torch.float64, device=DEV)
+    loss3 = torch.empty(nv + 1, dtype=torch.float32, device=DEV)
+    grad3 = torch.empty((C, 6), dtype=torch.float32, device=DEV)
+    L.call("fvr_tc_sncc_moments", *st.args(), L.ptr(poses), C, nv, views, fptrs, L.ptr(hp), L.ptr(lin), R, kap, 1, 0,
+           L.ptr(ws), ws_b, s)
+    L.call("fvr_tc_sncc_finalize", L.ptr(ws), C, R, nv, 1, 0, L.ptr(mom), L.ptr(loss3), None, s)
+    D, H, W = st.dims
+    L.call("fvr_tc_sncc_backward", L.ptr(mom), nv, views, L.ptr(gt), 1, L.ptr(poses), C, D, H, W, kap,
+           L.ptr(grad3), 0, s)
+    fw_b = int(L.query("fvr_tc_sncc_fused_workspace", C, R, nv))
+    fw = torch.zeros(fw_b, dtype=torch.uint8, device=DEV)
+    lossf = torch.empty(nv + 1, dtype=torch.float32, device=DEV)
+    gradf = torch.empty((C, 6), dtype=torch.float32, device=DEV)
+    L.call("fvr_tc_sncc_value_and_grad", *st.args(), L.ptr(poses), C, nv, views, fptrs, L.ptr(hp), L.ptr(lin), R,
+           kap, 0, L.ptr(gt), 1, L.ptr(fw), fw_b, L.ptr(lossf), None, L.ptr(gradf), 0, s)
+    torch.cuda.synchronize()
+    assert torch.allclose(loss3, lossf, rtol=1e-6, atol=1e-7)
+    assert rel_l2(grad3.cpu().numpy(), gradf.cpu().numpy()) < 1e-5
