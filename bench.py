@@ -754,84 +754,86 @@ REG_VOLUMES = ((128, 128, 128), (192, 192, 192), (160, 256, 256))  # (Z, Y, X) v
 REG_INITS = 4
 
 
-def _registration_run(torch, dev, model, lattice, init_seed, iters, n_cand):
-    """One multi-start registration: a seeded ground-truth pose, references
-    rendered there, n_cand candidates around the unperturbed start, iters Adam
-    iterations each one CUDA-graph replay.  Returns (wall ms, best loss, mTRE
-    of the best candidate on a 3x3x3 fiducial grid (mm), its rotation error
-    (deg), the start's mTRE (mm))."""
-    from fvr.registration import MultistartRegistration, sample_multistart_theta, se3_exp
-    from fvr import synthetic
-
-    initA = synthetic.make_pinhole_mats(1, 0, sad_mm=765.0, rot_deg=0.0, trans_mm=0.0, device=dev)
-    ry90 = torch.tensor([[0.0, 0.0, 1.0, 0.0], [0.0, 1.0, 0.0, 0.0], [-1.0, 0.0, 0.0, 0.0], [0.0, 0.0, 0.0, 1.0]],
-                        device=dev)
-    initB = ry90 @ initA
-
-    def render_pair(dT):
-        return model.forward_pinhole(dT @ initA, lattice), model.forward_pinhole(dT @ initB, lattice)
-
-    rng = np.random.default_rng(SEED + 7 + 100 * init_seed)
-    theta_gt = torch.tensor(np.concatenate([np.radians(rng.uniform(-10, 10, 3)), rng.uniform(-12, 12, 3)])[None],
-                            dtype=torch.float32, device=dev)
-    with torch.no_grad():
-        refA, refB = render_pair(se3_exp(theta_gt))
-    theta0 = sample_multistart_theta(n_cand, dev, SEED + 8 + 100 * init_seed)
-    reg = MultistartRegistration(render_pair, refA, refB, theta0, steps=iters, graph=True)
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    reg.run(iters)
-    losses, best = reg.evaluate()
-    b.record()
-    b.synchronize()
-    with torch.no_grad():
-        rel = se3_exp(best) @ torch.linalg.inv(se3_exp(theta_gt))
-        g = torch.linspace(-48.0, 48.0, 3, device=dev)
-        pts = torch.stack(torch.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
-        mtre = float((pts @ rel[0, :3, :3].T + rel[0, :3, 3] - pts).norm(dim=1).mean())
-        rot_err = float(torch.rad2deg(torch.arccos(torch.clamp((torch.trace(rel[0, :3, :3]) - 1) / 2, -1, 1))))
-        inv_gt = torch.linalg.inv(se3_exp(theta_gt))
-        init_mtre = float((pts @ inv_gt[0, :3, :3].T + inv_gt[0, :3, 3] - pts).norm(dim=1).mean())
-    del reg
-    return a.elapsed_time(b), float(losses.min()), mtre, rot_err, init_mtre
-
-
 def _registration_leg(torch, dev, iters=200, n_cand=CANDIDATES):
     """Secondary line: multi-start biplanar registration on three seeded
     ellipsoid volumes (128^3, 192^3, 256 x 256 x 160 at 1 mm), PoU-FVR 4x4x4
     blocks at block_res 64 (P = 128, bf16 spectra), pinhole SDD 1020 / SAD
     765 mm, 256^2 detector at 1.0 mm, AP and lateral views; per volume four
-    seeded ground-truth poses (inits), each registered from 64 candidates with
-    200 Adam iterations replayed as one captured CUDA graph per iteration."""
+    seeded ground-truth poses (inits), each registered from 64 candidates
+    with 200 Adam iterations.  All 12 registrations (768 candidates) advance
+    together: one CUDA-graph replay per Adam iteration renders every volume's
+    candidates in both views, forms the losses against each init's
+    references and takes the Adam step."""
     from fvr import synthetic
     from fvr.cone_beam_fvr import PerspectiveSlabFVR
+    from fvr.registration import MultiVolumeRegistration, sample_multistart_theta, se3_exp
 
     H, f = 256, 1020.0 / 1.0
     k_inv = torch.tensor([[1.0 / f, 0.0, -0.5 * H / f], [0.0, 1.0 / f, -0.5 * H / f], [0.0, 0.0, 1.0]], device=dev)
-    out = {"iterations": iters, "candidates_per_init": n_cand, "inits_per_volume": REG_INITS, "volumes": []}
+    initA = synthetic.make_pinhole_mats(1, 0, sad_mm=765.0, rot_deg=0.0, trans_mm=0.0, device=dev)
+    ry90 = torch.tensor([[0.0, 0.0, 1.0, 0.0], [0.0, 1.0, 0.0, 0.0], [-1.0, 0.0, 0.0, 0.0], [0.0, 0.0, 0.0, 1.0]],
+                        device=dev)
+    initB = ry90 @ initA
+    problems, gts, blocks = [], [], []
     for shape in REG_VOLUMES:
         vol = synthetic.make_ellipsoid_volume(max(shape), SEED, shape=shape)
         model = PerspectiveSlabFVR.from_volume(vol, vox_mm=1.0, grid_blocks=(4, 4, 4), block_res=64, overlap=0.5,
                                                dtype=torch.bfloat16, device=dev)
         lattice = model.make_pinhole_lattice(k_inv, 1020.0, H, H)
-        runs = [_registration_run(torch, dev, model, lattice, i, iters, n_cand) for i in range(REG_INITS)]
-        ms = [r[0] for r in runs]
-        out["volumes"].append({
-            "shape_zyx": list(shape), "blocks": int(model.B), "wall_ms_per_init": ms,
-            "ms_per_iteration": statistics.mean(ms) / iters, "best_loss": [r[1] for r in runs],
-            "mtre_mm": [r[2] for r in runs], "rot_err_deg": [r[3] for r in runs],
-            "init_mtre_mm": [r[4] for r in runs]})
-        del model, lattice
-        torch.cuda.empty_cache()
-    out["wall_ms_total"] = sum(sum(v["wall_ms_per_init"]) for v in out["volumes"])
+        refsA, refsB, thetas, vgt = [], [], [], []
+        for i in range(REG_INITS):
+            rng = np.random.default_rng(SEED + 7 + 100 * i)
+            theta_gt = torch.tensor(np.concatenate([np.radians(rng.uniform(-10, 10, 3)), rng.uniform(-12, 12, 3)])[None],
+                                    dtype=torch.float32, device=dev)
+            with torch.no_grad():
+                dT = se3_exp(theta_gt)
+                refsA.append(model.forward_pinhole(dT @ initA, lattice))
+                refsB.append(model.forward_pinhole(dT @ initB, lattice))
+            thetas.append(sample_multistart_theta(n_cand, dev, SEED + 8 + 100 * i))
+            vgt.append(theta_gt)
+        problems.append((model, lattice, initA, initB, torch.cat(refsA), torch.cat(refsB), torch.cat(thetas)))
+        gts.append(vgt)
+        blocks.append(int(model.B))
+    reg = MultiVolumeRegistration(problems, steps=iters)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    reg.run(iters)
+    best = reg.evaluate()
+    b.record()
+    b.synchronize()
+    total_ms = a.elapsed_time(b)
+    g = torch.linspace(-48.0, 48.0, 3, device=dev)
+    pts = torch.stack(torch.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+
+    def mtre(T):
+        return float((pts @ T[:3, :3].T + T[:3, 3] - pts).norm(dim=1).mean())
+
+    out = {"iterations": iters, "candidates_per_init": n_cand, "inits_per_volume": REG_INITS,
+           "candidates_total": reg.total, "wall_ms_total": total_ms, "ms_per_iteration": total_ms / iters,
+           "volumes": []}
+    with torch.no_grad():
+        for shape, nb, vgt, vbest in zip(REG_VOLUMES, blocks, gts, best):
+            res = {"shape_zyx": list(shape), "blocks": nb, "best_loss": [], "mtre_mm": [], "rot_err_deg": [],
+                   "init_mtre_mm": []}
+            for theta_gt, (loss, th) in zip(vgt, vbest):
+                rel = se3_exp(th[None]) @ torch.linalg.inv(se3_exp(theta_gt))
+                res["best_loss"].append(loss)
+                res["mtre_mm"].append(mtre(rel[0]))
+                res["rot_err_deg"].append(float(torch.rad2deg(torch.arccos(torch.clamp(
+                    (torch.trace(rel[0, :3, :3]) - 1) / 2, -1, 1)))))
+                res["init_mtre_mm"].append(mtre(torch.linalg.inv(se3_exp(theta_gt))[0]))
+            out["volumes"].append(res)
+    del reg, problems
+    torch.cuda.empty_cache()
     out["workload"] = ("multi-start biplanar registration: seeded ellipsoid volumes 128^3, 192^3, 256x256x160 "
                        "(Z 160), PoU-FVR 4x4x4 blocks @ block_res 64 (bf16), SDD 1020 / SAD 765 mm, 256^2 at "
                        "1.0 mm, AP + lateral; 4 seeded ground-truth poses per volume (rot U(+-10 deg), trans "
                        "U(+-12 mm)), each from 64 candidates (rot U(+-12 deg), trans U(+-15 mm)), 200 Adam "
-                       "iterations, each one CUDA-graph replay (render, 0.75 edge NCC + 0.25 NCC loss, adjoint, "
-                       "Adam); mTRE of the best candidate on a 3x3x3 fiducial grid (+-48 mm)")
-    out["timing"] = "CUDA events around each init's 200 replays and its final evaluation"
+                       "iterations for all 12 registrations at once, each iteration one CUDA-graph replay "
+                       "(render every volume's candidates in both views, 0.75 edge NCC + 0.25 NCC loss, adjoint, "
+                       "Adam); mTRE of each init's best candidate on a 3x3x3 fiducial grid (+-48 mm)")
+    out["timing"] = "CUDA events around the 200 replays and the final evaluation of all 12 registrations"
     return out
 
 

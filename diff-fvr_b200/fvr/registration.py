@@ -166,3 +166,65 @@ class MultistartRegistration:
         losses = biplanar_loss_per_candidate(imA, imB, self.refA, self.refB)
         best = int(torch.argmin(losses))
         return losses, self.theta[best:best + 1].clone()
+
+
+class MultiVolumeRegistration:
+    """Every volume's multi-start registrations advanced together, one CUDA-graph
+    replay per Adam iteration for all of them.
+
+    ``problems`` lists, per volume, ``(model, lattice, initA, initB, refA, refB,
+    theta0)``: a :class:`fvr.cone_beam_fvr.PerspectiveSlabFVR`, its pinhole
+    lattice, the two views' base camera matrices ([1, 4, 4]), the reference
+    images of each of that volume's initialisations ([I, 1, H, W] per view)
+    and the starting candidates ([I * C, 6], C per initialisation, grouped by
+    initialisation).  One iteration renders each volume's candidates in both
+    views with one ``forward_pinhole`` call (views stacked along the pose
+    axis), forms every candidate's loss against its own initialisation's
+    references and takes the Adam step for all candidates of all volumes
+    (the loop of exp30_gpu_multistart_registration.py:140-183, run over the
+    uneven volumes and their initialisations at once instead of one after
+    another)."""
+
+    def __init__(self, problems, steps: int, **adam):
+        self._vols = []
+        thetas, refsA, refsB = [], [], []
+        start = 0
+        for model, lattice, initA, initB, refA, refB, theta0 in problems:
+            n_init = int(refA.shape[0])
+            n = int(theta0.shape[0])
+            if n % n_init:
+                raise ValueError("theta0 must hold the same number of candidates for every initialisation")
+            per = n // n_init
+            self._vols.append((model, lattice, initA, initB, slice(start, start + n), n_init, per))
+            start += n
+            thetas.append(theta0)
+            refsA.append(refA.repeat_interleave(per, dim=0))
+            refsB.append(refB.repeat_interleave(per, dim=0))
+        self.total = start
+        self.reg = MultistartRegistration(self._render_all, torch.cat(refsA).contiguous(),
+                                          torch.cat(refsB).contiguous(), torch.cat(thetas), steps, **adam)
+
+    def _render_all(self, dT):
+        outA, outB = [], []
+        for model, lattice, initA, initB, sl, _, _ in self._vols:
+            d = dT[sl]
+            n = int(d.shape[0])
+            img = model.forward_pinhole(torch.cat([d @ initA, d @ initB]), lattice)
+            outA.append(img[:n])
+            outB.append(img[n:])
+        return torch.cat(outA), torch.cat(outB)
+
+    def run(self, steps: int) -> None:
+        self.reg.run(steps)
+
+    @torch.no_grad()
+    def evaluate(self):
+        """Per volume and initialisation: (best loss, best theta [6]) over its candidates."""
+        losses, _ = self.reg.evaluate()
+        out = []
+        for _, _, _, _, sl, n_init, per in self._vols:
+            lv = losses[sl].view(n_init, per)
+            tv = self.reg.theta[sl].view(n_init, per, 6)
+            best = torch.argmin(lv, dim=1)
+            out.append([(float(lv[i, best[i]]), tv[i, best[i]].clone()) for i in range(n_init)])
+        return out

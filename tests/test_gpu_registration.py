@@ -98,3 +98,52 @@ def test_registration_descends_towards_ground_truth():
     err_t = float((best[0, 3:] - theta_gt[0, 3:]).norm())
     err0 = float((theta0[:, 3:] - theta_gt[:, 3:]).norm(dim=1).min())
     assert err_t < err0
+
+
+def test_multi_volume_registration_equals_separate_runs():
+    """Two volumes of different size and block count, two initialisations
+    each: MultiVolumeRegistration (one graph replay per iteration for all of
+    them) gives every candidate the Adam trajectory that a separate
+    MultistartRegistration of its own (volume, initialisation) gives it."""
+    from fvr import synthetic
+    from fvr.cone_beam_fvr import PerspectiveSlabFVR
+    from fvr.registration import MultistartRegistration, MultiVolumeRegistration, sample_multistart_theta, se3_exp
+
+    H, sdd = 48, 600.0
+    f = sdd / 2.0
+    k_inv = torch.tensor([[1.0 / f, 0.0, -0.5 * H / f], [0.0, 1.0 / f, -0.5 * H / f], [0.0, 0.0, 1.0]], device=DEV)
+    initA = synthetic.make_pinhole_mats(1, 0, sad_mm=400.0, rot_deg=0.0, trans_mm=0.0, device=DEV)
+    Ry90 = torch.tensor([[0.0, 0.0, 1.0, 0.0], [0.0, 1.0, 0.0, 0.0], [-1.0, 0.0, 0.0, 0.0], [0.0, 0.0, 0.0, 1.0]],
+                        device=DEV)
+    initB = Ry90 @ initA
+    problems, separate = [], []
+    for vi, shape in enumerate(((40, 40, 40), (32, 48, 40))):
+        vol = synthetic.make_ellipsoid_volume(max(shape), 11 + vi, shape=shape)
+        m = PerspectiveSlabFVR.from_volume(vol, vox_mm=2.0, grid_blocks=(2, 2, 2), block_res=32, overlap=0.5)
+        lat = m.make_pinhole_lattice(k_inv, sdd, H, H)
+        refsA, refsB, thetas = [], [], []
+        for ii in range(2):
+            gt = torch.tensor([[0.03 * (ii + 1), -0.02, 0.01 * vi, 2.0 - ii, -1.0, 1.5 * vi]], device=DEV)
+            with torch.no_grad():
+                dT = se3_exp(gt)
+                rA, rB = m.forward_pinhole(dT @ initA, lat), m.forward_pinhole(dT @ initB, lat)
+            th0 = sample_multistart_theta(6, DEV, 20 + 3 * vi + ii, rot_deg_lim=5.0, trans_mm_lim=5.0)
+            refsA.append(rA)
+            refsB.append(rB)
+            thetas.append(th0)
+
+            def render_pair(d, m=m, lat=lat):
+                return m.forward_pinhole(d @ initA, lat), m.forward_pinhole(d @ initB, lat)
+
+            separate.append(MultistartRegistration(render_pair, rA, rB, th0, steps=10, graph=True))
+        problems.append((m, lat, initA, initB, torch.cat(refsA), torch.cat(refsB), torch.cat(thetas)))
+    multi = MultiVolumeRegistration(problems, steps=10)
+    multi.run(5)
+    for r in separate:
+        r.run(5)
+    torch.cuda.synchronize()
+    got = multi.reg.theta.view(4, 6, 6)
+    for k, r in enumerate(separate):
+        assert torch.allclose(got[k], r.theta, atol=2e-5, rtol=1e-4), k
+    best = multi.evaluate()
+    assert len(best) == 2 and all(len(v) == 2 for v in best)
