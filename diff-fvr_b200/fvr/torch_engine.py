@@ -82,6 +82,84 @@ def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
 _FUSED_VARIANTS = (0, 3, 6, 7)
 
 
+class _FusedCall:
+    """A prepared launch of fvr_tc_sncc_value_and_grad: every argument except
+    the poses, the two outputs and the stream converted to its C type once
+    (engine storage, shape, views, target spectra, high-pass table, chosen
+    launch variant, cached workspace), so a call costs one foreign call."""
+
+    __slots__ = ("fn", "head", "mid", "keep")
+
+    def launch(self, p, loss, grad, stream):
+        L.launch_count[0] += 2
+        rc = self.fn(*self.head, _ct_ptr(p), *self.mid, _ct_ptr(loss), None, _ct_ptr(grad), 0, stream)
+        if rc != 0:
+            raise L.FvrError(f"fvr_tc_sncc_value_and_grad failed with status {rc}: "
+                             f"{L.load().fvr_status_string(rc).decode()}")
+
+
+def _ct_ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _fused_call(eng, C, R, views, ftargs, hp, p):
+    """The prepared launch for this engine storage and call shape, built (and
+    the launch variant autotuned on the poses ``p``) on first use.  Target spectra already in
+    complex64 on the engine's device are used in place and the preparation
+    is cached by their addresses; others are converted for this call only."""
+    dev = eng._dev
+    st = eng._stencil
+    nv = len(views)
+    direct = all(f.is_cuda and f.device == dev and f.dtype == torch.complex64 and f.is_contiguous() for f in ftargs)
+    key = (C, R, tuple(views), tuple(int(f.data_ptr()) for f in ftargs), 0 if hp is None else int(hp.data_ptr()),
+           id(st))
+    hit = eng._fused_calls.get(key) if direct else None
+    if hit is not None:
+        return hit
+    ws_bytes = int(L.query("fvr_tc_sncc_fused_workspace", C, R, nv))
+    wkey = (C, R, nv, dev)
+    ws = eng._fused_ws.get(wkey)
+    if ws is None:
+        ws = torch.zeros(ws_bytes, dtype=torch.uint8, device=dev)  # zeroed once: the record flags start clear
+        eng._fused_ws[wkey] = ws
+    fts = [f.detach().to(device=dev, dtype=torch.complex64).contiguous() for f in ftargs]
+    for f in fts:
+        if f.numel() != R * R:
+            raise L.FvrError(f"target spectrum has {f.numel()} elements, expected {R}x{R}")
+    vcodes = (ctypes.c_int * nv)(*views)
+    fptrs = (ctypes.c_void_p * nv)(*[f.data_ptr() for f in fts])
+    lin = RT.linspace(R, dev)
+    call = _FusedCall()
+    call.fn = getattr(L.load(), "fvr_tc_sncc_value_and_grad")
+    call.head = st.args()
+    call.keep = (st, fts, hp, lin, ws, vcodes, fptrs)
+
+    def mid(variant):
+        return (ctypes.c_int64(C), ctypes.c_int(nv), vcodes, fptrs, L.ptr(hp), L.ptr(lin), ctypes.c_int64(R),
+                ctypes.c_double(RT.kappa(R, eng.spacing[0])), ctypes.c_int(int(variant)), None, ctypes.c_int64(0),
+                L.ptr(ws), ctypes.c_int64(ws_bytes))
+
+    def run(variant):
+        call.mid = mid(variant)
+        loss = torch.empty(nv + 1, dtype=torch.float32, device=dev)
+        grad = torch.empty((C, 6), dtype=torch.float32, device=dev)
+        call.launch(p, loss, grad, L.stream_ptr(dev))
+
+    variant = autotune.choose("sncc_fused", (st.code, C, R, nv, st.dims), run, L.load().fvr_tc_sncc_variants(),
+                              candidates=_FUSED_VARIANTS)
+    call.mid = mid(variant)
+    if direct:
+        if len(eng._fused_calls) > 64:
+            eng._fused_calls.clear()
+        eng._fused_calls[key] = call
+    return call
+
+
+def _current_stream(dev):
+    getter = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+    return ctypes.c_void_p(getter(dev.index)) if getter is not None else L.stream_ptr(dev)
+
+
 def _sncc_fused(eng, p, views, ftargs, hp, R, out=None, loss_out=None):
     """Moments kernel + its dependent epilogue: per-candidate finalize and pose
     gradient, view losses.  Returns (loss [nv + 1] f32, grad [C, 6] f32).  The
@@ -90,38 +168,17 @@ def _sncc_fused(eng, p, views, ftargs, hp, R, out=None, loss_out=None):
     dev = eng._dev
     C = int(p.shape[0])
     nv = len(views)
-    st = eng._stencil
-    ws_bytes = int(L.query("fvr_tc_sncc_fused_workspace", C, R, nv))
-    key = (C, R, nv, dev)
-    ws = eng._fused_ws.get(key)
-    if ws is None:
-        ws = torch.zeros(ws_bytes, dtype=torch.uint8, device=dev)
-        eng._fused_ws[key] = ws
+    call = _fused_call(eng, C, int(R), tuple(views), ftargs, hp, p)
     loss = torch.empty(nv + 1, dtype=torch.float32, device=dev) if loss_out is None else loss_out
     grad = torch.empty((C, 6), dtype=torch.float32, device=dev) if out is None else out
-    for t, shape in ((loss, (nv + 1,)), (grad, (C, 6))):
-        if tuple(t.shape) != shape or t.dtype != torch.float32 or not t.is_contiguous():
-            raise L.FvrError(f"output buffer must be a contiguous float32 tensor of shape {shape}")
-        if not (t.is_cuda or t.is_pinned()):
-            raise L.FvrError("output buffers must be device memory or pinned host memory")
-    fts = [f.detach().to(device=dev, dtype=torch.complex64).contiguous() for f in ftargs]
-    for f in fts:
-        if f.numel() != R * R:
-            raise L.FvrError(f"target spectrum has {f.numel()} elements, expected {R}x{R}")
-    vcodes = (ctypes.c_int * nv)(*views)
-    fptrs = (ctypes.c_void_p * nv)(*[f.data_ptr() for f in fts])
-    kap = RT.kappa(R, eng.spacing[0])
-    s = L.stream_ptr(dev)
-    lin = RT.linspace(R, dev)
-
-    def run(variant):
-        L.call("fvr_tc_sncc_value_and_grad", *st.args(), L.ptr(p), C, nv, vcodes, fptrs, L.ptr(hp), L.ptr(lin), R, kap,
-               int(variant), None, 0, L.ptr(ws), ws_bytes, L.ptr(loss), None, L.ptr(grad), 0, s)
-
-    variant = autotune.choose("sncc_fused", (st.code, C, R, nv, st.dims), run, L.load().fvr_tc_sncc_variants(),
-                              candidates=_FUSED_VARIANTS)
+    if out is not None or loss_out is not None:
+        for t, shape in ((loss, (nv + 1,)), (grad, (C, 6))):
+            if tuple(t.shape) != shape or t.dtype != torch.float32 or not t.is_contiguous():
+                raise L.FvrError(f"output buffer must be a contiguous float32 tensor of shape {shape}")
+            if not (t.is_cuda or t.is_pinned()):
+                raise L.FvrError("output buffers must be device memory or pinned host memory")
     with profiling.section("tc_sncc_moments"):
-        run(variant)
+        call.launch(p, loss, grad, _current_stream(dev))
     return loss, grad
 
 
@@ -320,6 +377,7 @@ class TorchDiffFVREngine(nn.Module):
         self.register_buffer("f_vol_5d", planar.to(dtype=dtype))
         self._stencil = RT.Stencil(self.f_vol_5d[0], True, self.pad_shape, self._stencil_dtype(dtype))
         self._fused_ws = {}  # (C, R, views, device) -> workspace of the fused value_and_grad
+        self._fused_calls = {}  # prepared launches of the fused value_and_grad
 
     @staticmethod
     def _stencil_dtype(dtype):
