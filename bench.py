@@ -428,6 +428,47 @@ def _pou_roofline(B, P, K, entry, pose_evals_per_s):
             "fallback 6.65 TB/s", "timing": "whole step (all kernels, eager autograd)"}
 
 
+_POU_SECTIONS = ("pou_slice", "pou_warp", "pou_warp_bwd", "pou_slice_adjoint")
+
+
+def _pou_kernel_times(torch, step, steps, flush):
+    """Mean CUDA-event time (ms) of each PoU kernel section over ``steps``
+    eager steps (events recorded on the launching stream around each kernel)."""
+    from fvr import profiling
+
+    timer = profiling.LaunchTimer(_POU_SECTIONS, capacity=4 * len(_POU_SECTIONS))
+    acc = {k: [] for k in _POU_SECTIONS}
+    for _ in range(steps):
+        flush.add_(1)
+        with timer:
+            step()
+        torch.cuda.synchronize()
+        for k in _POU_SECTIONS:
+            acc[k].extend(timer.durations_ms(k))
+    return {k: statistics.mean(v) for k, v in acc.items() if v}
+
+
+def _pou_kernel_rooflines(kern_ms, B, N, P, entry):
+    """Per-kernel HBM rooflines of the PoU step: algorithmic bytes per launch
+    over the kernel's event time.  Block-image kernels: every (block, pose)
+    slice sample reads one stencil entry (``entry`` bytes) and writes (forward)
+    or reads (adjoint) one float of the block image.  The warp kernels are
+    bound by issued instructions, not bytes: their times are listed only."""
+    peak, peak_kind = _peak_hbm()
+    samples = B * N * P * P
+    out = {"peak": peak, "unit": "GB/s", "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"
+           if peak_kind == "measured" else "fallback 6.65 TB/s"}
+    for name in ("pou_slice", "pou_slice_adjoint"):
+        if name in kern_ms:
+            alg = samples * (entry + 4)
+            ach = alg / (kern_ms[name] * 1e-3) / 1e9
+            out[name] = {"ms": kern_ms[name], "alg_bytes_per_launch": alg, "achieved": ach, "frac": ach / peak}
+    for name in ("pou_warp", "pou_warp_bwd"):
+        if name in kern_ms:
+            out[name] = {"ms": kern_ms[name], "bound": "issue (instructions), see profiles"}
+    return out
+
+
 def _pou_leg(torch, dev, flush, warmup, steps):
     """Secondary line: the PoU-FVR cone-beam step (192^3 ellipsoid volume, 4x4x4
     blocks at 50 % overlap, block_res 64 -> P = 128; pinhole SDD 1020 / SAD 765
@@ -456,8 +497,11 @@ def _pou_leg(torch, dev, flush, warmup, steps):
         t, _ = _time_steps(torch, step, steps, flush)
         ms = statistics.mean(t)
         value = CANDIDATES / (ms / 1e3)
+        kern = _pou_kernel_times(torch, step, steps, flush)
+        entry = 64 if name == "f32" else 32
         out[name] = {"value": value, "ms_per_step": ms, "blocks": int(m.B), "P": int(m.P),
-                     "roofline": _pou_roofline(int(m.B), int(m.P), 256 * 256, 64 if name == "f32" else 32, value)}
+                     "roofline": _pou_roofline(int(m.B), int(m.P), 256 * 256, entry, value),
+                     "kernels": _pou_kernel_rooflines(kern, int(m.B), CANDIDATES, int(m.P), entry)}
         del m, lattice
         torch.cuda.empty_cache()
     out["unit"] = UNIT

@@ -199,8 +199,9 @@ def _block_images_adjoint(model, geo, N, grad_imgs, s):
     if L.query("fvr_pou_image_supported", P):
         wsb = L.query("fvr_pou_slice_image_adjoint_workspace", B, N)
         ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
-        L.call("fvr_pou_slice_image_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
-               L.ptr(model._freqs), L.ptr(grad_imgs), L.ptr(ws), wsb, s)
+        with profiling.section("pou_slice_adjoint"):
+            L.call("fvr_pou_slice_image_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
+                   L.ptr(model._freqs), L.ptr(grad_imgs), L.ptr(ws), wsb, s)
         return ws, 1
     # adjoint of S -> Re fftshift(ifft2(ifftshift(S))): fftshift(fft2(ifftshift(g))) / P^2
     G = RT.fft2d(grad_imgs, inverse=False, in_shift=RT.SHIFT_IFFT, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P))
@@ -252,9 +253,11 @@ class _PinholeFn(torch.autograd.Function):
         goffs = torch.empty((3, B, N), dtype=torch.float64, device=dev)
         wsb = L.query("fvr_pou_warp_bwd_workspace", B, N, H * W)
         ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
-        L.call("fvr_pou_warp_bwd", L.ptr(imgs), B, N, P, L.ptr(offs), _ct.c_void_p(offs.data_ptr() + 8),
-               _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), H * W, 0,
-               1.0 / model.ds_block, float(P // 2), L.ptr(g), L.ptr(grad_imgs), L.ptr(goffs), None, L.ptr(ws), wsb, s)
+        with profiling.section("pou_warp_bwd"):
+            L.call("fvr_pou_warp_bwd", L.ptr(imgs), B, N, P, L.ptr(offs), _ct.c_void_p(offs.data_ptr() + 8),
+                   _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), H * W, 0,
+                   1.0 / model.ds_block, float(P // 2), L.ptr(g), L.ptr(grad_imgs), L.ptr(goffs), None, L.ptr(ws),
+                   wsb, s)
         ws2, tiles = _block_images_adjoint(model, geo, N, grad_imgs, s)
         del grad_imgs
         gm = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
