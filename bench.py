@@ -824,6 +824,12 @@ def _registration_leg(torch, dev, iters=200, n_cand=CANDIDATES):
         model = PerspectiveSlabFVR.from_volume(vol, vox_mm=1.0, grid_blocks=(4, 4, 4), block_res=64, overlap=0.5,
                                                dtype=torch.bfloat16, device=dev)
         lattice = model.make_pinhole_lattice(k_inv, 1020.0, H, H)
+        # references: rendered from f32 spectra (not the bf16 ones being registered) with seeded
+        # Gaussian noise of 2 % of each image's maximum added
+        ref_model = PerspectiveSlabFVR.from_volume(vol, vox_mm=1.0, grid_blocks=(4, 4, 4), block_res=64,
+                                                   overlap=0.5, dtype=torch.float32, device=dev)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(SEED + 9)
         refsA, refsB, thetas, vgt = [], [], [], []
         for i in range(REG_INITS):
             rng = np.random.default_rng(SEED + 7 + 100 * i)
@@ -831,10 +837,12 @@ def _registration_leg(torch, dev, iters=200, n_cand=CANDIDATES):
                                     dtype=torch.float32, device=dev)
             with torch.no_grad():
                 dT = se3_exp(theta_gt)
-                refsA.append(model.forward_pinhole(dT @ initA, lattice))
-                refsB.append(model.forward_pinhole(dT @ initB, lattice))
+                for refs, init in ((refsA, initA), (refsB, initB)):
+                    img = ref_model.forward_pinhole(dT @ init, lattice)
+                    refs.append(img + 0.02 * img.amax() * torch.randn(img.shape, generator=gen, device=dev))
             thetas.append(sample_multistart_theta(n_cand, dev, SEED + 8 + 100 * i))
             vgt.append(theta_gt)
+        del ref_model
         problems.append((model, lattice, initA, initB, torch.cat(refsA), torch.cat(refsB), torch.cat(thetas)))
         gts.append(vgt)
         blocks.append(int(model.B))
@@ -873,7 +881,8 @@ def _registration_leg(torch, dev, iters=200, n_cand=CANDIDATES):
     out["workload"] = ("multi-start biplanar registration: seeded ellipsoid volumes 128^3, 192^3, 256x256x160 "
                        "(Z 160), PoU-FVR 4x4x4 blocks @ block_res 64 (bf16), SDD 1020 / SAD 765 mm, 256^2 at "
                        "1.0 mm, AP + lateral; 4 seeded ground-truth poses per volume (rot U(+-10 deg), trans "
-                       "U(+-12 mm)), each from 64 candidates (rot U(+-12 deg), trans U(+-15 mm)), 200 Adam "
+                       "U(+-12 mm)) whose references are rendered from f32 spectra with 2% Gaussian noise, each "
+                       "from 64 candidates (rot U(+-12 deg), trans U(+-15 mm)), 200 Adam "
                        "iterations for all 12 registrations at once, each iteration one CUDA-graph replay "
                        "(render every volume's candidates in both views, 0.75 edge NCC + 0.25 NCC loss, adjoint, "
                        "Adam); mTRE of each init's best candidate on a 3x3x3 fiducial grid (+-48 mm)")
