@@ -489,12 +489,13 @@ __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kerne
 // Half-spectrum block images.  Only the real part of each block image is
 // used, and Re IFFT2(X) is the (real) inverse transform of the Hermitian part
 // X_h[a][b] = (X[a][b] + conj X[-a][-b]) / 2 of the transform input X =
-// ifftshift(S).  X_h is determined by its P/2 + 1 columns b = 0 .. P/2, so a
-// CTA keeps a P x (P/2 + 1) complex array in shared memory (half of the full
-// image): complex inverse FFTs down those columns, then the rows are real
-// transforms of Hermitian row spectra, done two at a time (row y1 + i row y2
-// through one complex FFT: the real part is y1's image row, the imaginary
-// part y2's).  The adjoint mirrors it: the FFT of the real image gradient is
+// ifftshift(S).  X_h is determined by half of its rows (or columns), so a
+// CTA keeps about half of the full complex image in shared memory.  Forward:
+// complex inverse FFTs along the P/2 + 1 half rows, then the image columns
+// are real transforms of Hermitian column spectra, done two at a time
+// (column x1 + i column x2 through one complex FFT: the real part is x1's
+// image column, the imaginary part x2's).  The adjoint mirrors it with the
+// halves swapped: the FFT of the real image gradient is
 // Hermitian, so two real rows share one complex FFT (separated as
 // (Z[k] + conj Z[-k]) / 2 and (Z[k] - conj Z[-k]) / 2i), half the columns are
 // transformed, and the other half of G is read as conj G[-a][-b].  Every
@@ -529,35 +530,51 @@ __device__ __forceinline__ void pou_tab_gather(const Stencil& st, const AxisTabl
   tab_load<DT>(st, cell, raw);
 }
 
+// Forward layout: the P/2 + 1 half rows of the row-transformed spectrum,
+// pitch P + 1 (odd, so a warp reading one column hits distinct 64-bit banks),
+// then the tables.  After the column pass each column's slots hold that
+// column of the real image: float ((y >> 1) * pitch + c) * 2 + (y & 1).
+__host__ __device__ constexpr int64_t pou_c2r_smem(int P) {
+  return static_cast<int64_t>(pou_half_cols(P)) * (P + 1) * 8 + 40 * 2 * static_cast<int64_t>(P) + 32;
+}
+
+// The rows are gathered along the slice's u axis (lanes on consecutive slice
+// columns, so a warp's stencil reads fall on neighbouring entries), the half
+// rows ka = 0 .. P/2 of X_h are inverse-transformed along the row, then each
+// warp takes two image columns at a time: its columns of every half row
+// (the other half read as conj Y[-ka]), one inverse FFT along the column,
+// real part -> column x1, imaginary part -> column x2, written back into
+// the two columns' own slots (only this warp ever reads them).
 template <int DT, int M>
 __global__ void __launch_bounds__(kPouHalfThreads, 2) pou_slice_c2r_kernel(PouSliceArgs a, float* __restrict__ imgs) {
-  constexpr int P = 32 * M, H = P / 2, NC = pou_half_cols(P), PITCH = NC, NW = kPouHalfThreads / 32;
+  constexpr int P = 32 * M, H = P / 2, NR = pou_half_cols(P), PITCH = P + 1, NW = kPouHalfThreads / 32;
+  constexpr int TAB = ((NR * PITCH * 8 + 15) / 16) * 16;
   extern __shared__ __align__(16) unsigned char smem[];
   Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem);
-  const AxisTables tab = axis_tables(smem + pou_half_tab_offset<M>(), 2 * P);
+  float* bf = reinterpret_cast<float*>(smem);
+  const AxisTables tab = axis_tables(smem + TAB, 2 * P);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  float* scratch = reinterpret_cast<float*>(smem + pou_half_tab_offset<M>() + 40 * 2 * P) + wid * 2 * P;
   const int n = blockIdx.x, b = blockIdx.y;
   const Stencil st = pou_block_stencil(a, b);
   pou_image_tables(tab, a, a.geo + n * kGeo);
   WarpFft<M, true> fft;
   fft.init(lane);
   __syncthreads();
-  // columns kb = 0 .. H of X_h, each an inverse FFT along the rows
-  for (int kb = wid; kb < NC; kb += NW) {
-    const int j = kb + H < P ? kb + H : kb - H;          // S column of X[., kb]
-    const int jm = H - kb >= 0 ? H - kb : H - kb + P;    // S column of X[., -kb]
+  // half rows ka = 0 .. H of X_h, each an inverse FFT along the row
+  for (int ka = wid; ka < NR; ka += NW) {
+    const int i = ka + H < P ? ka + H : ka - H;        // S row of X[ka, .]
+    const int im = H - ka >= 0 ? H - ka : H - ka + P;  // S row of X[-ka, .]
     Cx<float> x[M];
     {
       Raw<DT> raw[M];
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        const int ka = lane + 32 * m;
-        pou_tab_gather<DT>(st, tab, P, ka + H < P ? ka + H : ka - H, j, raw[m]);
+        const int kb = lane + 32 * m;
+        pou_tab_gather<DT>(st, tab, P, i, kb + H < P ? kb + H : kb - H, raw[m]);
       }
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        const int ka = lane + 32 * m, i = ka + H < P ? ka + H : ka - H;
+        const int kb = lane + 32 * m, j = kb + H < P ? kb + H : kb - H;
         Interp o;
         pou_table_sample<DT, false>(st, raw[m], tab.frac[P + i], tab.frac[j], o);
         x[m] = Cx<float>{0.5f * o.sr, 0.5f * o.si};
@@ -567,12 +584,12 @@ __global__ void __launch_bounds__(kPouHalfThreads, 2) pou_slice_c2r_kernel(PouSl
       Raw<DT> raw[M];
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        const int ka = lane + 32 * m;
-        pou_tab_gather<DT>(st, tab, P, H - ka >= 0 ? H - ka : H - ka + P, jm, raw[m]);
+        const int kb = lane + 32 * m;
+        pou_tab_gather<DT>(st, tab, P, im, H - kb >= 0 ? H - kb : H - kb + P, raw[m]);
       }
 #pragma unroll
       for (int m = 0; m < M; ++m) {
-        const int ka = lane + 32 * m, im = H - ka >= 0 ? H - ka : H - ka + P;
+        const int kb = lane + 32 * m, jm = H - kb >= 0 ? H - kb : H - kb + P;
         Interp o;
         pou_table_sample<DT, false>(st, raw[m], tab.frac[P + im], tab.frac[jm], o);
         x[m].x = fmaf(0.5f, o.sr, x[m].x);
@@ -581,43 +598,40 @@ __global__ void __launch_bounds__(kPouHalfThreads, 2) pou_slice_c2r_kernel(PouSl
     }
     fft.run(x, lane);
 #pragma unroll
-    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + kb] = x[k];
+    for (int k = 0; k < M; ++k) buf[ka * PITCH + lane + 32 * k] = x[k];  // slot of image column k + M brev5(lane)
   }
   __syncthreads();
-  // rows two at a time: row y1 + i row y2 (Hermitian row spectra, the upper
-  // half read as conj of the lower), one inverse FFT, real part -> y1, imaginary -> y2
+  // image columns two at a time (Hermitian column spectra, the upper half
+  // read as conj of the lower)
   const float scale = 1.f / static_cast<float>(P * P);
-  float* out = imgs + (static_cast<int64_t>(b) * a.N + n) * P * P;
   for (int t = wid; t < H; t += NW) {
-    const int y1 = 2 * t, y2 = 2 * t + 1;
-    const Cx<float>* r1 = buf + wfft_pos<M>(y1) * PITCH;
-    const Cx<float>* r2 = buf + wfft_pos<M>(y2) * PITCH;
+    const int c1 = wfft_pos<M>(2 * t), c2 = wfft_pos<M>(2 * t + 1);
     Cx<float> z[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-      const int kc = lane + 32 * m;
-      const bool lo = kc <= H;
-      const int src = lo ? kc : P - kc;
-      const Cx<float> c1 = r1[src], c2 = r2[src];
+      const int ka = lane + 32 * m;
+      const bool lo = ka <= H;
+      const int row = (lo ? ka : P - ka) * PITCH;
+      const Cx<float> v1 = buf[row + c1], v2 = buf[row + c2];
       const float s = lo ? 1.f : -1.f;  // conjugate the mirrored half
-      z[m] = Cx<float>{c1.x - s * c2.y, s * c1.y + c2.x};
+      z[m] = Cx<float>{v1.x - s * v2.y, s * v1.y + v2.x};
     }
     fft.run(z, lane);
 #pragma unroll
     for (int k = 0; k < M; ++k) {
-      const int xi = k + M * brev5(lane);
-      scratch[xi] = z[k].x * scale;
-      scratch[P + xi] = z[k].y * scale;
+      const int y = k + M * brev5(lane);
+      const int e1 = ((y >> 1) * PITCH + c1) * 2 + (y & 1), e2 = ((y >> 1) * PITCH + c2) * 2 + (y & 1);
+      if (fvr_checked(e1, 2LL * NR * PITCH, kSiteHalfImage)) bf[e1] = z[k].x * scale;
+      if (fvr_checked(e2, 2LL * NR * PITCH, kSiteHalfImage)) bf[e2] = z[k].y * scale;
     }
-    __syncwarp();
-    const int oy1 = y1 + H < P ? y1 + H : y1 - H, oy2 = y2 + H < P ? y2 + H : y2 - H;
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int xo = lane + 32 * m, xs = xo + H < P ? xo + H : xo - H;  // fftshift of the row
-      out[oy1 * P + xo] = scratch[xs];
-      out[oy2 * P + xo] = scratch[P + xs];
-    }
-    __syncwarp();
+  }
+  __syncthreads();
+  // fftshift-ordered image rows, coalesced
+  float* out = imgs + (static_cast<int64_t>(b) * a.N + n) * P * P;
+  for (int q = threadIdx.x; q < P * P; q += kPouHalfThreads) {
+    const int yo = q / P, xo = q - yo * P;
+    const int y = yo + H < P ? yo + H : yo - H, x = xo + H < P ? xo + H : xo - H;
+    out[q] = bf[((y >> 1) * PITCH + wfft_pos<M>(x)) * 2 + (y & 1)];
   }
 }
 
@@ -1379,7 +1393,7 @@ static bool pou_half_attr(K kernel, int64_t smem) {
 template <int DT, int M>
 static int pou_image_launch(bool adjoint, const PouSliceArgs& a, int B, const float* gimg, float* imgs,
                             double* part, cudaStream_t s) {
-  const int64_t smem = pou_half_smem(32 * M);
+  const int64_t smem = adjoint ? pou_half_smem(32 * M) : pou_c2r_smem(32 * M);
   dim3 grid(static_cast<unsigned>(a.N), static_cast<unsigned>(B));
   if (adjoint) {
     static const bool attr = pou_half_attr(pou_r2c_slice_adjoint_kernel<DT, M>, smem);

@@ -370,9 +370,12 @@ class TorchDiffFVREngine(nn.Module):
         d, h, w = (int(s) for s in volume.shape)
         self.pad_shape = torch.Size((int(round(d * pad_factor)), int(round(h * pad_factor)),
                                      int(round(w * pad_factor))))
-        vol = volume.to(self._dev).contiguous()
-        spec = RT.spectrum3d(vol, self.pad_shape, 0)  # complex64 [Dp, Hp, Wp]
-        planar = torch.view_as_real(spec).permute(3, 0, 1, 2).unsqueeze(0).contiguous()
+        # the one-time transform runs in fp64 (a 512^3 float32 FFT alone would
+        # carry ~1e-5 of relative error into the images); storage is rounded once
+        vol = volume.to(device=self._dev, dtype=torch.float64).contiguous()
+        spec = RT.spectrum3d(vol, self.pad_shape, 0, prec=L.F64_)  # complex128 [Dp, Hp, Wp]
+        del vol
+        planar = torch.view_as_real(spec).permute(3, 0, 1, 2).unsqueeze(0).to(torch.float32).contiguous()
         del spec
         self.register_buffer("f_vol_5d", planar.to(dtype=dtype))
         self._stencil = RT.Stencil(self.f_vol_5d[0], True, self.pad_shape, self._stencil_dtype(dtype))

@@ -125,4 +125,5 @@ def test_pinhole_cpu_mats_and_lattice(golden):
     out_gpu = model.forward_pinhole(m_gpu, lat_gpu)
     (out_gpu * torch.from_numpy(g["pin_inv_w"]).float().cuda()).sum().backward()
     assert torch.equal(out_cpu.detach(), out_gpu.detach().cpu())
-    assert torch.equal(m_cpu.grad, m_gpu.grad.cpu())
+    # the warp adjoint accumulates with atomics: equal up to the order of float additions
+    assert rel_l2(m_cpu.grad.numpy(), m_gpu.grad.cpu().numpy()) < 1e-5
