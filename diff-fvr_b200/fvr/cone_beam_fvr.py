@@ -475,6 +475,9 @@ class PerspectiveSlabFVR(nn.Module):
     def _forward_from_lattice(self, pose_mats, lattice):
         """Camera-frame lattice moved by pose matrices (cone_beam_fvr.py:670-688)."""
         home = pose_mats.device
+        if pose_mats.shape[0] == 0:  # no poses: an empty batch of images
+            H, W = int(lattice[1].shape[0]), int(lattice[1].shape[1])
+            return torch.zeros((0, 1, H, W), dtype=torch.float32, device=home) + 0.0 * pose_mats.sum()
         if len(lattice) >= 11:
             key, _, (rx, ry, ic), _ = _prepared_lattice(lattice, self._dev)
             mats = pose_mats if home == self._dev else pose_mats.to(self._dev)

@@ -423,7 +423,11 @@ class TorchDiffFVREngine(nn.Module):
         return _SliceFn.apply(self._prep_poses(poses), self, _view_code(view), int(out_res), 0)
 
     def _forward_core(self, poses: torch.Tensor, view: str = "ap", out_res: int = 128) -> torch.Tensor:
-        return _ImageFn.apply(self._prep_poses(poses), self, _view_code(view), int(out_res))
+        p = self._prep_poses(poses)
+        if p.shape[0] == 0:  # an empty batch renders no image (still connected to the poses)
+            R = int(out_res)
+            return torch.zeros((0, 1, R, R), dtype=torch.float32, device=self._dev) + 0.0 * p.sum()
+        return _ImageFn.apply(p, self, _view_code(view), int(out_res))
 
     def forward(self, poses: torch.Tensor, view: str = "ap", out_res: int = 128) -> torch.Tensor:
         """Batched differentiable forward pass returning ``(B, 1, out_res, out_res)``."""
@@ -441,6 +445,8 @@ class TorchDiffFVREngine(nn.Module):
         return f
 
     def _spectral_ncc_core(self, poses, f_targ_precomputed, view="ap", high_pass=True, cutoff_sigma=4.0):
+        if poses.shape[0] == 0:  # 1 - mean over no candidates, as torch's mean of an empty batch
+            return torch.full((), float("nan"), dtype=torch.float32, device=self._dev) + 0.0 * poses.sum().to(self._dev)
         R = int(f_targ_precomputed.shape[-1])
         hp = RT.hp_filter(R, R, cutoff_sigma, self._dev) if high_pass else None
         return _SpectralNCCFn.apply(self._prep_poses(poses), self, (_view_code(view),), hp, R, f_targ_precomputed)

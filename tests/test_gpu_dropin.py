@@ -127,3 +127,27 @@ def test_pinhole_cpu_mats_and_lattice(golden):
     assert torch.equal(out_cpu.detach(), out_gpu.detach().cpu())
     # the warp adjoint accumulates with atomics: equal up to the order of float additions
     assert rel_l2(m_cpu.grad.numpy(), m_gpu.grad.cpu().numpy()) < 1e-5
+
+
+def test_empty_batches_follow_torch_semantics():
+    """No candidate poses: empty image batches, and the spectral NCC of an
+    empty batch is NaN (1 - the mean over nothing, as the reference's torch
+    code gives); gradients flow to the empty pose tensors."""
+    from fvr import TorchDiffFVREngine
+    from fvr.cone_beam_fvr import PerspectiveSlabFVR
+    from fvr.synthetic import make_ellipsoid_volume
+
+    eng = TorchDiffFVREngine(torch.from_numpy(make_ellipsoid_volume(16, 2)))
+    p0 = torch.zeros((0, 6), requires_grad=True)
+    img = eng(p0, view="ap", out_res=16)
+    assert img.shape == (0, 1, 16, 16)
+    ft = eng.prepare_spectral_target(eng(torch.zeros((1, 6)), view="ap", out_res=16))
+    loss = eng.forward_spectral_ncc(p0, ft, view="ap")
+    assert bool(torch.isnan(loss))
+    (img.sum() + 0.0 * loss.nan_to_num()).backward()
+    assert p0.grad is not None and p0.grad.shape == (0, 6)
+    m = PerspectiveSlabFVR.from_volume(make_ellipsoid_volume(32, 3), vox_mm=2.0, grid_blocks=(2, 2, 2), block_res=16)
+    k_inv = torch.tensor([[1 / 300.0, 0.0, -0.05], [0.0, 1 / 300.0, -0.05], [0.0, 0.0, 1.0]])
+    lat = m.make_pinhole_lattice(k_inv, 600.0, 30, 30)
+    out = m.forward_pinhole(torch.zeros((0, 4, 4)), lat)
+    assert out.shape == (0, 1, 30, 30)
