@@ -64,7 +64,6 @@ const char* fvr_status_string(int status) {
     case FVR_ERR_UNSUPPORTED: return "unsupported size (e.g. FFT length with a prime factor above 127)";
     case FVR_ERR_WORKSPACE: return "workspace too small";
     case FVR_ERR_CUDA: return "CUDA launch or driver error";
-    case FVR_ERR_TIMEOUT: return "device-side wait timed out";
     default: return "unknown fvr status";
   }
 }

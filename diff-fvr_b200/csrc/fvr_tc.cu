@@ -142,12 +142,6 @@ struct SnccArgs {
   const float* g;      // dL/dloss_v at g[v * g_stride]; null = all ones
   int g_stride, accumulate;
   double kappa;
-  // value-and-gradient path: record hand-off from the moments CTAs to the
-  // epilogue (null on the other paths)
-  unsigned* flags;       // per partial record: the call number that wrote it
-  unsigned* calls;       // calls completed on this workspace
-  int* status;           // FVR_ERR_TIMEOUT when a record never arrived (null: not reported)
-  long long timeout_ns;  // the epilogue's limit on waiting for one record
 };
 
 // dL/dpose of one candidate from its per-view moment records (record of view v
@@ -273,38 +267,6 @@ __device__ __forceinline__ void sncc_item_axes(const SnccArgs& a, int v, int c, 
 // without such a launch.
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
-// Record hand-off of the value-and-gradient path.  A moments CTA stores its
-// partial record, then (after a CTA barrier and a fence) releases the
-// record's flag with the workspace's current call number; the epilogue
-// acquires each record's flag before reading the record, so it sums the
-// records of CTAs that have finished while later ones still run.  The flags
-// need no clearing between calls: call k waits for the value k, and the
-// epilogue advances the workspace's call counter when it ends.  A wait gives
-// up after the epilogue's time limit (%globaltimer), marks the call timed out
-// and stops waiting.
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-// true once *flag == want; false when the deadline passes first
-__device__ __forceinline__ bool wait_record(const unsigned* flag, unsigned want, unsigned long long deadline) {
-  while (ld_acquire_gpu(flag) != want) {
-    if (global_ns() > deadline) return false;
-    __nanosleep(100);
-  }
-  return true;
-}
-constexpr long long kRecordWaitNs = 1000000000LL;  // one second
 
 // Cell of the sample at (row entry a, column entry b) for the moments
 // kernels: the column table's integer part already carries the +1 entry
@@ -478,12 +440,8 @@ __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(Snc
   const int row_begin = tile * a.tile_rows;
   const int row_end = min(row_begin + a.tile_rows, R);
   const SnccTab tab = sncc_tab(tab_smem, R + a.tile_rows);
-  __shared__ unsigned s_call;
   pdl_launch_dependents();
-  if (threadIdx.x == 0) {
-    sncc_item_axes(a, v, c, ax_s);
-    if (a.flags) s_call = *a.calls + 1;
-  }
+  if (threadIdx.x == 0) sncc_item_axes(a, v, c, ax_s);
   __syncthreads();
   build_sncc_tables(tab, R, row_begin, row_end - row_begin, a.lin, ax_s, a.sx, a.sy, a.sz, a.kpi);
   __syncthreads();
@@ -491,15 +449,7 @@ __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(Snc
 #pragma unroll
   for (int m = 0; m < NM; ++m) acc[m] = make_float2(0.f, 0.f);
   sncc_run<DT, GRAD, GROUP, NM>(a, tab, view_target(a, v), row_begin, row_end, acc);
-  const int64_t rec = (static_cast<int64_t>(v) * a.C + c) * gridDim.x + tile;
-  sncc_store_record<NM>(acc, red, a.partial, rec);
-  if (a.flags) {
-    __syncthreads();  // the record's words are stored
-    if (threadIdx.x == 0) {
-      __threadfence();
-      st_release_gpu(a.flags + rec, s_call);
-    }
-  }
+  sncc_store_record<NM>(acc, red, a.partial, (static_cast<int64_t>(v) * a.C + c) * gridDim.x + tile);
 }
 
 // Value-and-gradient epilogue, launched right after the moments kernel as its
@@ -530,17 +480,6 @@ __global__ void __launch_bounds__(kFinalThreads) tc_sncc_final_kernel(SnccArgs a
   const double s3[3] = {a.sx, a.sy, a.sz};
   double lsum[kMaxViews] = {0.0, 0.0, 0.0, 0.0};
   const int cch = kFinalChunkItems / nv;  // candidates per chunk; chunk item li = v * cn + (c - c0)
-  __shared__ int s_timed_out;
-  const bool handoff = a.flags != nullptr;
-  unsigned call = 0;
-  unsigned long long deadline = 0;
-  bool waiting = true;  // false once a wait has given up
-  if (t == 0) s_timed_out = 0;
-  __syncthreads();
-  if (handoff) {
-    call = *a.calls + 1;
-    deadline = global_ns() + static_cast<unsigned long long>(a.timeout_ns);
-  }
   for (int c0 = 0; c0 < C; c0 += cch) {
     const int cn = min(cch, C - c0), ni = cn * nv;
     if (c0 > 0) __syncthreads();  // the previous chunk is done with the shared arrays
@@ -549,36 +488,23 @@ __global__ void __launch_bounds__(kFinalThreads) tc_sncc_final_kernel(SnccArgs a
       double ax[8];
       slice_axes_jac(a.poses + 6 * c, view_lateral(a, v), a.sx, a.sy, a.sz, ax, s_jac[t]);
     }
-    // without the record hand-off: the moments kernel has completed and its records are visible
-    if (c0 == 0 && !handoff) pdl_wait();
+    if (c0 == 0) pdl_wait();  // the moments kernel has completed and its records are visible
     // record sums: the thread's pairs p = t + k * 512, all their loads in one round
     const double* src[kFinalPairs];
-    const unsigned* flg[kFinalPairs];
 #pragma unroll
     for (int k = 0; k < kFinalPairs; ++k) {
       const int p = t + k * kFinalThreads;
       src[k] = nullptr;
-      flg[k] = nullptr;
       if (p < ni * M_NGRAD) {
         const int li = p / M_NGRAD, m = p - li * M_NGRAD, v = li / cn;
         const int64_t it = static_cast<int64_t>(v) * C + c0 + (li - v * cn);
         src[k] = a.partial + it * tiles * M_NGRAD + m;
-        if (handoff) flg[k] = a.flags + it * tiles;
       }
     }
     double sum[kFinalPairs];
 #pragma unroll
     for (int k = 0; k < kFinalPairs; ++k) sum[k] = 0.0;
     for (int r0 = 0; r0 < tiles; r0 += kFinalRecords) {
-      if (handoff && waiting) {
-#pragma unroll
-        for (int k = 0; k < kFinalPairs; ++k)
-          for (int r = 0; r < kFinalRecords && flg[k] && r0 + r < tiles && waiting; ++r)
-            if (!wait_record(flg[k] + r0 + r, call, deadline)) {
-              waiting = false;
-              atomicOr(&s_timed_out, 1);
-            }
-      }
       double x[kFinalPairs][kFinalRecords];
 #pragma unroll
       for (int k = 0; k < kFinalPairs; ++k)
@@ -657,23 +583,16 @@ __global__ void __launch_bounds__(kFinalThreads) tc_sncc_final_kernel(SnccArgs a
   }
   __syncthreads();
   if (t == 0) {
-    const bool bad = s_timed_out != 0;
     double total = 0.0;
     for (int v = 0; v < nv; ++v) {
       double sv = 0.0;
       for (int k = 0; k < kFinalThreads / 32; ++k) sv += red[v][k];
       const double l = 1.0 - sv / C;
-      a.loss[v] = bad ? __int_as_float(0x7fffffff) : static_cast<float>(l);
+      a.loss[v] = static_cast<float>(l);
       total += l;
     }
-    a.loss[nv] = bad ? __int_as_float(0x7fffffff) : static_cast<float>(total);
-    if (handoff && bad && a.status) *a.status = FVR_ERR_TIMEOUT;
+    a.loss[nv] = static_cast<float>(total);
   }
-  // this grid ends after the moments grid it depends on (a no-op without one);
-  // only then does the call counter advance, so no moments CTA of this call
-  // can still read it
-  pdl_wait();
-  if (t == 0 && handoff) *a.calls = call;
 }
 
 // Launch the epilogue as a programmatic dependent of the kernel before it on
@@ -1099,73 +1018,9 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
 
 // Fused workspace: partial records | moments [nv][C][18]; both written by a
 // call before they are read.
-// Fused workspace: partial records, per-item moment records, then one flag
-// word per partial record, the call counter and the status word.
-static int64_t fused_flags_offset(int64_t C, int64_t R, int64_t nviews) {
-  return fvr_tc_sncc_workspace(C, R, nviews) + nviews * C * kMomStride * (int64_t)sizeof(double);
-}
-static int64_t fused_records(int64_t C, int64_t R, int64_t nviews) { return nviews * C * cdiv64(R * R, kSnccThreads); }
-
 int64_t fvr_tc_sncc_fused_workspace(int64_t C, int64_t R, int64_t nviews) {
   if (C < 1 || R < 1 || nviews < 1) return 0;
-  return fused_flags_offset(C, R, nviews) + (fused_records(C, R, nviews) + 4) * (int64_t)sizeof(unsigned);
-}
-
-// Point the value-and-gradient arguments at a fused workspace.
-static void fused_bind(SnccArgs* a, void* workspace, int64_t C, int64_t R, int nviews, long long timeout_ns) {
-  char* ws = static_cast<char*>(workspace);
-  a->partial = reinterpret_cast<double*>(ws);
-  a->mom = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews));
-  a->flags = reinterpret_cast<unsigned*>(ws + fused_flags_offset(C, R, nviews));
-  a->calls = a->flags + fused_records(C, R, nviews);
-  a->status = reinterpret_cast<int*>(a->calls + 1);
-  a->timeout_ns = timeout_ns;
-}
-
-int fvr_tc_sncc_fused_status(void* workspace, int64_t C, int64_t R, int nviews, int* status, int clear) {
-  if (!workspace || !status || C < 1 || R < 1 || nviews < 1) return FVR_ERR_ARG;
-  SnccArgs a{};
-  fused_bind(&a, workspace, C, R, nviews, 0);
-  if (cudaMemcpy(status, a.status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return FVR_ERR_CUDA;
-  if (clear && cudaMemset(a.status, 0, sizeof(int)) != cudaSuccess) return FVR_ERR_CUDA;
-  return FVR_OK;
-}
-
-int fvr_tc_sncc_finish(const float* poses, int64_t C, int nviews, const int* views, int64_t D, int64_t H, int64_t W,
-                       int64_t R, double kappa, int variant, const float* g, int64_t g_stride, void* workspace,
-                       int64_t ws_bytes, float* loss, float* ncc_out, float* grad_poses, int accumulate,
-                       int64_t timeout_us, void* stream) {
-  if (!poses || !views || !workspace || !loss || !grad_poses || C < 1 || R < 1 || C > 65535) return FVR_ERR_ARG;
-  if (nviews < 1 || nviews > kMaxViews || variant < 0 || variant >= kSnccVariants || timeout_us < 0)
-    return FVR_ERR_ARG;
-  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return FVR_ERR_ARG;
-  if (ws_bytes < fvr_tc_sncc_fused_workspace(C, R, nviews)) return FVR_ERR_WORKSPACE;
-  const SnccPlan plan = sncc_plan(C, R, nviews, variant);
-  SnccArgs a{};
-  a.poses = poses;
-  for (int v = 0; v < nviews; ++v) {
-    if (views[v] != 0 && views[v] != 1) return FVR_ERR_ARG;
-    a.lateral[v] = views[v];
-  }
-  a.R = (int)R;
-  a.C = (int)C;
-  a.nv = nviews;
-  a.tile_rows = plan.tile_rows;
-  a.tiles = plan.tiles;
-  a.kappa = kappa;
-  a.sx = half_extent(W);
-  a.sy = half_extent(H);
-  a.sz = half_extent(D);
-  fused_bind(&a, workspace, C, R, nviews, static_cast<long long>(timeout_us) * 1000LL);
-  a.loss = loss;
-  a.ncc_out = ncc_out;
-  a.grad = grad_poses;
-  a.g = g;
-  a.g_stride = (int)g_stride;
-  a.accumulate = accumulate;
-  tc_sncc_final_kernel<<<1, kFinalThreads, 0, static_cast<cudaStream_t>(stream)>>>(a);
-  FVR_LAUNCH_CHECK();
-  return FVR_OK;
+  return fvr_tc_sncc_workspace(C, R, nviews) + nviews * C * kMomStride * (int64_t)sizeof(double);
 }
 
 int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scales, int64_t D, int64_t H, int64_t W,
@@ -1183,7 +1038,9 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
   if (!workspace || !loss || !grad_poses) return FVR_ERR_ARG;
   if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return FVR_ERR_ARG;
   if (ws_bytes < fvr_tc_sncc_fused_workspace(C, R, nviews)) return FVR_ERR_WORKSPACE;
-  fused_bind(&a, workspace, C, R, nviews, kRecordWaitNs);
+  char* ws = static_cast<char*>(workspace);
+  a.partial = reinterpret_cast<double*>(ws);
+  a.mom = reinterpret_cast<double*>(ws + fvr_tc_sncc_workspace(C, R, nviews));
   a.loss = loss;
   a.ncc_out = ncc_out;
   a.grad = grad_poses;

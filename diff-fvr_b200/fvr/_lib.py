@@ -52,8 +52,6 @@ SIGNATURES = {
     "fvr_tc_sncc_fused_workspace": (I64, [I64, I64, I64]),
     "fvr_tc_sncc_value_and_grad_static": (I32, [I32, P, P, I64, I64, I64, P, I64, I32, P, P, P, P, I64, F64, I32, P,
                                                 I64, P, P, P, I32, P]),
-    "fvr_tc_sncc_finish": (I32, [P, I64, I32, P, I64, I64, I64, I64, F64, I32, P, I64, P, I64, P, P, P, I32, I64, P]),
-    "fvr_tc_sncc_fused_status": (I32, [P, I64, I64, I32, P, I32]),
     "fvr_se3_exp": (I32, [P, I64, P, P]),
     "fvr_se3_exp_backward": (I32, [P, P, I64, P, P]),
     "fvr_edge_ncc_workspace": (I64, [I64, I64, I64, I64, I64]),

@@ -31,8 +31,7 @@ typedef enum {
   FVR_ERR_DTYPE = 2,       /* unsupported storage dtype for this entry      */
   FVR_ERR_UNSUPPORTED = 3, /* e.g. FFT length with a prime factor above 127 */
   FVR_ERR_WORKSPACE = 4,   /* caller workspace smaller than the query says  */
-  FVR_ERR_CUDA = 5,        /* launch or driver error (cudaGetLastError)     */
-  FVR_ERR_TIMEOUT = 6      /* a bounded device-side wait gave up            */
+  FVR_ERR_CUDA = 5         /* launch or driver error (cudaGetLastError)     */
 } fvr_status;
 
 typedef enum { FVR_F32 = 0, FVR_BF16 = 1, FVR_F16 = 2, FVR_F64 = 3 } fvr_dtype;
@@ -158,14 +157,8 @@ int fvr_tc_sncc_backward(const double* mom, int nviews, const int* views, const 
  * (optional) and grad_poses[c][6] (g = dL/dloss_v at g[v * g_stride], NULL =
  * all ones; accumulate != 0 adds), and loss[nviews + 1] as
  * fvr_tc_sncc_finalize does.  `workspace` (>= fvr_tc_sncc_fused_workspace
- * bytes, 256-byte aligned) must be zeroed once before its first use and then
- * left to the library: the moments CTAs hand each partial record to the
- * epilogue through a flag word holding the workspace's call number, so the
- * epilogue sums records while later CTAs still run.  The epilogue waits at
- * most one second for any record; when a wait gives up, the losses are NaN
- * and the workspace's status word reads FVR_ERR_TIMEOUT
- * (fvr_tc_sncc_fused_status).  Calls sharing one workspace must be
- * stream-ordered.  loss, ncc_out and grad_poses may be
+ * bytes, 256-byte aligned) needs no initialisation.  Calls sharing one
+ * workspace must be stream-ordered.  loss, ncc_out and grad_poses may be
  * device memory or page-locked host memory mapped into the device address
  * space (the epilogue kernel writes them directly).
  * Replaces the forward + autograd backward of TorchDiffFVREngine.
@@ -177,22 +170,6 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
                                double kappa, int variant, const float* g, int64_t g_stride, void* workspace,
                                int64_t ws_bytes, float* loss, float* ncc_out, float* grad_poses, int accumulate,
                                void* stream);
-/* The epilogue of fvr_tc_sncc_value_and_grad alone (same arguments, minus
- * those of the gather): sums the partial records that the moments launch of
- * the same (C, R, nviews, variant) handed over in `workspace`, waiting at
- * most timeout_us for each, and writes the same outputs.  Lets a caller put
- * other work between the two launches; with no moments launch before it the
- * first wait runs out, the losses are NaN and the status word reads
- * FVR_ERR_TIMEOUT.  No reference counterpart (the reference's backward is
- * autograd, src/fvr/torch_engine.py:269-307). */
-int fvr_tc_sncc_finish(const float* poses, int64_t C, int nviews, const int* views, int64_t D, int64_t H, int64_t W,
-                       int64_t R, double kappa, int variant, const float* g, int64_t g_stride, void* workspace,
-                       int64_t ws_bytes, float* loss, float* ncc_out, float* grad_poses, int accumulate,
-                       int64_t timeout_us, void* stream);
-/* Status word of a fused workspace (FVR_OK, or FVR_ERR_TIMEOUT after an
- * epilogue wait gave up), copied to *status (host) synchronously; clear != 0
- * resets it.  No reference counterpart. */
-int fvr_tc_sncc_fused_status(void* workspace, int64_t C, int64_t R, int nviews, int* status, int clear);
 /* Allocation-free form of fvr_tc_sncc_value_and_grad (no counterpart in the
  * reference): same arguments and results, but the workspace is a fixed
  * per-device scratch array inside the library (about 352 KB), so the call

@@ -99,7 +99,13 @@ double fvr_oracle_sncc(const double* spec, int D, int H, int W, const double* po
   const double sc[3] = {0.5 * (W > 1 ? W - 1 : 1), 0.5 * (H > 1 ? H - 1 : 1), 0.5 * (D > 1 ? D - 1 : 1)};
   const double kap = -2.0 * M_PI / (R * spacing0 + 1e-6);
   double* lin = (double*)malloc(sizeof(double) * R);
-  for (int i = 0; i < R; ++i) lin[i] = R > 1 ? -1.0 + 2.0 * i / (R - 1) : -1.0;
+  /* the float32 values of torch.linspace(-1, 1, R): a float32 step, each value
+   * rounded once to float32 from the exact start + step i (lower half) or
+   * end - step (R - 1 - i) (upper half) */
+  const float step = R > 1 ? 2.0f / (float)(R - 1) : 0.0f;
+  for (int i = 0; i < R; ++i)
+    lin[i] = R == 1 ? -1.0
+                    : (double)(float)(i < R / 2 ? -1.0 + (double)step * i : 1.0 - (double)step * (R - 1 - i));
   double et = 0;
   for (int q = 0; q < R * R; ++q) et += ftarg[2 * q] * ftarg[2 * q] + ftarg[2 * q + 1] * ftarg[2 * q + 1];
   double nsum = 0;

@@ -127,9 +127,24 @@ def slice_axes(poses, view, pad_shape):
     return R[:, 0, :] * c, R[:, 1, :] * c, c, R
 
 
+def linspace_f32(start, end, n):
+    """The float32 values of ``torch.linspace(start, end, n)``: a float32 step,
+    then each value start + step * i (lower half) or end - step * (n - 1 - i)
+    (upper half) rounded once to float32; returned as float64."""
+    if n == 1:
+        return np.array([float(np.float32(start))])
+    s32, e32 = np.float32(start), np.float32(end)
+    step = np.float64(np.float32((e32 - s32) / np.float32(n - 1)))
+    i = np.arange(n, dtype=np.float64)
+    lo = (np.float64(s32) + step * i).astype(np.float32)
+    hi = (np.float64(e32) - step * (n - 1 - i)).astype(np.float32)
+    return np.where(np.arange(n) < n // 2, lo, hi).astype(np.float64)
+
+
 def freq_grid(out_res):
-    """``ku, kv = meshgrid(linspace(-1,1,R), linspace(-1,1,R), 'ij')`` (torch_engine.py:115-121)."""
-    lin = np.linspace(-1.0, 1.0, out_res)
+    """``ku, kv = meshgrid(linspace(-1,1,R), linspace(-1,1,R), 'ij')`` with the
+    float32 grid values the reference samples at (torch_engine.py:115-121)."""
+    lin = linspace_f32(-1.0, 1.0, out_res)
     ku, kv = np.meshgrid(lin, lin, indexing="ij")
     return ku, kv
 
