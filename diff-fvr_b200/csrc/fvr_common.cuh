@@ -77,7 +77,6 @@ enum : unsigned {
   kSiteWarpGrad,          // PoU warp adjoint image-gradient atomic
   kSiteWarpStrip,         // PoU warp row-strip shared-memory access
   kSiteWarpStripRow,      // PoU warp row-strip image row read
-  kSiteHalfImage,         // PoU half-spectrum image shared-memory access
 };
 
 template <typename T>

@@ -486,258 +486,6 @@ __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kerne
 
 
 // ----------------------------------------------------------------------------
-// Half-spectrum block images.  Only the real part of each block image is
-// used, and Re IFFT2(X) is the (real) inverse transform of the Hermitian part
-// X_h[a][b] = (X[a][b] + conj X[-a][-b]) / 2 of the transform input X =
-// ifftshift(S).  X_h is determined by half of its rows (or columns), so a
-// CTA keeps about half of the full complex image in shared memory.  Forward:
-// complex inverse FFTs along the P/2 + 1 half rows, then the image columns
-// are real transforms of Hermitian column spectra, done two at a time
-// (column x1 + i column x2 through one complex FFT: the real part is x1's
-// image column, the imaginary part x2's).  The adjoint mirrors it with the
-// halves swapped: the FFT of the real image gradient is
-// Hermitian, so two real rows share one complex FFT (separated as
-// (Z[k] + conj Z[-k]) / 2 and (Z[k] - conj Z[-k]) / 2i), half the columns are
-// transformed, and the other half of G is read as conj G[-a][-b].  Every
-// slice sample is still gathered (X_h needs both S(k) and S(-k); the
-// zero-padded interpolation is not exactly Hermitian near the edges).  Half
-// the shared memory lets two CTAs share an SM, one gathering while the other
-// transforms.
-// ----------------------------------------------------------------------------
-constexpr int kPouHalfThreads = 256;
-
-__host__ __device__ constexpr int pou_half_cols(int P) { return P / 2 + 1; }
-
-// Half image (P x (P/2 + 1) complex, pitch P/2 + 1: odd, so a warp's column
-// accesses fall in distinct 64-bit banks), the 2P-entry tables, and one
-// P-complex scratch row per warp.
-__host__ __device__ constexpr int64_t pou_half_smem(int P) {
-  return static_cast<int64_t>(P) * pou_half_cols(P) * 8 + 40 * 2 * static_cast<int64_t>(P) +
-         static_cast<int64_t>(kPouHalfThreads / 32) * P * 8 + 32;
-}
-
-template <int M>
-__device__ __forceinline__ int pou_half_tab_offset() {
-  constexpr int P = 32 * M;
-  return ((P * pou_half_cols(P) * 8 + 15) / 16) * 16;
-}
-
-// One slice sample (row entry P + i, column entry j) of block stencil st.
-template <int DT>
-__device__ __forceinline__ void pou_tab_gather(const Stencil& st, const AxisTables& tab, int P, int i, int j,
-                                               Raw<DT>& raw) {
-  const TabCell cell = tab_cell(st, tab.idx[P + i], tab.frac[P + i], tab.idx[j], tab.frac[j]);
-  tab_load<DT>(st, cell, raw);
-}
-
-// Forward layout: the P/2 + 1 half rows of the row-transformed spectrum,
-// pitch P + 1 (odd, so a warp reading one column hits distinct 64-bit banks),
-// then the tables.  After the column pass each column's slots hold that
-// column of the real image: float ((y >> 1) * pitch + c) * 2 + (y & 1).
-__host__ __device__ constexpr int64_t pou_c2r_smem(int P) {
-  return static_cast<int64_t>(pou_half_cols(P)) * (P + 1) * 8 + 40 * 2 * static_cast<int64_t>(P) + 32;
-}
-
-// The rows are gathered along the slice's u axis (lanes on consecutive slice
-// columns, so a warp's stencil reads fall on neighbouring entries), the half
-// rows ka = 0 .. P/2 of X_h are inverse-transformed along the row, then each
-// warp takes two image columns at a time: its columns of every half row
-// (the other half read as conj Y[-ka]), one inverse FFT along the column,
-// real part -> column x1, imaginary part -> column x2, written back into
-// the two columns' own slots (only this warp ever reads them).
-template <int DT, int M>
-__global__ void __launch_bounds__(kPouHalfThreads, 2) pou_slice_c2r_kernel(PouSliceArgs a, float* __restrict__ imgs) {
-  constexpr int P = 32 * M, H = P / 2, NR = pou_half_cols(P), PITCH = P + 1, NW = kPouHalfThreads / 32;
-  constexpr int TAB = ((NR * PITCH * 8 + 15) / 16) * 16;
-  extern __shared__ __align__(16) unsigned char smem[];
-  Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem);
-  float* bf = reinterpret_cast<float*>(smem);
-  const AxisTables tab = axis_tables(smem + TAB, 2 * P);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int n = blockIdx.x, b = blockIdx.y;
-  const Stencil st = pou_block_stencil(a, b);
-  pou_image_tables(tab, a, a.geo + n * kGeo);
-  WarpFft<M, true> fft;
-  fft.init(lane);
-  __syncthreads();
-  // half rows ka = 0 .. H of X_h, each an inverse FFT along the row
-  for (int ka = wid; ka < NR; ka += NW) {
-    const int i = ka + H < P ? ka + H : ka - H;        // S row of X[ka, .]
-    const int im = H - ka >= 0 ? H - ka : H - ka + P;  // S row of X[-ka, .]
-    Cx<float> x[M];
-    {
-      Raw<DT> raw[M];
-#pragma unroll
-      for (int m = 0; m < M; ++m) {
-        const int kb = lane + 32 * m;
-        pou_tab_gather<DT>(st, tab, P, i, kb + H < P ? kb + H : kb - H, raw[m]);
-      }
-#pragma unroll
-      for (int m = 0; m < M; ++m) {
-        const int kb = lane + 32 * m, j = kb + H < P ? kb + H : kb - H;
-        Interp o;
-        pou_table_sample<DT, false>(st, raw[m], tab.frac[P + i], tab.frac[j], o);
-        x[m] = Cx<float>{0.5f * o.sr, 0.5f * o.si};
-      }
-    }
-    {
-      Raw<DT> raw[M];
-#pragma unroll
-      for (int m = 0; m < M; ++m) {
-        const int kb = lane + 32 * m;
-        pou_tab_gather<DT>(st, tab, P, im, H - kb >= 0 ? H - kb : H - kb + P, raw[m]);
-      }
-#pragma unroll
-      for (int m = 0; m < M; ++m) {
-        const int kb = lane + 32 * m, jm = H - kb >= 0 ? H - kb : H - kb + P;
-        Interp o;
-        pou_table_sample<DT, false>(st, raw[m], tab.frac[P + im], tab.frac[jm], o);
-        x[m].x = fmaf(0.5f, o.sr, x[m].x);
-        x[m].y = fmaf(-0.5f, o.si, x[m].y);
-      }
-    }
-    fft.run(x, lane);
-#pragma unroll
-    for (int k = 0; k < M; ++k) buf[ka * PITCH + lane + 32 * k] = x[k];  // slot of image column k + M brev5(lane)
-  }
-  __syncthreads();
-  // image columns two at a time (Hermitian column spectra, the upper half
-  // read as conj of the lower)
-  const float scale = 1.f / static_cast<float>(P * P);
-  for (int t = wid; t < H; t += NW) {
-    const int c1 = wfft_pos<M>(2 * t), c2 = wfft_pos<M>(2 * t + 1);
-    Cx<float> z[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int ka = lane + 32 * m;
-      const bool lo = ka <= H;
-      const int row = (lo ? ka : P - ka) * PITCH;
-      const Cx<float> v1 = buf[row + c1], v2 = buf[row + c2];
-      const float s = lo ? 1.f : -1.f;  // conjugate the mirrored half
-      z[m] = Cx<float>{v1.x - s * v2.y, s * v1.y + v2.x};
-    }
-    fft.run(z, lane);
-#pragma unroll
-    for (int k = 0; k < M; ++k) {
-      const int y = k + M * brev5(lane);
-      const int e1 = ((y >> 1) * PITCH + c1) * 2 + (y & 1), e2 = ((y >> 1) * PITCH + c2) * 2 + (y & 1);
-      if (fvr_checked(e1, 2LL * NR * PITCH, kSiteHalfImage)) bf[e1] = z[k].x * scale;
-      if (fvr_checked(e2, 2LL * NR * PITCH, kSiteHalfImage)) bf[e2] = z[k].y * scale;
-    }
-  }
-  __syncthreads();
-  // fftshift-ordered image rows, coalesced
-  float* out = imgs + (static_cast<int64_t>(b) * a.N + n) * P * P;
-  for (int q = threadIdx.x; q < P * P; q += kPouHalfThreads) {
-    const int yo = q / P, xo = q - yo * P;
-    const int y = yo + H < P ? yo + H : yo - H, x = xo + H < P ? xo + H : xo - H;
-    out[q] = bf[((y >> 1) * PITCH + wfft_pos<M>(x)) * 2 + (y & 1)];
-  }
-}
-
-// Adjoint of pou_slice_c2r_kernel: G = fftshift(fft2(ifftshift(g))) / P^2 kept
-// as its columns kb = 0 .. P/2, then the per-sample products with the
-// spectrum derivatives as in pou_fft_slice_adjoint_kernel.
-template <int DT, int M>
-__global__ void __launch_bounds__(kPouHalfThreads, 2) pou_r2c_slice_adjoint_kernel(PouSliceArgs a,
-                                                                                  const float* __restrict__ gimg,
-                                                                                  double* __restrict__ partial) {
-  constexpr int P = 32 * M, H = P / 2, NC = pou_half_cols(P), PITCH = NC, NW = kPouHalfThreads / 32, GROUP = 4;
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ double red[6 * NW];
-  Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem);
-  const AxisTables tab = axis_tables(smem + pou_half_tab_offset<M>(), 2 * P);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  Cx<float>* zrow = reinterpret_cast<Cx<float>*>(smem + pou_half_tab_offset<M>() + 40 * 2 * P) + wid * P;
-  const int n = blockIdx.x, b = blockIdx.y;
-  const Stencil st = pou_block_stencil(a, b);
-  pou_image_tables(tab, a, a.geo + n * kGeo);
-  WarpFft<M, false> fft;
-  fft.init(lane);
-  const float* g = gimg + (static_cast<int64_t>(b) * a.N + n) * P * P;
-  // rows of ifftshift(g) two at a time through one complex FFT, separated
-  // into the two Hermitian row spectra; columns 0 .. H kept (natural row order)
-  for (int t = wid; t < H; t += NW) {
-    const int a1 = 2 * t, a2 = 2 * t + 1;
-    const int y1 = a1 + H < P ? a1 + H : a1 - H, y2 = a2 + H < P ? a2 + H : a2 - H;
-    Cx<float> z[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int c = lane + 32 * m, xs = c + H < P ? c + H : c - H;
-      z[m] = Cx<float>{__ldg(g + y1 * P + xs), __ldg(g + y2 * P + xs)};
-    }
-    fft.run(z, lane);
-#pragma unroll
-    for (int k = 0; k < M; ++k) zrow[k + M * brev5(lane)] = z[k];
-    __syncwarp();
-    for (int kb = lane; kb < NC; kb += 32) {
-      const Cx<float> p = zrow[kb], q = zrow[kb == 0 ? 0 : P - kb];  // Z[k], Z[-k]
-      // G1 = (Z[k] + conj Z[-k]) / 2, G2 = (Z[k] - conj Z[-k]) / 2i
-      buf[a1 * PITCH + kb] = Cx<float>{0.5f * (p.x + q.x), 0.5f * (p.y - q.y)};
-      buf[a2 * PITCH + kb] = Cx<float>{0.5f * (p.y + q.y), 0.5f * (q.x - p.x)};
-    }
-    __syncwarp();
-  }
-  __syncthreads();
-  for (int kb = wid; kb < NC; kb += NW) {
-    Cx<float> x[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) x[m] = buf[(lane + 32 * m) * PITCH + kb];
-    fft.run(x, lane);
-#pragma unroll
-    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + kb] = x[k];
-  }
-  __syncthreads();
-  const float scale = 1.f / static_cast<float>(P * P);
-  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  for (int q0 = threadIdx.x; q0 < P * P; q0 += kPouHalfThreads * GROUP) {
-    Raw<DT> raw[GROUP];
-#pragma unroll
-    for (int u = 0; u < GROUP; ++u) {
-      const int q = q0 + u * kPouHalfThreads;
-      const int i = q < P * P ? q / P : 0, j = q < P * P ? q - (q / P) * P : 0;
-      TabCell cell = tab_cell(st, tab.idx[P + i], tab.frac[P + i], tab.idx[j], tab.frac[j]);
-      if (q >= P * P) cell.e = -1;
-      tab_load<DT>(st, cell, raw[u]);
-    }
-#pragma unroll
-    for (int u = 0; u < GROUP; ++u) {
-      const int q = q0 + u * kPouHalfThreads;
-      if (q >= P * P) continue;
-      const int i = q / P, j = q - i * P;
-      const float4 fa = tab.frac[P + i], fb = tab.frac[j];
-      Interp o;
-      pou_table_sample<DT, true>(st, raw[u], fa, fb, o);
-      const int ka = i + H < P ? i + H : i - H, kb = j + H < P ? j + H : j - H;
-      const bool lo = kb <= H;
-      const int gpos = lo ? wfft_pos<M>(ka) * PITCH + kb : wfft_pos<M>(ka == 0 ? 0 : P - ka) * PITCH + (P - kb);
-      Cx<float> G = fvr_checked(gpos, P * PITCH, kSiteHalfImage) ? buf[gpos] : Cx<float>{0.f, 0.f};
-      if (!lo) G.y = -G.y;
-      const float gx = G.x * scale, gy = G.y * scale;
-      const float e0 = gx * o.dxr + gy * o.dxi, e1 = gx * o.dyr + gy * o.dyi, e2 = gx * o.dzr + gy * o.dzi;
-      const float fx = fb.w, fy = fa.w;
-      acc[0] = fmaf(fx, e0, acc[0]);
-      acc[1] = fmaf(fx, e1, acc[1]);
-      acc[2] = fmaf(fx, e2, acc[2]);
-      acc[3] = fmaf(fy, e0, acc[3]);
-      acc[4] = fmaf(fy, e1, acc[4]);
-      acc[5] = fmaf(fy, e2, acc[5]);
-    }
-  }
-#pragma unroll
-  for (int m = 0; m < 6; ++m) {
-    const double v = warp_sum(static_cast<double>(acc[m]));
-    if (lane == 0) red[m * NW + wid] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x < 6) {
-    double sum = 0.0;
-    for (int w = 0; w < NW; ++w) sum += red[threadIdx.x * NW + w];
-    partial[(static_cast<int64_t>(n) * gridDim.y + b) * 6 + threadIdx.x] = sum;
-  }
-}
-
-// ----------------------------------------------------------------------------
 // pinhole warp + sum  (triton_slice.py:348-407 / 409-496)
 // ----------------------------------------------------------------------------
 
@@ -1381,28 +1129,29 @@ static PouBase make_base(const double* base12) {
 
 using namespace fvr;
 
-// Opt a half-spectrum image kernel in to its dynamic shared memory (above the
-// default 48 KB) with the largest shared-memory carve-out, so two CTAs fit.
-template <typename K>
-static bool pou_half_attr(K kernel, int64_t smem) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) ==
-             cudaSuccess &&
-         cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100) == cudaSuccess;
-}
-
 template <int DT, int M>
 static int pou_image_launch(bool adjoint, const PouSliceArgs& a, int B, const float* gimg, float* imgs,
                             double* part, cudaStream_t s) {
-  const int64_t smem = adjoint ? pou_half_smem(32 * M) : pou_c2r_smem(32 * M);
+  const int64_t smem = pou_image_smem(32 * M);
   dim3 grid(static_cast<unsigned>(a.N), static_cast<unsigned>(B));
   if (adjoint) {
-    static const bool attr = pou_half_attr(pou_r2c_slice_adjoint_kernel<DT, M>, smem);
-    if (!attr) return FVR_ERR_CUDA;
-    pou_r2c_slice_adjoint_kernel<DT, M><<<grid, kPouHalfThreads, smem, s>>>(a, gimg, part);
+    static bool attr = false;
+    if (!attr) {
+      if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)) != cudaSuccess)
+        return FVR_ERR_CUDA;
+      attr = true;
+    }
+    pou_fft_slice_adjoint_kernel<DT, M><<<grid, kPouImgThreads, smem, s>>>(a, gimg, part);
   } else {
-    static const bool attr = pou_half_attr(pou_slice_c2r_kernel<DT, M>, smem);
-    if (!attr) return FVR_ERR_CUDA;
-    pou_slice_c2r_kernel<DT, M><<<grid, kPouHalfThreads, smem, s>>>(a, imgs);
+    static bool attr = false;
+    if (!attr) {
+      if (cudaFuncSetAttribute(pou_slice_ifft_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem)) != cudaSuccess)
+        return FVR_ERR_CUDA;
+      attr = true;
+    }
+    pou_slice_ifft_kernel<DT, M><<<grid, kPouImgThreads, smem, s>>>(a, imgs);
   }
   FVR_LAUNCH_CHECK();
   return FVR_OK;
