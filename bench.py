@@ -306,12 +306,14 @@ def run_b200(args, torch):
         alg_bytes = samples * (8 * 4 + 8 * 4 + 8 + 4)
         min_bytes = samples * (32 + 8)
         achieved = alg_bytes / (kern_avg_ms * 1e-3) / 1e9
-        traffic = None
+        traffic, ncu = None, {}
         tf = REPO / "profiles" / "tc_sncc_moments_f16_128cube_64cand_traffic.txt"
         if tf.exists():
             for line in tf.read_text().splitlines():
-                if line.startswith("dram_bytes_per_launch:"):
-                    traffic = float(line.split(":", 1)[1])
+                if ":" in line and not line.startswith("#"):
+                    k, v = line.split(":", 1)
+                    ncu[k.strip()] = float(v)
+            traffic = ncu.get("dram_bytes_per_launch")
         cpu = _cpu_baseline_leg(vol, poses_np, f_ap, f_lat, results)
         single_value = 1.0 / (statistics.mean(t_single) / 1e3)
         res = {
@@ -363,6 +365,13 @@ def run_b200(args, torch):
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6.65 TB/s",
                 "traffic": traffic,
+                "ncu_capture": {"source": "profiles/tc_sncc_moments_f16_128cube_64cand.md (cold, serialised)",
+                                "kernel_us": ncu.get("ncu_kernel_us"),
+                                "dram_pct_of_peak": ncu.get("dram_pct_of_peak"),
+                                "l2_bytes_per_launch": ncu.get("l2_bytes_per_launch"),
+                                "l2_gbs": (ncu["l2_bytes_per_launch"] / ncu["ncu_kernel_us"] / 1e3
+                                           if "l2_bytes_per_launch" in ncu and "ncu_kernel_us" in ncu else None),
+                                "l2_pct_of_peak": ncu.get("l2_pct_of_peak")},
                 "alg_bytes_per_launch": alg_bytes,
                 "alg_bytes_note": "64 pose-evals x 2.49 MB: 2 views x 16384 samples x (8 corners x 4 B forward "
                                   "gather + 8 corners x 4 B adjoint gather + 8 B target + 4 B brick scale)",
