@@ -57,6 +57,12 @@ def _record(ev):
     L.call("fvr_event_record", ctypes.c_void_p(ev.cuda_event), L.stream_ptr(), ext)
 
 
+def timing(name):
+    """True when a LaunchTimer is collecting ``name`` (a cheap check before
+    entering :func:`section` on a hot path)."""
+    return _active is not None and name in _active.names
+
+
 @contextlib.contextmanager
 def section(name):
     t = _active
