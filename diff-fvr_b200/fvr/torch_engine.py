@@ -34,6 +34,11 @@ from . import _lib as L
 from . import _runtime as RT
 from . import autotune, profiling
 
+try:  # native autograd binding (csrc/fvr_autograd.cpp, built next to the CUDA library)
+    from . import _fvr_autograd as _NATIVE
+except ImportError:
+    _NATIVE = None
+
 VIEW_AP, VIEW_LATERAL = 0, 1
 
 
@@ -86,9 +91,11 @@ class _FusedCall:
     """A prepared launch of fvr_tc_sncc_value_and_grad: every argument except
     the poses, the two outputs and the stream converted to its C type once
     (engine storage, shape, views, target spectra, high-pass table, chosen
-    launch variant, cached workspace), so a call costs one foreign call."""
+    launch variant, cached workspace), so a call costs one foreign call.
+    ``native`` is the same launch prepared for the native autograd binding
+    (None without it)."""
 
-    __slots__ = ("fn", "head", "mid", "keep")
+    __slots__ = ("fn", "head", "mid", "keep", "native")
 
     def launch(self, p, loss, grad, stream):
         L.launch_count[0] += 2
@@ -139,15 +146,31 @@ def _fused_call(eng, C, R, views, ftargs, hp, p):
                 ctypes.c_double(RT.kappa(R, eng.spacing[0])), ctypes.c_int(int(variant)), None, ctypes.c_int64(0),
                 L.ptr(ws), ctypes.c_int64(ws_bytes))
 
+    p32 = []
+
     def run(variant):
+        if not p32:
+            p32.append(p.detach().to(device=dev, dtype=torch.float32).contiguous())
         call.mid = mid(variant)
         loss = torch.empty(nv + 1, dtype=torch.float32, device=dev)
         grad = torch.empty((C, 6), dtype=torch.float32, device=dev)
-        call.launch(p, loss, grad, L.stream_ptr(dev))
+        call.launch(p32[0], loss, grad, L.stream_ptr(dev))
 
     variant = autotune.choose("sncc_fused", (st.code, C, R, nv, st.dims), run, L.load().fvr_tc_sncc_variants(),
                               candidates=_FUSED_VARIANTS)
     call.mid = mid(variant)
+    call.native = None
+    if _NATIVE is not None:
+        lib = L.load()
+        addr = lambda f: ctypes.cast(f, ctypes.c_void_p).value  # noqa: E731
+        sp = 0 if st.scales is None else int(st.scales.data_ptr())
+        call.native = _NATIVE.SnccCall(
+            fn=addr(lib.fvr_tc_sncc_value_and_grad), status=addr(lib.fvr_status_string), dtype=st.code,
+            stencil=int(st.data.data_ptr()), scales=sp, D=st.dims[0], H=st.dims[1], W=st.dims[2], C=C,
+            views=list(views), ftargs=[int(f.data_ptr()) for f in fts], hp=0 if hp is None else int(hp.data_ptr()),
+            lin=int(lin.data_ptr()), R=R, kappa=RT.kappa(R, eng.spacing[0]), variant=int(variant),
+            ws=int(ws.data_ptr()), ws_bytes=ws_bytes, device=dev.index,
+            keep=[t for t in (st.data, st.scales, hp, lin, ws) if t is not None] + fts)
     if direct:
         if len(eng._fused_calls) > 64:
             eng._fused_calls.clear()
@@ -183,6 +206,23 @@ def _sncc_fused(eng, p, views, ftargs, hp, R, out=None, loss_out=None):
     else:
         call.launch(p, loss, grad, _current_stream(dev))
     return loss, grad
+
+
+def _sncc_loss(eng, p, views, hp, R, ftargs):
+    """sum_v forward_spectral_ncc(p, ftargs[v], views[v]) as one autograd node.
+    With a pose gradient to compute, the native binding runs the fused launch
+    (moments kernel + dependent epilogue) and keeps dL/dposes; otherwise (or
+    without the binding, or while launches are being timed) the Python node
+    below does the same."""
+    if (_NATIVE is not None and p.requires_grad and torch.is_grad_enabled()
+            and not profiling.timing("tc_sncc_moments")):
+        call = _fused_call(eng, int(p.shape[0]), R, views, ftargs, hp, p)
+        L.launch_count[0] += 2
+        try:
+            return _NATIVE.sncc_loss(p, call.native)
+        except RuntimeError as e:
+            raise L.FvrError(str(e)) from None
+    return _SpectralNCCFn.apply(p, eng, views, hp, R, *ftargs)
 
 
 class _SpectralNCCFn(torch.autograd.Function):
@@ -452,7 +492,7 @@ class TorchDiffFVREngine(nn.Module):
             return torch.full((), float("nan"), dtype=torch.float32, device=self._dev) + 0.0 * poses.sum().to(self._dev)
         R = int(f_targ_precomputed.shape[-1])
         hp = RT.hp_filter(R, R, cutoff_sigma, self._dev) if high_pass else None
-        return _SpectralNCCFn.apply(self._prep_poses(poses), self, (_view_code(view),), hp, R, f_targ_precomputed)
+        return _sncc_loss(self, self._prep_poses(poses), (_view_code(view),), hp, R, (f_targ_precomputed,))
 
     def forward_spectral_ncc(self, poses: torch.Tensor, f_targ_precomputed: torch.Tensor, view: str = "ap",
                              high_pass: bool = True, cutoff_sigma: float = 4.0) -> torch.Tensor:
@@ -467,7 +507,7 @@ class TorchDiffFVREngine(nn.Module):
         R = int(f_targs[0].shape[-1])
         hp = RT.hp_filter(R, R, cutoff_sigma, self._dev) if high_pass else None
         codes = tuple(_view_code(v) for v in views)
-        return _SpectralNCCFn.apply(self._prep_poses(poses), self, codes, hp, R, *f_targs)
+        return _sncc_loss(self, self._prep_poses(poses), codes, hp, R, tuple(f_targs))
 
     def spectral_ncc_value_and_grad(self, poses, f_targs, views=("ap", "lateral"), high_pass=True,
                                     cutoff_sigma=4.0, out_grad=None, out_loss=None):

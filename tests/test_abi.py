@@ -78,3 +78,24 @@ def test_product_path_fails_loudly_without_a_gpu():
     f = torch.zeros(4)
     with pytest.raises(L.FvrError):
         fourier_slice_3d(vol, u, u, f, f, (1.5, 1.5, 1.5))
+
+
+def test_native_autograd_binding_loads():
+    """The native autograd binding (csrc/fvr_autograd.cpp) builds against the
+    installed PyTorch, imports, and refuses a prepared launch with null
+    pointers before anything runs (no GPU needed)."""
+    import sys
+
+    import torch
+
+    sys.path.insert(0, str(REPO / "diff-fvr_b200" / "csrc"))
+    import build_autograd
+
+    build_autograd.build()
+    from fvr import _fvr_autograd as A
+    from fvr import torch_engine
+
+    assert torch_engine._NATIVE is A
+    with pytest.raises(RuntimeError, match="null pointer"):
+        A.SnccCall(fn=0, status=0, dtype=0, stencil=0, scales=0, D=1, H=1, W=1, C=1, views=[0], ftargs=[0], hp=0,
+                   lin=0, R=1, kappa=0.0, variant=0, ws=0, ws_bytes=0, device=0, keep=[torch.zeros(1)])

@@ -410,6 +410,54 @@ def test_fused_variants_agree_on_ragged_shapes(big, monkeypatch, C, R):
         assert torch.allclose(ga, g0, rtol=1e-4, atol=1e-5 * scale), variant
 
 
+def test_native_autograd_binding_matches_python_node(big):
+    """forward_spectral_ncc with a pose gradient runs through the native
+    autograd binding: same loss and gradient bits as the Python autograd
+    node (the same prepared launch), an upstream factor scales the gradient,
+    float64 / CPU / non-contiguous poses get their gradient in their own
+    dtype and device, and two views' nodes accumulate as torch adds them."""
+    import fvr._lib as L
+    from fvr import torch_engine as TE
+
+    assert TE._NATIVE is not None
+    _, eng, _ = big
+    poses = tc.make_poses(8, 21)
+    tp = _t(tc.make_poses(1, 22))
+    fa = eng.prepare_spectral_target(eng(tp, view="ap", out_res=128))
+    fl = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=128))
+    hp = eng._get_hp_filter(128, 128, 4.0).view(-1)
+
+    p_py = _t(poses).requires_grad_(True)
+    l_py = TE._SpectralNCCFn.apply(p_py, eng, (0,), hp, 128, fa)
+    (2.5 * l_py).backward()
+    p_nat = _t(poses).requires_grad_(True)
+    n0 = L.launch_count[0]
+    l_nat = eng.forward_spectral_ncc(p_nat, fa, view="ap")
+    assert L.launch_count[0] == n0 + 2
+    assert l_nat.grad_fn is not None and l_nat.grad_fn.name() == "SnccLoss"
+    (2.5 * l_nat).backward()
+    assert float(l_nat) == float(l_py)
+    assert torch.equal(p_nat.grad, p_py.grad)
+
+    p64 = torch.from_numpy(poses.astype(np.float64)).requires_grad_(True)  # CPU, float64
+    l64 = eng.forward_spectral_ncc(p64, fa, view="ap") + eng.forward_spectral_ncc(p64, fl, view="lateral")
+    l64.backward()
+    assert p64.grad.dtype == torch.float64 and p64.grad.device.type == "cpu"
+    p32 = _t(poses).requires_grad_(True)
+    lb = TE._SpectralNCCFn.apply(p32, eng, (0,), hp, 128, fa) + TE._SpectralNCCFn.apply(p32, eng, (1,), hp, 128, fl)
+    lb.backward()
+    assert abs(float(l64) - float(lb)) < 1e-6
+    assert torch.allclose(p64.grad.float(), p32.grad.cpu(), rtol=1e-6, atol=1e-9)
+
+    base = torch.zeros((8, 12), device="cuda")
+    base[:, ::2] = _t(poses)
+    pnc = base[:, ::2].detach().requires_grad_(True)  # non-contiguous leaf
+    eng.forward_spectral_ncc(pnc, fa, view="ap").backward()
+    assert torch.allclose(pnc.grad, p_py.grad / 2.5, rtol=1e-6, atol=0.0)
+    with torch.no_grad():  # no gradient wanted: the value-only moments
+        assert abs(float(eng.forward_spectral_ncc(_t(poses), fa, view="ap")) - float(l_py)) < 1e-6
+
+
 def test_host_io_graph_step_matches_device_step(big):
     """The host-to-host graph (pinned-host read of the poses, the kernels, the
     epilogue writing pinned host outputs, in one replay) returns exactly the
