@@ -434,7 +434,7 @@ def test_native_autograd_binding_matches_python_node(big):
     n0 = L.launch_count[0]
     l_nat = eng.forward_spectral_ncc(p_nat, fa, view="ap")
     assert L.launch_count[0] == n0 + 2
-    assert l_nat.grad_fn is not None and l_nat.grad_fn.name() == "SnccLoss"
+    assert l_nat.grad_fn is not None and "SnccLoss" in l_nat.grad_fn.name()
     (2.5 * l_nat).backward()
     assert float(l_nat) == float(l_py)
     assert torch.equal(p_nat.grad, p_py.grad)
