@@ -6,6 +6,10 @@ namespace {
 // dst[0..n) = src[0..n); 16-byte words when both ends and n allow it.
 __global__ void __launch_bounds__(256) copy_bytes_kernel(unsigned char* __restrict__ dst,
                                                          const unsigned char* __restrict__ src, int64_t n) {
+  // a kernel launched after this one as its programmatic dependent may be
+  // scheduled now; it still waits (griddepcontrol.wait) for this grid to
+  // complete before it reads anything (no-op without such a dependent)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   const bool wide = ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15) == 0;

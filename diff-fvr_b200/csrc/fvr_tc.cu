@@ -441,6 +441,7 @@ __global__ void __launch_bounds__(kSnccThreads, MINB) tc_sncc_moments_kernel(Snc
   const int row_end = min(row_begin + a.tile_rows, R);
   const SnccTab tab = sncc_tab(tab_smem, R + a.tile_rows);
   pdl_launch_dependents();
+  pdl_wait();  // launched as a programmatic dependent: the kernel before it has completed (else a no-op)
   if (threadIdx.x == 0) sncc_item_axes(a, v, c, ax_s);
   __syncthreads();
   build_sncc_tables(tab, R, row_begin, row_end - row_begin, a.lin, ax_s, a.sx, a.sy, a.sz, a.kpi);
@@ -825,19 +826,36 @@ static SnccPlan sncc_plan(int64_t C, int64_t R, int nv, int variant) {
 static int64_t sncc_smem(int64_t R, int tile_rows) { return (R + tile_rows) * kSnccTabEntryBytes; }
 constexpr int64_t kSnccMaxSmem = 200 * 1024;
 
+// pdl: launch as a programmatic dependent of the kernel before it on the
+// stream (the moments kernel waits for that kernel's completion before its
+// first read, so only the launch overlaps it); plain launch where refused.
 template <int DT, bool GRAD, int VI>
-static void launch_sncc_v(dim3 grid, int smem, cudaStream_t st, const SnccArgs& a) {
+static void launch_sncc_v(dim3 grid, int smem, cudaStream_t st, const SnccArgs& a, bool pdl) {
   constexpr SnccVariant v = sncc_variant(VI);
   auto k = tc_sncc_moments_kernel<DT, GRAD, v.group, v.min_blocks>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (pdl) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(kSnccThreads);
+    cfg.dynamicSmemBytes = static_cast<size_t>(smem);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k, a) == cudaSuccess) return;
+    (void)cudaGetLastError();
+  }
   k<<<grid, kSnccThreads, smem, st>>>(a);
 }
 
 template <int DT, bool GRAD>
-static void launch_sncc(int variant, dim3 grid, int smem, cudaStream_t s, const SnccArgs& a) {
+static void launch_sncc(int variant, dim3 grid, int smem, cudaStream_t s, const SnccArgs& a, bool pdl = false) {
   switch (variant) {
 #define FVR_V(n) \
-  case n: launch_sncc_v<DT, GRAD, n>(grid, smem, s, a); break;
+  case n: launch_sncc_v<DT, GRAD, n>(grid, smem, s, a, pdl); break;
     FVR_V(0) FVR_V(1) FVR_V(2) FVR_V(3) FVR_V(4) FVR_V(5) FVR_V(6) FVR_V(7)
 #undef FVR_V
     default: break;
@@ -1049,9 +1067,9 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
   a.accumulate = accumulate;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (dtype) {
-    case FVR_F32: launch_sncc<FVR_F32, true>(variant, grid, (int)smem, s, a); break;
-    case FVR_BF16: launch_sncc<FVR_BF16, true>(variant, grid, (int)smem, s, a); break;
-    case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_F32: launch_sncc<FVR_F32, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_BF16: launch_sncc<FVR_BF16, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a, true); break;
   }
   FVR_LAUNCH_CHECK();
   launch_sncc_final(s, a);
@@ -1180,9 +1198,9 @@ int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const floa
   a.accumulate = accumulate;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   switch (dtype) {
-    case FVR_F32: launch_sncc<FVR_F32, true>(variant, grid, (int)smem, s, a); break;
-    case FVR_BF16: launch_sncc<FVR_BF16, true>(variant, grid, (int)smem, s, a); break;
-    case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a); break;
+    case FVR_F32: launch_sncc<FVR_F32, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_BF16: launch_sncc<FVR_BF16, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a, true); break;
   }
   FVR_LAUNCH_CHECK();
   launch_sncc_final(s, a);
