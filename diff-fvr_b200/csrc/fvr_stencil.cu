@@ -118,6 +118,91 @@ __global__ void stencil_build_kernel(const MT* __restrict__ m0, int64_t plane, i
   }
 }
 
+// ---- x-pair layout (16-bit): entry (ez, ey, ex) = the 4 complex values of
+// voxel column x = ex - 1 at (y, z) = (ey - 1 + dy, ez - 1 + dz), k = dz*2 + dy.
+template <typename MT>
+__device__ __forceinline__ void pair_values(const MT* m, int64_t plane, int D, int H, int W, int ez, int ey, int ex,
+                                            float (&re)[4], float (&im)[4]) {
+  const int x = ex - 1;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int z = ez - 1 + (k >> 1), y = ey - 1 + (k & 1);
+    if (z >= 0 && z < D && y >= 0 && y < H && x >= 0 && x < W) {
+      const float2 v = master_load(m, (static_cast<int64_t>(z) * H + y) * W + x, plane);
+      re[k] = v.x;
+      im[k] = v.y;
+    } else {
+      re[k] = 0.f;
+      im[k] = 0.f;
+    }
+  }
+}
+
+// f16 scale slabs: kBrick x kBrick (z, y) entry rows over the whole x extent,
+// so the two entries of every sample share one scale.
+struct PairGrid {
+  int ew, eh, ed;  // entries along x, y, z: W + 2, H + 1, D + 1
+  int by;          // slabs along y
+  __device__ __forceinline__ int64_t slab(int ez, int ey) const {
+    return static_cast<int64_t>(ez / kBrick) * by + ey / kBrick;
+  }
+};
+
+__host__ __device__ inline PairGrid pair_grid(int D, int H, int W) {
+  PairGrid g;
+  g.ew = W + 2;
+  g.eh = H + 1;
+  g.ed = D + 1;
+  g.by = (g.eh + kBrick - 1) / kBrick;
+  return g;
+}
+
+template <typename MT>
+__global__ void pair_slab_max_kernel(const MT* __restrict__ m, int64_t plane, int D, int H, int W,
+                                     unsigned int* __restrict__ smax) {
+  const PairGrid g = pair_grid(D, H, W);
+  const int64_t n = static_cast<int64_t>(g.ed) * g.eh * g.ew;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int ex = static_cast<int>(e % g.ew), ey = static_cast<int>((e / g.ew) % g.eh);
+    const int ez = static_cast<int>(e / (static_cast<int64_t>(g.ew) * g.eh));
+    float re[4], im[4];
+    pair_values(m, plane, D, H, W, ez, ey, ex, re, im);
+    float mx = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mx = fmaxf(mx, fmaxf(fabsf(re[k]), fabsf(im[k])));
+    atomicMax(smax + g.slab(ez, ey), __float_as_uint(mx));  // non-negative floats order like their bits
+  }
+}
+
+template <typename MT, int DT>
+__global__ void pair_build_kernel(const MT* __restrict__ m, int64_t plane, int D, int H, int W,
+                                  uint4* __restrict__ out, const float* __restrict__ scales) {
+  const PairGrid g = pair_grid(D, H, W);
+  const int64_t n = static_cast<int64_t>(g.ed) * g.eh * g.ew;
+  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int ex = static_cast<int>(e % g.ew), ey = static_cast<int>((e / g.ew) % g.eh);
+    const int ez = static_cast<int>(e / (static_cast<int64_t>(g.ew) * g.eh));
+    float re[4], im[4];
+    pair_values(m, plane, D, H, W, ez, ey, ex, re, im);
+    uint32_t w[4];
+    if constexpr (DT == FVR_BF16_PAIR) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        w[k] = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(re[k]))) |
+               (static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(im[k]))) << 16);
+    } else {
+      const float inv = 1.f / scales[g.slab(ez, ey)];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        w[k] = static_cast<uint32_t>(__half_as_ushort(__float2half_rn(re[k] * inv))) |
+               (static_cast<uint32_t>(__half_as_ushort(__float2half_rn(im[k] * inv))) << 16);
+    }
+    out[e] = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
 // relu mask of the saved image, as complex: G = (img > 0) * g
 __global__ void relu_mask_kernel(const float* __restrict__ img, const float* __restrict__ g, float* __restrict__ out,
                                  int64_t n) {
@@ -188,6 +273,9 @@ int fvr_stencil_build(const void* master, int master_dtype, int master_planar, i
     else if (master_dtype == FVR_BF16)
       stencil_brick_max_kernel<__nv_bfloat16>
           <<<grid, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(master), plane, items, d, h, w, scratch_max);
+    else if (master_dtype == FVR_F16)
+      stencil_brick_max_kernel<__half>
+          <<<grid, 256, 0, s>>>(static_cast<const __half*>(master), plane, items, d, h, w, scratch_max);
     else
       return FVR_ERR_DTYPE;
     stencil_scale_kernel<<<static_cast<unsigned>(cdiv64(nb, 256)), 256, 0, s>>>(scratch_max, scales, nb);
@@ -210,10 +298,72 @@ int fvr_stencil_build(const void* master, int master_dtype, int master_planar, i
       case FVR_F16: FVR_BUILD(__nv_bfloat16, FVR_F16)
       default: return FVR_ERR_DTYPE;
     }
+  } else if (master_dtype == FVR_F16) {
+    switch (out_dtype) {
+      case FVR_F32: FVR_BUILD(__half, FVR_F32)
+      case FVR_BF16: FVR_BUILD(__half, FVR_BF16)
+      case FVR_F16: FVR_BUILD(__half, FVR_F16)
+      default: return FVR_ERR_DTYPE;
+    }
   } else {
     return FVR_ERR_DTYPE;
   }
 #undef FVR_BUILD
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+int64_t fvr_stencil_pair_bytes(int64_t D, int64_t H, int64_t W, int dtype) {
+  if (D < 1 || H < 1 || W < 1 || (dtype != FVR_BF16_PAIR && dtype != FVR_F16_PAIR)) return 0;
+  return (D + 1) * (H + 1) * (W + 2) * 16;
+}
+
+int64_t fvr_stencil_pair_scale_count(int64_t D, int64_t H, int64_t W) {
+  if (D < 1 || H < 1 || W < 1) return 0;
+  return cdiv64(D + 1, kBrick) * cdiv64(H + 1, kBrick);
+}
+
+int fvr_stencil_pair_build(const void* master, int master_dtype, int master_planar, int64_t D, int64_t H, int64_t W,
+                           int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream) {
+  if (!master || !out || D < 1 || H < 1 || W < 1 || D > 8192 || H > 8192 || W > 8192) return FVR_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(out) & 15) != 0) return FVR_ERR_ARG;
+  if (out_dtype != FVR_BF16_PAIR && out_dtype != FVR_F16_PAIR) return FVR_ERR_DTYPE;
+  if (master_dtype != FVR_F32 && master_dtype != FVR_BF16 && master_dtype != FVR_F16) return FVR_ERR_DTYPE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int64_t n = (D + 1) * (H + 1) * (W + 2);
+  const int64_t nblk = cdiv64(n, 256);
+  const unsigned grid = static_cast<unsigned>(nblk < 148 * 64 ? nblk : 148 * 64);
+  const int d = (int)D, h = (int)H, w = (int)W;
+  const int64_t plane = master_planar ? D * H * W : 0;
+  if (out_dtype == FVR_F16_PAIR) {
+    if (!scales || !scratch_max) return FVR_ERR_ARG;
+    const int64_t nb = fvr_stencil_pair_scale_count(D, H, W);
+    if (cudaMemsetAsync(scratch_max, 0, nb * sizeof(unsigned int), s) != cudaSuccess) return FVR_ERR_CUDA;
+    if (master_dtype == FVR_F32)
+      pair_slab_max_kernel<float><<<grid, 256, 0, s>>>(static_cast<const float*>(master), plane, d, h, w, scratch_max);
+    else if (master_dtype == FVR_BF16)
+      pair_slab_max_kernel<__nv_bfloat16>
+          <<<grid, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(master), plane, d, h, w, scratch_max);
+    else
+      pair_slab_max_kernel<__half><<<grid, 256, 0, s>>>(static_cast<const __half*>(master), plane, d, h, w,
+                                                        scratch_max);
+    stencil_scale_kernel<<<static_cast<unsigned>(cdiv64(nb, 256)), 256, 0, s>>>(scratch_max, scales, nb);
+  }
+#define FVR_PAIR(MT)                                                                                          \
+  if (out_dtype == FVR_F16_PAIR)                                                                              \
+    pair_build_kernel<MT, FVR_F16_PAIR><<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, d, h, w,  \
+                                                             static_cast<uint4*>(out), scales);                \
+  else                                                                                                        \
+    pair_build_kernel<MT, FVR_BF16_PAIR><<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, d, h, w, \
+                                                              static_cast<uint4*>(out), nullptr);
+  if (master_dtype == FVR_F32) {
+    FVR_PAIR(float)
+  } else if (master_dtype == FVR_BF16) {
+    FVR_PAIR(__nv_bfloat16)
+  } else {
+    FVR_PAIR(__half)
+  }
+#undef FVR_PAIR
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }

@@ -362,7 +362,10 @@ class PerspectiveSlabFVR(nn.Module):
         del real
         F_ri = torch.view_as_real(spec).permute(0, 4, 1, 2, 3).contiguous()
         del spec
+        # the stencil comes from the float32 spectra (f16 storage takes its brick scales from them)
+        self._stencil = RT.Stencil(F_ri, True, (self.P,) * 3, self._stencil_dtype(dtype), items=self.B)
         self.register_buffer("F_blk_ri", F_ri.to(dtype=dtype))
+        del F_ri
         self.register_buffer("centers", torch.tensor(centers, dtype=torch.float32, device=dev))
         freqs = torch.from_numpy(np.fft.fftshift(np.fft.fftfreq(self.P, d=self.ds_block)).astype(np.float32)).to(dev)
         fy, fx = torch.meshgrid(freqs, freqs, indexing="ij")
@@ -371,7 +374,6 @@ class PerspectiveSlabFVR(nn.Module):
         self.register_buffer("FX_flat", fx.reshape(-1).contiguous())
         self.register_buffer("FY_flat", fy.reshape(-1).contiguous())
         self._freqs = freqs.contiguous()
-        self._stencil = RT.Stencil(self.F_blk_ri, True, (self.P,) * 3, self._stencil_dtype(dtype), items=self.B)
 
     @staticmethod
     def _stencil_dtype(dtype):
