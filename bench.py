@@ -418,15 +418,14 @@ def _f16_from_f32(eng, vol, dev, torch):
 
     fresh = fvr.TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0, device=dev)
     fresh.to_precision(torch.float16)
-    eng._stencil = fresh._stencil
-    eng.f_vol_5d = fresh.f_vol_5d
+    eng._stencil, eng._pair, eng.f_vol_5d = fresh._stencil, fresh._pair, fresh.f_vol_5d
 
 
 def _pou_roofline(B, P, K, entry, pose_evals_per_s):
     """Whole-step logical bytes per pose-eval of the PoU step: forward = slice gather B P^2 x entry + block-image
     IFFT B P^2 x 12 B + warp K (B x 16 B of taps + 16 B rays / out);
     adjoint = warp 2 x B K x 16 B + IFFT B P^2 x 12 B + slice B P^2 x entry
-    (entry: 64 B f32 / 32 B bf16 stencil entry), over the whole step time."""
+    (entry: 64 B f32 / 32 B bf16 or f16 stencil entry), over the whole step time."""
     peak, peak_kind = _peak_hbm()
     fwd = B * P * P * entry + B * P * P * 12 + K * (B * 16 + 16)
     adj = 2 * B * K * 16 + B * P * P * 12 + B * P * P * entry
@@ -487,7 +486,7 @@ def _pou_leg(torch, dev, flush, warmup, steps):
     from fvr.cone_beam_fvr import PerspectiveSlabFVR
 
     out = {}
-    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
         vol = synthetic.make_ellipsoid_volume(192, SEED)
         m = PerspectiveSlabFVR.from_volume(vol, vox_mm=1.0, grid_blocks=(4, 4, 4), block_res=64, overlap=0.5,
                                            dtype=dt, device=dev)
@@ -644,7 +643,7 @@ def _large_volume_leg(torch, dev, flush, warmup, steps):
         elif name == "f16":  # brick-scaled f16 from the full-precision spectrum, not from the bf16 cast
             fresh = fvr.TorchDiffFVREngine(torch.from_numpy(vol), spacing=sp, pad_factor=2.0, device=dev)
             fresh.to_precision(dt)
-            eng._stencil, eng.f_vol_5d = fresh._stencil, fresh.f_vol_5d
+            eng._stencil, eng._pair, eng.f_vol_5d = fresh._stencil, fresh._pair, fresh.f_vol_5d
             del fresh
         step = BiplanarSpectralNCCStep(eng, f_ap, f_lat, C, warmup=warmup)
         step(poses)

@@ -144,6 +144,35 @@ struct Raw<FVR_F16> {
   uint4 q[2];
   float sc;
 };
+// x-pair storage (16-bit): q[0] = entry ex (the cell's x = 0 corners), q[1] =
+// entry ex + 1 (x = 1), each ordered dz*2 + dy; f16: the scale of their
+// (z, y) slab, which spans every x.
+template <>
+struct Raw<FVR_BF16_PAIR> {
+  uint4 q[2];
+};
+template <>
+struct Raw<FVR_F16_PAIR> {
+  uint4 q[2];
+  float sc;
+};
+
+constexpr bool is_pair(int dt) { return dt == FVR_BF16_PAIR || dt == FVR_F16_PAIR; }
+
+// x-pair entry grid: (D+1)(H+1)(W+2) entries; f16 scales per (z, y) slab of
+// kBrick x kBrick entry rows.
+__device__ __forceinline__ int64_t pair_entries(const Stencil& s) {
+  return static_cast<int64_t>(s.D + 1) * (s.H + 1) * (s.W + 2);
+}
+__device__ __forceinline__ int64_t pair_scales(const Stencil& s) {
+  return static_cast<int64_t>((s.D + kBrick) / kBrick) * ((s.H + kBrick) / kBrick);
+}
+
+// Two 128-bit read-only loads of the 32 contiguous bytes at p (16-byte aligned).
+__device__ __forceinline__ void ldg128x2(const uint4* p, uint4& a, uint4& b) {
+  a = __ldg(p);
+  b = __ldg(p + 1);
+}
 
 // Cell address of p (FP64 voxel coordinates; zero-padding partial or hard cut-off).
 struct Cell {
@@ -352,7 +381,21 @@ __device__ __forceinline__ void tab_decode(const Raw<DT>& r, Sample8& v) {
 // Corners as (re, im) pairs, f16 without its brick scale (as tab_decode).
 template <int DT>
 __device__ __forceinline__ void tab_decode2(const Raw<DT>& r, Sample8c& v) {
-  if constexpr (DT == FVR_F32) {
+  if constexpr (is_pair(DT)) {
+    // corner c = dz*4 + dy*2 + dx: x = 0 corners from q[0], x = 1 from q[1]
+    const uint32_t w0[4] = {r.q[0].x, r.q[0].y, r.q[0].z, r.q[0].w};
+    const uint32_t w1[4] = {r.q[1].x, r.q[1].y, r.q[1].z, r.q[1].w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if constexpr (DT == FVR_BF16_PAIR) {
+        v.c[2 * k] = make_float2(bf_lo(w0[k]), bf_hi(w0[k]));
+        v.c[2 * k + 1] = make_float2(bf_lo(w1[k]), bf_hi(w1[k]));
+      } else {
+        v.c[2 * k] = make_float2(h_lo(w0[k]), h_hi(w0[k]));
+        v.c[2 * k + 1] = make_float2(h_lo(w1[k]), h_hi(w1[k]));
+      }
+    }
+  } else if constexpr (DT == FVR_F32) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       v.c[2 * i] = make_float2(r.q[i].x, r.q[i].y);
@@ -372,7 +415,7 @@ __device__ __forceinline__ void tab_decode2(const Raw<DT>& r, Sample8c& v) {
 
 template <int DT>
 __device__ __forceinline__ float raw_scale(const Raw<DT>& r) {
-  if constexpr (DT == FVR_F16)
+  if constexpr (DT == FVR_F16 || DT == FVR_F16_PAIR)
     return r.sc;
   else
     return 1.f;

@@ -278,6 +278,7 @@ struct SCell {
   int ex, ey, ez;
 };
 
+template <int DT>
 __device__ __forceinline__ SCell sncc_cell(const Stencil& s, int4 ia, float4 fa, int4 ib1, float4 fb) {
   SCell c;
   c.tx = fa.x + fb.x;
@@ -292,14 +293,27 @@ __device__ __forceinline__ SCell sncc_cell(const Stencil& s, int4 ia, float4 fa,
   const bool ok = static_cast<unsigned>(c.ex) <= static_cast<unsigned>(s.W) &&
                   static_cast<unsigned>(c.ey) <= static_cast<unsigned>(s.H) &&
                   static_cast<unsigned>(c.ez) <= static_cast<unsigned>(s.D);
-  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + 1) + c.ex : -1;
+  // x-pair storage: W + 2 entries per x row, the cell's two at e and e + 1
+  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + (is_pair(DT) ? 2 : 1)) + c.ex : -1;
   return c;
 }
 
 // Entry load of cell c (zeros when e < 0); f16: the brick scale, unapplied.
 template <int DT>
 __device__ __forceinline__ void sncc_load(const Stencil& s, const SCell& c, Raw<DT>& r) {
-  if constexpr (DT == FVR_F32) {
+  if constexpr (is_pair(DT)) {
+    if (c.e < 0 || !fvr_checked(c.e + 1, pair_entries(s), kSiteStencilEntry)) {
+      r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
+      if constexpr (DT == FVR_F16_PAIR) r.sc = 0.f;
+      return;
+    }
+    ldg128x2(static_cast<const uint4*>(s.data) + static_cast<int64_t>(c.e), r.q[0], r.q[1]);
+    if constexpr (DT == FVR_F16_PAIR) {
+      const unsigned by = static_cast<unsigned>(s.H + kBrick) / kBrick;
+      const unsigned si = (static_cast<unsigned>(c.ez) / kBrick) * by + static_cast<unsigned>(c.ey) / kBrick;
+      r.sc = fvr_checked(si, pair_scales(s), kSiteStencilScale) ? __ldg(s.scales + si) : 0.f;
+    }
+  } else if constexpr (DT == FVR_F32) {
     if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -389,7 +403,7 @@ __device__ __forceinline__ void sncc_run(const SnccArgs& a, const SnccTab& tab, 
         const int ig = i + g * rpp;
         const bool ok = ig < row_end;
         const int rn = R + (ok ? ig : row_begin) - row_begin;
-        SCell cell = sncc_cell(a.st, tab.idx[rn], tab.frac[rn], ib, fb);
+        SCell cell = sncc_cell<DT>(a.st, tab.idx[rn], tab.frac[rn], ib, fb);
         if (!ok) cell.e = -1;
         sncc_load<DT>(a.st, cell, raw[g]);
         const int q = ig * R + j;
@@ -408,7 +422,7 @@ __device__ __forceinline__ void sncc_run(const SnccArgs& a, const SnccTab& tab, 
         if (tz >= 1.f) tz -= 1.f;
         // f16: the brick scale rides on the high-pass weight (every moment is
         // linear in h S or quadratic in it) instead of rescaling 8 values
-        const float h = DT == FVR_F16 ? hs[g] * raw_scale(raw[g]) : hs[g];
+        const float h = (DT == FVR_F16 || DT == FVR_F16_PAIR) ? hs[g] * raw_scale(raw[g]) : hs[g];
         sncc_accumulate<DT, GRAD, NM>(raw[g], tx, ty, tz, tab.kph[rn], kb, Ts[g], h, acc);
       }
     }
@@ -778,11 +792,14 @@ __global__ void tc_adjoint_grad_kernel(const double* __restrict__ part, int tile
   for (int k = 0; k < 6; ++k) o[k] = accumulate ? o[k] + r[k] : r[k];
 }
 
+// pair_ok: the caller's kernels also read the x-pair storage (the moments kernels).
 static int stencil_from(int dtype, const void* data, const float* scales, int64_t D, int64_t H, int64_t W,
-                        Stencil* s) {
+                        Stencil* s, bool pair_ok = false) {
   if (!data || D < 1 || H < 1 || W < 1 || D > 8192 || H > 8192 || W > 8192) return FVR_ERR_ARG;
-  if (dtype != FVR_F32 && dtype != FVR_BF16 && dtype != FVR_F16) return FVR_ERR_DTYPE;
-  if (dtype == FVR_F16 && !scales) return FVR_ERR_ARG;
+  if (dtype != FVR_F32 && dtype != FVR_BF16 && dtype != FVR_F16 &&
+      !(pair_ok && (dtype == FVR_BF16_PAIR || dtype == FVR_F16_PAIR)))
+    return FVR_ERR_DTYPE;
+  if ((dtype == FVR_F16 || dtype == FVR_F16_PAIR) && !scales) return FVR_ERR_ARG;
   if ((reinterpret_cast<uintptr_t>(data) & 15) != 0) return FVR_ERR_ARG;
   *s = Stencil{data, scales, static_cast<int>(D), static_cast<int>(H), static_cast<int>(W), dtype};
   return FVR_OK;
@@ -869,7 +886,7 @@ static int sncc_setup(int dtype, const void* stencil, const float* scales, int64
                       const float* hp, const float* lin, int64_t R, double kappa, int variant, SnccArgs* a,
                       dim3* grid, int64_t* smem) {
   Stencil st;
-  int rc = stencil_from(dtype, stencil, scales, D, H, W, &st);
+  int rc = stencil_from(dtype, stencil, scales, D, H, W, &st, true);
   if (rc) return rc;
   if (!poses || !views || !ftargs || !lin || C < 1 || R < 1 || C > 65535) return FVR_ERR_ARG;
   if (nviews < 1 || nviews > kMaxViews || R * R > (int64_t)1 << 30) return FVR_ERR_ARG;
@@ -1028,6 +1045,8 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
     case FVR_F32: FVR_SNCC(FVR_F32)
     case FVR_BF16: FVR_SNCC(FVR_BF16)
     case FVR_F16: FVR_SNCC(FVR_F16)
+    case FVR_BF16_PAIR: FVR_SNCC(FVR_BF16_PAIR)
+    case FVR_F16_PAIR: FVR_SNCC(FVR_F16_PAIR)
   }
 #undef FVR_SNCC
   FVR_LAUNCH_CHECK();
@@ -1070,6 +1089,8 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
     case FVR_F32: launch_sncc<FVR_F32, true>(variant, grid, (int)smem, s, a, true); break;
     case FVR_BF16: launch_sncc<FVR_BF16, true>(variant, grid, (int)smem, s, a, true); break;
     case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_BF16_PAIR: launch_sncc<FVR_BF16_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_F16_PAIR: launch_sncc<FVR_F16_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
   }
   FVR_LAUNCH_CHECK();
   launch_sncc_final(s, a);
@@ -1201,6 +1222,8 @@ int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const floa
     case FVR_F32: launch_sncc<FVR_F32, true>(variant, grid, (int)smem, s, a, true); break;
     case FVR_BF16: launch_sncc<FVR_BF16, true>(variant, grid, (int)smem, s, a, true); break;
     case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_BF16_PAIR: launch_sncc<FVR_BF16_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_F16_PAIR: launch_sncc<FVR_F16_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
   }
   FVR_LAUNCH_CHECK();
   launch_sncc_final(s, a);

@@ -171,6 +171,39 @@ class Stencil:
         return (self.code, L.ptr(self.data), L.ptr(self.scales), D, H, W)
 
 
+class PairStencil:
+    """x-pair copy of a centred spectrum for the spectral-NCC moments kernels
+    (16-bit only; see fvr_stencil_pair_build in include/fvr_b200.h): half the
+    bytes of the stencil, a sample's two entries side by side."""
+
+    def __init__(self, master, planar, dims, dtype):
+        dev = L.require_cuda(master)
+        D, H, W = (int(s) for s in dims)
+        self.dims = (D, H, W)
+        self.dtype = dtype
+        if dtype == torch.float16:
+            self.code = L.F16_PAIR_
+        elif dtype == torch.bfloat16:
+            self.code = L.BF16_PAIR_
+        else:
+            raise L.FvrError(f"x-pair storage is 16-bit only, not {dtype}")
+        nbytes = L.query("fvr_stencil_pair_bytes", D, H, W, self.code)
+        self.data = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        self.scales = None
+        scratch = None
+        if self.code == L.F16_PAIR_:
+            n = L.query("fvr_stencil_pair_scale_count", D, H, W)
+            self.scales = torch.empty(n, dtype=torch.float32, device=dev)
+            scratch = torch.empty(n, dtype=torch.int32, device=dev)
+        m = master.contiguous()
+        L.call("fvr_stencil_pair_build", L.ptr(m), L.dtype_code(m.dtype), int(planar), D, H, W, self.code,
+               L.ptr(self.data), L.ptr(self.scales), L.ptr(scratch), L.stream_ptr(dev))
+
+    def args(self):
+        D, H, W = self.dims
+        return (self.code, L.ptr(self.data), L.ptr(self.scales), D, H, W)
+
+
 def kappa(out_res, spacing0):
     """-2 pi / (R * spacing + 1e-6): phase = kappa * (ku tx + kv ty) (torch_engine.py:227-232)."""
     return -2.0 * math.pi / (out_res * float(spacing0) + 1e-6)

@@ -147,7 +147,7 @@ class BiplanarSpectralNCCStep:
     def __init__(self, engine, f_targ_ap, f_targ_lat, n_candidates, high_pass=True, cutoff_sigma=4.0, graph=True,
                  warmup=3, capture_context=None, host_io=False):
         self.engine = engine
-        self._stencil = engine._stencil
+        self._stencil = (engine._stencil, engine._pair)  # the storage the captured kernels read
         self.f_ap = f_targ_ap
         self.f_lat = f_targ_lat
         self.hp = bool(high_pass)

@@ -52,7 +52,7 @@ def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
     dev = eng._dev
     C = int(p.shape[0])
     nv = len(views)
-    st = eng._stencil
+    st = eng._sncc_storage()
     ws_bytes = L.query("fvr_tc_sncc_workspace", C, R, nv)
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
     mom = torch.empty((nv, C, int(L.query("fvr_tc_sncc_mom_stride"))), dtype=torch.float64, device=dev)
@@ -115,7 +115,7 @@ def _fused_call(eng, C, R, views, ftargs, hp, p):
     complex64 on the engine's device are used in place and the preparation
     is cached by their addresses; others are converted for this call only."""
     dev = eng._dev
-    st = eng._stencil
+    st = eng._sncc_storage()
     nv = len(views)
     direct = all(f.is_cuda and f.device == dev and f.dtype == torch.complex64 and f.is_contiguous() for f in ftargs)
     key = (C, R, tuple(views), tuple(int(f.data_ptr()) for f in ftargs), 0 if hp is None else int(hp.data_ptr()),
@@ -421,9 +421,19 @@ class TorchDiffFVREngine(nn.Module):
         planar = torch.view_as_real(spec).permute(3, 0, 1, 2).unsqueeze(0).to(torch.float32).contiguous()
         del spec
         self.register_buffer("f_vol_5d", planar.to(dtype=dtype))
-        self._stencil = RT.Stencil(self.f_vol_5d[0], True, self.pad_shape, self._stencil_dtype(dtype))
+        # storage copies come from the float32 spectrum (f16 takes its brick scales from it)
+        self._stencil = RT.Stencil(planar[0], True, self.pad_shape, self._stencil_dtype(dtype))
+        self._pair = (RT.PairStencil(planar[0], True, self.pad_shape, dtype)
+                      if dtype in (torch.float16, torch.bfloat16) else None)
+        self.use_pair_storage = True  # 16-bit: the spectral-NCC moments read the x-pair copy
+        del planar
         self._fused_ws = {}  # (C, R, views, device) -> workspace of the fused value_and_grad
         self._fused_calls = {}  # prepared launches of the fused value_and_grad
+
+    def _sncc_storage(self):
+        """The spectrum copy the spectral-NCC moments kernels read: the x-pair
+        copy of 16-bit storage (unless ``use_pair_storage`` is off), else the stencil."""
+        return self._pair if (self._pair is not None and self.use_pair_storage) else self._stencil
 
     @staticmethod
     def _stencil_dtype(dtype):
@@ -443,6 +453,10 @@ class TorchDiffFVREngine(nn.Module):
         """
         src = self.f_vol_5d[0]
         self._stencil = RT.Stencil(src, True, self.pad_shape, self._stencil_dtype(dtype))
+        # 16-bit storage: the spectral-NCC moments kernels read an x-pair copy
+        # (half the stencil's bytes; the image path keeps the stencil)
+        self._pair = (RT.PairStencil(src, True, self.pad_shape, dtype)
+                      if dtype in (torch.float16, torch.bfloat16) else None)
         self.f_vol_5d = self.f_vol_5d.to(dtype=dtype)
         self._compiled_forward_core = None
         self._compiled_spectral_ncc = None

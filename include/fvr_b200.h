@@ -34,7 +34,9 @@ typedef enum {
   FVR_ERR_CUDA = 5         /* launch or driver error (cudaGetLastError)     */
 } fvr_status;
 
-typedef enum { FVR_F32 = 0, FVR_BF16 = 1, FVR_F16 = 2, FVR_F64 = 3 } fvr_dtype;
+/* FVR_BF16_PAIR / FVR_F16_PAIR name the x-pair spectrum storage (below),
+ * accepted by the spectral-NCC moments entry points only. */
+typedef enum { FVR_F32 = 0, FVR_BF16 = 1, FVR_F16 = 2, FVR_F64 = 3, FVR_BF16_PAIR = 4, FVR_F16_PAIR = 5 } fvr_dtype;
 
 const char* fvr_status_string(int status);
 int fvr_version(void);
@@ -80,7 +82,7 @@ int fvr_fft2d(const void* in, int in_real, int64_t batch, int64_t n0, int64_t n1
  * entries, each the 8 complex corners of one trilinear cell (corners outside
  * the volume are zero).  f32: 64 B per entry; bf16 / f16: 32 B per entry, f16
  * with a power-of-two scale per 16^3-entry brick.  Built from a "master"
- * spectrum in f32 or bf16, planar [2][D][H][W] (master_planar = 1, the
+ * spectrum in f32, bf16 or f16, planar [2][D][H][W] (master_planar = 1, the
  * reference's f_vol_5d[0]) or interleaved [D][H][W][2] (master_planar = 0).  Storage for the
  * spectrum buffer f_vol_5d of src/fvr/torch_engine.py:83-88 and its
  * to_precision cast (:90-95). */
@@ -91,6 +93,20 @@ int64_t fvr_stencil_scale_count(int64_t D, int64_t H, int64_t W);
  * scratch_max: items * fvr_stencil_scale_count() uint32 (f16 only, else NULL). */
 int fvr_stencil_build(const void* master, int master_dtype, int master_planar, int64_t items, int64_t D, int64_t H,
                       int64_t W, int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream);
+/* x-pair layout of the same spectrum, 16-bit only (out_dtype FVR_BF16_PAIR or
+ * FVR_F16_PAIR): (D+1)(H+1)(W+2) entries of 16 B; entry (ez, ey, ex) holds the
+ * 4 complex values of voxel column x = ex-1 at (y, z) = (ey-1+dy, ez-1+dz),
+ * ordered dz*2 + dy (zero outside the volume).  A trilinear sample in the
+ * stencil cell (ez, ey, ex) reads entries ex and ex+1: 32 contiguous bytes,
+ * half the storage of the stencil, so the samples of many slices meet in
+ * fewer sectors.  f16: a power-of-two scale per slab of 16 x 16 (z, y)
+ * entry rows over the whole x extent, so a sample's two entries share it
+ * (fvr_stencil_pair_scale_count floats).  Same master formats as
+ * fvr_stencil_build, one spectrum; scratch_max as there (f16 only). */
+int64_t fvr_stencil_pair_bytes(int64_t D, int64_t H, int64_t W, int dtype);
+int64_t fvr_stencil_pair_scale_count(int64_t D, int64_t H, int64_t W);
+int fvr_stencil_pair_build(const void* master, int master_dtype, int master_planar, int64_t D, int64_t H, int64_t W,
+                           int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream);
 
 /* --------------------------------------- drop-in trilinear slice gather -- */
 /* fourier_slice_3d on the reference layout vol[B][2][D][H][W] (dtype f32 /
@@ -128,9 +144,11 @@ int64_t fvr_tc_sncc_mom_stride(void);
  * with_grad also the 14 pose-gradient moments.  Partial sums (one record per
  * CTA and (candidate, view) it covers) go to `workspace`.
  * lin = torch.linspace(-1, 1, R).  `variant` in [0, fvr_tc_sncc_variants())
- * selects the launch shape (tile grid or one equal sample range per resident
- * CTA, samples in flight per thread, resident CTAs per SM); results do not
- * depend on it beyond float summation order.
+ * selects the launch shape (rows in flight per thread, resident CTAs per SM);
+ * results do not depend on it beyond float summation order.  dtype: the
+ * stencil storage (FVR_F32 / FVR_BF16 / FVR_F16) or the x-pair storage
+ * (FVR_BF16_PAIR / FVR_F16_PAIR; stencil = its data, scales = its slab
+ * scales), in this and the two value-and-gradient entry points below.
  * Replaces TorchDiffFVREngine._spectral_ncc_core / forward_spectral_ncc,
  * src/fvr/torch_engine.py:269-307 (the gather of :176-234 included). */
 int fvr_tc_sncc_variants(void);

@@ -379,6 +379,7 @@ def test_fused_value_and_grad_every_variant_repeatable(big, monkeypatch):
     l1.backward()
     for variant in range(L.load().fvr_tc_sncc_variants()):
         monkeypatch.setenv("FVR_SNCC_FUSED_VARIANT", str(variant))
+        eng._fused_calls.clear()  # prepared launches keep the variant they were made with
         la, ga = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
         lb, gb = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
         assert torch.equal(la, lb) and torch.equal(ga, gb), variant
@@ -401,10 +402,12 @@ def test_fused_variants_agree_on_ragged_shapes(big, monkeypatch, C, R):
     fa = eng.prepare_spectral_target(eng(tp, view="ap", out_res=R))
     fl = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=R))
     monkeypatch.setenv("FVR_SNCC_FUSED_VARIANT", "0")
+    eng._fused_calls.clear()  # prepared launches keep the variant they were made with
     l0, g0 = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
     scale = float(g0.abs().max())
     for variant in range(1, L.load().fvr_tc_sncc_variants()):
         monkeypatch.setenv("FVR_SNCC_FUSED_VARIANT", str(variant))
+        eng._fused_calls.clear()
         la, ga = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
         assert abs(float(la) - float(l0)) < 2e-6, variant
         assert torch.allclose(ga, g0, rtol=1e-4, atol=1e-5 * scale), variant
@@ -530,3 +533,87 @@ def test_three_kernel_abi_path_matches_fused(big, g):
     torch.cuda.synchronize()
     assert torch.allclose(loss3, lossf, rtol=1e-6, atol=1e-7)
     assert rel_l2(grad3.cpu().numpy(), gradf.cpu().numpy()) < 1e-5
+
+
+def _bf16_round(x):
+    """float32 -> bfloat16 (round to nearest even) as float32, in numpy."""
+    b = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) >> 16
+    return (b.astype(np.uint32) << 16).view(np.float32)
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+def test_pair_storage_build_matches_restatement(dtype):
+    """fvr_stencil_pair_build on a small planar spectrum: every 16-byte entry
+    (ez, ey, ex) holds voxel column x = ex - 1 at (y, z) = (ey - 1 + dy,
+    ez - 1 + dz), zero outside; bf16 rounded to nearest, f16 divided by its
+    (z, y) slab's power-of-two scale (2^(e - 15) for the slab maximum
+    m = f 2^e; a slab is 16 x 16 entry rows over every x)."""
+    import fvr._runtime as RT
+
+    D, H, W = 5, 19, 18  # a slab boundary along y (H + 1 = 20 > 16)
+    rng = np.random.default_rng(3)
+    master = (rng.standard_normal((2, D, H, W)) * np.exp(rng.uniform(-3, 6, (2, D, H, W)))).astype(np.float32)
+    ps = RT.PairStencil(torch.from_numpy(master).cuda(), True, (D, H, W), dtype)
+    raw = ps.data.cpu().numpy().view(np.uint16).reshape(D + 1, H + 1, W + 2, 4, 2)
+    want = np.zeros((D + 1, H + 1, W + 2, 4, 2), np.float32)
+    for ez in range(D + 1):
+        for ey in range(H + 1):
+            for ex in range(W + 2):
+                x = ex - 1
+                for k in range(4):
+                    z, y = ez - 1 + (k >> 1), ey - 1 + (k & 1)
+                    if 0 <= z < D and 0 <= y < H and 0 <= x < W:
+                        want[ez, ey, ex, k] = master[:, z, y, x]
+    if dtype == torch.bfloat16:
+        got = (raw.astype(np.uint32) << 16).view(np.float32)
+        assert np.array_equal(got, _bf16_round(want))
+    else:
+        sc = ps.scales.cpu().numpy()
+        bz, by = (D + 16) // 16, (H + 16) // 16
+        assert sc.size == bz * by
+        m = np.abs(want).max(axis=(2, 3, 4))
+        for iz in range(bz):
+            for iy in range(by):
+                e = np.frexp(np.float32(m[16 * iz:16 * iz + 16, 16 * iy:16 * iy + 16].max()))[1]
+                assert sc[iz * by + iy] == np.float32(2.0 ** (int(e) - 15))
+        scale = np.repeat(np.repeat(sc.reshape(bz, by), 16, 0), 16, 1)[:D + 1, :H + 1]
+        exp = (want / scale[:, :, None, None, None]).astype(np.float16)
+        assert np.array_equal(raw.view(np.float16), exp)
+
+
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("C,R", [(64, 128), (7, 37), (300, 16)])
+def test_pair_storage_moments_match_stencil(big, dtype, C, R):
+    """The spectral-NCC moments read the x-pair copy of 16-bit storage: loss
+    and pose gradient agree with the stencil copy of the same storage to the
+    storage's rounding (both are rounded once from the float32 spectrum; f16
+    scaled over different entry groups), for every launch variant."""
+    import os
+
+    import fvr._lib as L
+    from fvr.torch_engine import TorchDiffFVREngine
+
+    vol = big[0]
+    eng = TorchDiffFVREngine(torch.from_numpy(vol), spacing=(1.0, 1.0, 1.0), pad_factor=2.0).to_precision(dtype)
+    assert eng._pair is not None and eng._sncc_storage() is eng._pair
+    poses = _t(tc.make_poses(C, 31))
+    tp = _t(tc.make_poses(1, 32))
+    fa = eng.prepare_spectral_target(eng(tp, view="ap", out_res=R))
+    fl = eng.prepare_spectral_target(eng(tp, view="lateral", out_res=R))
+    eng.use_pair_storage = False
+    l0, g0 = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
+    eng.use_pair_storage = True
+    scale = float(g0.abs().max())
+    tol = 2e-3 if dtype == torch.float16 else 2e-2
+    try:
+        for variant in range(L.load().fvr_tc_sncc_variants()):
+            os.environ["FVR_SNCC_FUSED_VARIANT"] = str(variant)
+            eng._fused_calls.clear()  # prepared launches keep the variant they were made with
+            l1, g1 = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
+            assert abs(float(l1) - float(l0)) < tol * max(1.0, abs(float(l0))), variant
+            assert float((g1 - g0).norm() / g0.norm()) < tol, variant
+            assert float((g1 - g0).abs().max()) < 10 * tol * scale, variant
+    finally:
+        os.environ.pop("FVR_SNCC_FUSED_VARIANT", None)
+    del eng
