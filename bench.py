@@ -301,13 +301,13 @@ def run_b200(args, torch):
         # 8-corner gather of the forward pass and again of the adjoint (4 B a
         # corner), the 8 B target and a 4 B brick scale.  The kernel fuses the
         # adjoint into the forward pass and reads each 32 B entry once, so it
-        # moves fewer bytes (min_bytes: entry + target; traffic: ncu's DRAM bytes)
+        # moves fewer bytes (min_bytes: 32 B of spectrum + target; traffic: ncu's DRAM bytes)
         samples = 2 * CANDIDATES * OUT_RES * OUT_RES
         alg_bytes = samples * (8 * 4 + 8 * 4 + 8 + 4)
         min_bytes = samples * (32 + 8)
         achieved = alg_bytes / (kern_avg_ms * 1e-3) / 1e9
         traffic, ncu = None, {}
-        tf = REPO / "profiles" / "tc_sncc_moments_f16_128cube_64cand_traffic.txt"
+        tf = REPO / "profiles" / "tc_sncc_moments_f16pair_128cube_64cand_traffic.txt"
         if tf.exists():
             for line in tf.read_text().splitlines():
                 if ":" in line and not line.startswith("#"):
@@ -336,9 +336,10 @@ def run_b200(args, torch):
                 "candidates_per_gpu": CANDIDATES,
                 "views": 2,
                 "out_res": OUT_RES,
-                "spectrum_storage": "f16 stencil with per-16^3-brick power-of-two scales (32-byte entry of 8 "
-                                    "complex corners); f32 interpolation, positions and phases from fp64 "
-                                    "per-row/column tables, fp64 reductions",
+                "spectrum_storage": "f16 with power-of-two scales; the moments kernel reads the x-pair copy (two "
+                                    "16-byte entries of 4 complex (y, z) corners side by side per sample, "
+                                    "scale per 16x16 (z, y) slab); f32 interpolation, positions and phases "
+                                    "from fp64 per-row/column tables, fp64 reductions",
                 "step": "CUDA-graph replay of two kernels: gather + NCC/pose moments for both views, then the "
                         "fp64 finalize, pose gradient and losses as its programmatic dependent launch; the "
                         "roofline's kernel time comes from a second capture with event nodes around the kernels",
@@ -365,7 +366,7 @@ def run_b200(args, torch):
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6.65 TB/s",
                 "traffic": traffic,
-                "ncu_capture": {"source": "profiles/tc_sncc_moments_f16_128cube_64cand.md (cold, serialised)",
+                "ncu_capture": {"source": "profiles/tc_sncc_moments_f16pair_128cube_64cand.md (cold, serialised)",
                                 "kernel_us": ncu.get("ncu_kernel_us"),
                                 "dram_pct_of_peak": ncu.get("dram_pct_of_peak"),
                                 "l2_bytes_per_launch": ncu.get("l2_bytes_per_launch"),
@@ -378,7 +379,8 @@ def run_b200(args, torch):
                 "min_bytes_per_launch": min_bytes,
                 "achieved_min_bytes_gbs": min_bytes / (kern_avg_ms * 1e-3) / 1e9,
                 "frac_min_bytes": min_bytes / (kern_avg_ms * 1e-3) / 1e9 / peak,
-                "min_bytes_note": "what the fused kernel must read: one 32 B stencil entry + 8 B target per sample",
+                "min_bytes_note": "what the fused kernel must read: 32 B of spectrum (two x-pair entries) + 8 B "
+                                  "target per sample",
                 "kernel_ms": kern_avg_ms,
                 "kernel_launches_timed": len(f16["kern_ms"]),
             },
