@@ -158,12 +158,15 @@ __host__ __device__ inline PairGrid pair_grid(int D, int H, int W) {
 }
 
 template <typename MT>
-__global__ void pair_slab_max_kernel(const MT* __restrict__ m, int64_t plane, int D, int H, int W,
-                                     unsigned int* __restrict__ smax) {
+__global__ void pair_slab_max_kernel(const MT* __restrict__ m0, int64_t plane, int64_t items, int D, int H, int W,
+                                     unsigned int* __restrict__ smax0) {
   const PairGrid g = pair_grid(D, H, W);
-  const int64_t n = static_cast<int64_t>(g.ed) * g.eh * g.ew;
-  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  const int64_t n1 = static_cast<int64_t>(g.ed) * g.eh * g.ew;
+  const int64_t nb1 = static_cast<int64_t>((g.ed + kBrick - 1) / kBrick) * g.by;
+  for (int64_t ee = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; ee < n1 * items;
+       ee += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t item = ee / n1, e = ee - item * n1;
+    const MT* m = m0 + item * 2 * static_cast<int64_t>(D) * H * W;
     const int ex = static_cast<int>(e % g.ew), ey = static_cast<int>((e / g.ew) % g.eh);
     const int ez = static_cast<int>(e / (static_cast<int64_t>(g.ew) * g.eh));
     float re[4], im[4];
@@ -171,35 +174,44 @@ __global__ void pair_slab_max_kernel(const MT* __restrict__ m, int64_t plane, in
     float mx = 0.f;
 #pragma unroll
     for (int k = 0; k < 4; ++k) mx = fmaxf(mx, fmaxf(fabsf(re[k]), fabsf(im[k])));
-    atomicMax(smax + g.slab(ez, ey), __float_as_uint(mx));  // non-negative floats order like their bits
+    atomicMax(smax0 + item * nb1 + g.slab(ez, ey), __float_as_uint(mx));  // non-negative floats order like their bits
   }
 }
 
 template <typename MT, int DT>
-__global__ void pair_build_kernel(const MT* __restrict__ m, int64_t plane, int D, int H, int W,
-                                  uint4* __restrict__ out, const float* __restrict__ scales) {
+__global__ void pair_build_kernel(const MT* __restrict__ m0, int64_t plane, int64_t items, int D, int H, int W,
+                                  void* __restrict__ out0, const float* __restrict__ scales0) {
   const PairGrid g = pair_grid(D, H, W);
-  const int64_t n = static_cast<int64_t>(g.ed) * g.eh * g.ew;
-  for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n;
-       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+  const int64_t n1 = static_cast<int64_t>(g.ed) * g.eh * g.ew;
+  const int64_t nb1 = static_cast<int64_t>((g.ed + kBrick - 1) / kBrick) * g.by;
+  for (int64_t ee = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; ee < n1 * items;
+       ee += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t item = ee / n1, e = ee - item * n1;
+    const MT* m = m0 + item * 2 * static_cast<int64_t>(D) * H * W;
     const int ex = static_cast<int>(e % g.ew), ey = static_cast<int>((e / g.ew) % g.eh);
     const int ez = static_cast<int>(e / (static_cast<int64_t>(g.ew) * g.eh));
     float re[4], im[4];
     pair_values(m, plane, D, H, W, ez, ey, ex, re, im);
-    uint32_t w[4];
-    if constexpr (DT == FVR_BF16_PAIR) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        w[k] = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(re[k]))) |
-               (static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(im[k]))) << 16);
+    if constexpr (DT == FVR_F32_PAIR) {
+      float4* p = static_cast<float4*>(out0) + (item * n1 + e) * 2;
+      p[0] = make_float4(re[0], im[0], re[1], im[1]);
+      p[1] = make_float4(re[2], im[2], re[3], im[3]);
     } else {
-      const float inv = 1.f / scales[g.slab(ez, ey)];
+      uint32_t w[4];
+      if constexpr (DT == FVR_BF16_PAIR) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        w[k] = static_cast<uint32_t>(__half_as_ushort(__float2half_rn(re[k] * inv))) |
-               (static_cast<uint32_t>(__half_as_ushort(__float2half_rn(im[k] * inv))) << 16);
+        for (int k = 0; k < 4; ++k)
+          w[k] = static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(re[k]))) |
+                 (static_cast<uint32_t>(__bfloat16_as_ushort(__float2bfloat16_rn(im[k]))) << 16);
+      } else {
+        const float inv = 1.f / scales0[item * nb1 + g.slab(ez, ey)];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          w[k] = static_cast<uint32_t>(__half_as_ushort(__float2half_rn(re[k] * inv))) |
+                 (static_cast<uint32_t>(__half_as_ushort(__float2half_rn(im[k] * inv))) << 16);
+      }
+      static_cast<uint4*>(out0)[item * n1 + e] = make_uint4(w[0], w[1], w[2], w[3]);
     }
-    out[e] = make_uint4(w[0], w[1], w[2], w[3]);
   }
 }
 
@@ -314,8 +326,11 @@ int fvr_stencil_build(const void* master, int master_dtype, int master_planar, i
 }
 
 int64_t fvr_stencil_pair_bytes(int64_t D, int64_t H, int64_t W, int dtype) {
-  if (D < 1 || H < 1 || W < 1 || (dtype != FVR_BF16_PAIR && dtype != FVR_F16_PAIR)) return 0;
-  return (D + 1) * (H + 1) * (W + 2) * 16;
+  if (D < 1 || H < 1 || W < 1) return 0;
+  const int64_t n = (D + 1) * (H + 1) * (W + 2);
+  if (dtype == FVR_BF16_PAIR || dtype == FVR_F16_PAIR) return n * 16;
+  if (dtype == FVR_F32_PAIR) return n * 32;
+  return 0;
 }
 
 int64_t fvr_stencil_pair_scale_count(int64_t D, int64_t H, int64_t W) {
@@ -323,39 +338,50 @@ int64_t fvr_stencil_pair_scale_count(int64_t D, int64_t H, int64_t W) {
   return cdiv64(D + 1, kBrick) * cdiv64(H + 1, kBrick);
 }
 
-int fvr_stencil_pair_build(const void* master, int master_dtype, int master_planar, int64_t D, int64_t H, int64_t W,
-                           int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream) {
-  if (!master || !out || D < 1 || H < 1 || W < 1 || D > 8192 || H > 8192 || W > 8192) return FVR_ERR_ARG;
-  if ((reinterpret_cast<uintptr_t>(out) & 15) != 0) return FVR_ERR_ARG;
-  if (out_dtype != FVR_BF16_PAIR && out_dtype != FVR_F16_PAIR) return FVR_ERR_DTYPE;
+int fvr_stencil_pair_build(const void* master, int master_dtype, int master_planar, int64_t items, int64_t D,
+                           int64_t H, int64_t W, int out_dtype, void* out, float* scales, unsigned int* scratch_max,
+                           void* stream) {
+  if (!master || !out || items < 1 || D < 1 || H < 1 || W < 1 || D > 8192 || H > 8192 || W > 8192)
+    return FVR_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(out) & 31) != 0) return FVR_ERR_ARG;
+  if (out_dtype != FVR_BF16_PAIR && out_dtype != FVR_F16_PAIR && out_dtype != FVR_F32_PAIR) return FVR_ERR_DTYPE;
   if (master_dtype != FVR_F32 && master_dtype != FVR_BF16 && master_dtype != FVR_F16) return FVR_ERR_DTYPE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int64_t n = (D + 1) * (H + 1) * (W + 2);
+  const int64_t n = (D + 1) * (H + 1) * (W + 2) * items;
   const int64_t nblk = cdiv64(n, 256);
   const unsigned grid = static_cast<unsigned>(nblk < 148 * 64 ? nblk : 148 * 64);
   const int d = (int)D, h = (int)H, w = (int)W;
   const int64_t plane = master_planar ? D * H * W : 0;
   if (out_dtype == FVR_F16_PAIR) {
     if (!scales || !scratch_max) return FVR_ERR_ARG;
-    const int64_t nb = fvr_stencil_pair_scale_count(D, H, W);
+    const int64_t nb = fvr_stencil_pair_scale_count(D, H, W) * items;
     if (cudaMemsetAsync(scratch_max, 0, nb * sizeof(unsigned int), s) != cudaSuccess) return FVR_ERR_CUDA;
     if (master_dtype == FVR_F32)
-      pair_slab_max_kernel<float><<<grid, 256, 0, s>>>(static_cast<const float*>(master), plane, d, h, w, scratch_max);
+      pair_slab_max_kernel<float>
+          <<<grid, 256, 0, s>>>(static_cast<const float*>(master), plane, items, d, h, w, scratch_max);
     else if (master_dtype == FVR_BF16)
       pair_slab_max_kernel<__nv_bfloat16>
-          <<<grid, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(master), plane, d, h, w, scratch_max);
+          <<<grid, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(master), plane, items, d, h, w, scratch_max);
     else
-      pair_slab_max_kernel<__half><<<grid, 256, 0, s>>>(static_cast<const __half*>(master), plane, d, h, w,
-                                                        scratch_max);
+      pair_slab_max_kernel<__half>
+          <<<grid, 256, 0, s>>>(static_cast<const __half*>(master), plane, items, d, h, w, scratch_max);
     stencil_scale_kernel<<<static_cast<unsigned>(cdiv64(nb, 256)), 256, 0, s>>>(scratch_max, scales, nb);
   }
 #define FVR_PAIR(MT)                                                                                          \
-  if (out_dtype == FVR_F16_PAIR)                                                                              \
-    pair_build_kernel<MT, FVR_F16_PAIR><<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, d, h, w,  \
-                                                             static_cast<uint4*>(out), scales);                \
-  else                                                                                                        \
-    pair_build_kernel<MT, FVR_BF16_PAIR><<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, d, h, w, \
-                                                              static_cast<uint4*>(out), nullptr);
+  switch (out_dtype) {                                                                                        \
+    case FVR_F16_PAIR:                                                                                        \
+      pair_build_kernel<MT, FVR_F16_PAIR>                                                                     \
+          <<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, items, d, h, w, out, scales);           \
+      break;                                                                                                  \
+    case FVR_BF16_PAIR:                                                                                       \
+      pair_build_kernel<MT, FVR_BF16_PAIR>                                                                    \
+          <<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, items, d, h, w, out, nullptr);          \
+      break;                                                                                                  \
+    default:                                                                                                  \
+      pair_build_kernel<MT, FVR_F32_PAIR>                                                                     \
+          <<<grid, 256, 0, s>>>(static_cast<const MT*>(master), plane, items, d, h, w, out, nullptr);          \
+      break;                                                                                                  \
+  }
   if (master_dtype == FVR_F32) {
     FVR_PAIR(float)
   } else if (master_dtype == FVR_BF16) {

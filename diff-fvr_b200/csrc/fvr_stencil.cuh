@@ -156,8 +156,13 @@ struct Raw<FVR_F16_PAIR> {
   uint4 q[2];
   float sc;
 };
+// f32 x-pair: q[0..1] = entry ex, q[2..3] = entry ex + 1 (two complex each).
+template <>
+struct Raw<FVR_F32_PAIR> {
+  float4 q[4];
+};
 
-constexpr bool is_pair(int dt) { return dt == FVR_BF16_PAIR || dt == FVR_F16_PAIR; }
+constexpr bool is_pair(int dt) { return dt == FVR_BF16_PAIR || dt == FVR_F16_PAIR || dt == FVR_F32_PAIR; }
 
 // x-pair entry grid: (D+1)(H+1)(W+2) entries; f16 scales per (z, y) slab of
 // kBrick x kBrick entry rows.
@@ -172,6 +177,35 @@ __device__ __forceinline__ int64_t pair_scales(const Stencil& s) {
 __device__ __forceinline__ void ldg128x2(const uint4* p, uint4& a, uint4& b) {
   a = __ldg(p);
   b = __ldg(p + 1);
+}
+
+// The two x-pair entries of cell index e (entry ex of its row; e + 1 is
+// entry ex + 1), f16 with the scale of the cell's (z, y) slab; zeros and a
+// zero scale when e < 0 or (checked build) out of bounds.
+template <int DT>
+__device__ __forceinline__ void pair_load(const Stencil& s, int64_t e, int ez, int ey, Raw<DT>& r) {
+  if (e < 0 || !fvr_checked(e + 1, pair_entries(s), kSiteStencilEntry)) {
+    if constexpr (DT == FVR_F32_PAIR) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
+      if constexpr (DT == FVR_F16_PAIR) r.sc = 0.f;
+    }
+    return;
+  }
+  if constexpr (DT == FVR_F32_PAIR) {
+    const float4* p = static_cast<const float4*>(s.data) + e * 2;  // 32-byte entries
+    ldg256(p, r.q[0], r.q[1]);
+    ldg256(p + 2, r.q[2], r.q[3]);
+  } else {
+    ldg128x2(static_cast<const uint4*>(s.data) + e, r.q[0], r.q[1]);
+    if constexpr (DT == FVR_F16_PAIR) {
+      const unsigned by = static_cast<unsigned>(s.H + kBrick) / kBrick;
+      const unsigned si = (static_cast<unsigned>(ez) / kBrick) * by + static_cast<unsigned>(ey) / kBrick;
+      r.sc = fvr_checked(si, pair_scales(s), kSiteStencilScale) ? __ldg(s.scales + si) : 0.f;
+    }
+  }
 }
 
 // Cell address of p (FP64 voxel coordinates; zero-padding partial or hard cut-off).
@@ -317,6 +351,7 @@ struct TabCell {
   int ex, ey, ez;
 };
 
+template <int DT = FVR_F32>
 __device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa, int4 ib, float4 fb) {
   TabCell c;
   c.tx = fa.x + fb.x;
@@ -332,7 +367,8 @@ __device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa
   const bool ok = static_cast<unsigned>(c.ex) <= static_cast<unsigned>(s.W) &&
                   static_cast<unsigned>(c.ey) <= static_cast<unsigned>(s.H) &&
                   static_cast<unsigned>(c.ez) <= static_cast<unsigned>(s.D);
-  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + 1) + c.ex : -1;
+  // x-pair storage: W + 2 entries per x row, the cell's two at e and e + 1
+  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + (is_pair(DT) ? 2 : 1)) + c.ex : -1;
   return c;
 }
 
@@ -340,7 +376,9 @@ __device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa
 // interpolated value and derivatives instead: 8 products, not 16).
 template <int DT>
 __device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw<DT>& r) {
-  if constexpr (DT == FVR_F32) {
+  if constexpr (is_pair(DT)) {
+    pair_load<DT>(s, c.e, c.ez, c.ey, r);
+  } else if constexpr (DT == FVR_F32) {
     if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -365,8 +403,19 @@ __device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw
 }
 
 template <int DT>
+__device__ __forceinline__ void tab_decode2(const Raw<DT>& r, Sample8c& v);
+
+template <int DT>
 __device__ __forceinline__ void tab_decode(const Raw<DT>& r, Sample8& v) {
-  if constexpr (DT == FVR_F16) {
+  if constexpr (is_pair(DT)) {
+    Sample8c c;
+    tab_decode2<DT>(r, c);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v.re[i] = c.c[i].x;
+      v.im[i] = c.c[i].y;
+    }
+  } else if constexpr (DT == FVR_F16) {
     const uint32_t w[8] = {r.q[0].x, r.q[0].y, r.q[0].z, r.q[0].w, r.q[1].x, r.q[1].y, r.q[1].z, r.q[1].w};
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -381,7 +430,17 @@ __device__ __forceinline__ void tab_decode(const Raw<DT>& r, Sample8& v) {
 // Corners as (re, im) pairs, f16 without its brick scale (as tab_decode).
 template <int DT>
 __device__ __forceinline__ void tab_decode2(const Raw<DT>& r, Sample8c& v) {
-  if constexpr (is_pair(DT)) {
+  if constexpr (DT == FVR_F32_PAIR) {
+    // corner c = dz*4 + dy*2 + dx: x = 0 corners from entry ex, x = 1 from ex + 1
+    v.c[0] = make_float2(r.q[0].x, r.q[0].y);
+    v.c[2] = make_float2(r.q[0].z, r.q[0].w);
+    v.c[4] = make_float2(r.q[1].x, r.q[1].y);
+    v.c[6] = make_float2(r.q[1].z, r.q[1].w);
+    v.c[1] = make_float2(r.q[2].x, r.q[2].y);
+    v.c[3] = make_float2(r.q[2].z, r.q[2].w);
+    v.c[5] = make_float2(r.q[3].x, r.q[3].y);
+    v.c[7] = make_float2(r.q[3].z, r.q[3].w);
+  } else if constexpr (is_pair(DT)) {
     // corner c = dz*4 + dy*2 + dx: x = 0 corners from q[0], x = 1 from q[1]
     const uint32_t w0[4] = {r.q[0].x, r.q[0].y, r.q[0].z, r.q[0].w};
     const uint32_t w1[4] = {r.q[1].x, r.q[1].y, r.q[1].z, r.q[1].w};

@@ -302,17 +302,7 @@ __device__ __forceinline__ SCell sncc_cell(const Stencil& s, int4 ia, float4 fa,
 template <int DT>
 __device__ __forceinline__ void sncc_load(const Stencil& s, const SCell& c, Raw<DT>& r) {
   if constexpr (is_pair(DT)) {
-    if (c.e < 0 || !fvr_checked(c.e + 1, pair_entries(s), kSiteStencilEntry)) {
-      r.q[0] = r.q[1] = make_uint4(0u, 0u, 0u, 0u);
-      if constexpr (DT == FVR_F16_PAIR) r.sc = 0.f;
-      return;
-    }
-    ldg128x2(static_cast<const uint4*>(s.data) + static_cast<int64_t>(c.e), r.q[0], r.q[1]);
-    if constexpr (DT == FVR_F16_PAIR) {
-      const unsigned by = static_cast<unsigned>(s.H + kBrick) / kBrick;
-      const unsigned si = (static_cast<unsigned>(c.ez) / kBrick) * by + static_cast<unsigned>(c.ey) / kBrick;
-      r.sc = fvr_checked(si, pair_scales(s), kSiteStencilScale) ? __ldg(s.scales + si) : 0.f;
-    }
+    pair_load<DT>(s, c.e, c.ez, c.ey, r);
   } else if constexpr (DT == FVR_F32) {
     if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
 #pragma unroll
@@ -797,9 +787,10 @@ static int stencil_from(int dtype, const void* data, const float* scales, int64_
                         Stencil* s, bool pair_ok = false) {
   if (!data || D < 1 || H < 1 || W < 1 || D > 8192 || H > 8192 || W > 8192) return FVR_ERR_ARG;
   if (dtype != FVR_F32 && dtype != FVR_BF16 && dtype != FVR_F16 &&
-      !(pair_ok && (dtype == FVR_BF16_PAIR || dtype == FVR_F16_PAIR)))
+      !(pair_ok && (dtype == FVR_BF16_PAIR || dtype == FVR_F16_PAIR || dtype == FVR_F32_PAIR)))
     return FVR_ERR_DTYPE;
   if ((dtype == FVR_F16 || dtype == FVR_F16_PAIR) && !scales) return FVR_ERR_ARG;
+  if (dtype == FVR_F32_PAIR && (reinterpret_cast<uintptr_t>(data) & 31) != 0) return FVR_ERR_ARG;  // 256-bit loads
   if ((reinterpret_cast<uintptr_t>(data) & 15) != 0) return FVR_ERR_ARG;
   *s = Stencil{data, scales, static_cast<int>(D), static_cast<int>(H), static_cast<int>(W), dtype};
   return FVR_OK;
@@ -1047,6 +1038,7 @@ int fvr_tc_sncc_moments(int dtype, const void* stencil, const float* scales, int
     case FVR_F16: FVR_SNCC(FVR_F16)
     case FVR_BF16_PAIR: FVR_SNCC(FVR_BF16_PAIR)
     case FVR_F16_PAIR: FVR_SNCC(FVR_F16_PAIR)
+    case FVR_F32_PAIR: FVR_SNCC(FVR_F32_PAIR)
   }
 #undef FVR_SNCC
   FVR_LAUNCH_CHECK();
@@ -1091,6 +1083,7 @@ int fvr_tc_sncc_value_and_grad(int dtype, const void* stencil, const float* scal
     case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a, true); break;
     case FVR_BF16_PAIR: launch_sncc<FVR_BF16_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
     case FVR_F16_PAIR: launch_sncc<FVR_F16_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_F32_PAIR: launch_sncc<FVR_F32_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
   }
   FVR_LAUNCH_CHECK();
   launch_sncc_final(s, a);
@@ -1224,6 +1217,7 @@ int fvr_tc_sncc_value_and_grad_static(int dtype, const void* stencil, const floa
     case FVR_F16: launch_sncc<FVR_F16, true>(variant, grid, (int)smem, s, a, true); break;
     case FVR_BF16_PAIR: launch_sncc<FVR_BF16_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
     case FVR_F16_PAIR: launch_sncc<FVR_F16_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
+    case FVR_F32_PAIR: launch_sncc<FVR_F32_PAIR, true>(variant, grid, (int)smem, s, a, true); break;
   }
   FVR_LAUNCH_CHECK();
   launch_sncc_final(s, a);

@@ -27,6 +27,7 @@ F16_ = 2
 F64_ = 3
 BF16_PAIR_ = 4
 F16_PAIR_ = 5
+F32_PAIR_ = 6
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -43,7 +44,7 @@ SIGNATURES = {
     "fvr_stencil_build": (I32, [P, I32, I32, I64, I64, I64, I64, I32, P, P, P, P]),
     "fvr_stencil_pair_bytes": (I64, [I64, I64, I64, I32]),
     "fvr_stencil_pair_scale_count": (I64, [I64, I64, I64]),
-    "fvr_stencil_pair_build": (I32, [P, I32, I32, I64, I64, I64, I32, P, P, P, P]),
+    "fvr_stencil_pair_build": (I32, [P, I32, I32, I64, I64, I64, I64, I32, P, P, P, P]),
     "fvr_slice3d_fwd": (I32, [P, I32, I64, I64, I64, I64, P, P, I64, P, P, I64, F32, F32, F32, P, P]),
     "fvr_slice3d_bwd_workspace": (I64, [I64, I64]),
     "fvr_slice3d_bwd": (I32, [P, I32, I64, I64, I64, I64, P, P, P, I64, P, P, I64, F32, F32, F32, P, P, P, I64, P]),

@@ -172,32 +172,32 @@ class Stencil:
 
 
 class PairStencil:
-    """x-pair copy of a centred spectrum for the spectral-NCC moments kernels
-    (16-bit only; see fvr_stencil_pair_build in include/fvr_b200.h): half the
-    bytes of the stencil, a sample's two entries side by side."""
+    """x-pair copy of a centred spectrum (see fvr_stencil_pair_build in
+    include/fvr_b200.h), read by the spectral-NCC moments kernels and the
+    fused PoU block-image kernels: half the bytes of the stencil, a sample's
+    two entries side by side.  ``items`` spectra back to back, as Stencil."""
 
-    def __init__(self, master, planar, dims, dtype):
+    def __init__(self, master, planar, dims, dtype, items=1):
         dev = L.require_cuda(master)
         D, H, W = (int(s) for s in dims)
         self.dims = (D, H, W)
+        self.items = int(items)
         self.dtype = dtype
-        if dtype == torch.float16:
-            self.code = L.F16_PAIR_
-        elif dtype == torch.bfloat16:
-            self.code = L.BF16_PAIR_
-        else:
-            raise L.FvrError(f"x-pair storage is 16-bit only, not {dtype}")
-        nbytes = L.query("fvr_stencil_pair_bytes", D, H, W, self.code)
-        self.data = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        codes = {torch.float16: L.F16_PAIR_, torch.bfloat16: L.BF16_PAIR_, torch.float32: L.F32_PAIR_}
+        if dtype not in codes:
+            raise L.FvrError(f"unsupported x-pair storage dtype {dtype}")
+        self.code = codes[dtype]
+        self.item_bytes = L.query("fvr_stencil_pair_bytes", D, H, W, self.code)
+        self.data = torch.empty(self.item_bytes * self.items, dtype=torch.uint8, device=dev)
         self.scales = None
         scratch = None
         if self.code == L.F16_PAIR_:
-            n = L.query("fvr_stencil_pair_scale_count", D, H, W)
+            n = L.query("fvr_stencil_pair_scale_count", D, H, W) * self.items
             self.scales = torch.empty(n, dtype=torch.float32, device=dev)
             scratch = torch.empty(n, dtype=torch.int32, device=dev)
         m = master.contiguous()
-        L.call("fvr_stencil_pair_build", L.ptr(m), L.dtype_code(m.dtype), int(planar), D, H, W, self.code,
-               L.ptr(self.data), L.ptr(self.scales), L.ptr(scratch), L.stream_ptr(dev))
+        L.call("fvr_stencil_pair_build", L.ptr(m), L.dtype_code(m.dtype), int(planar), self.items, D, H, W,
+               self.code, L.ptr(self.data), L.ptr(self.scales), L.ptr(scratch), L.stream_ptr(dev))
 
     def args(self):
         D, H, W = self.dims

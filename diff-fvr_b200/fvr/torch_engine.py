@@ -423,16 +423,15 @@ class TorchDiffFVREngine(nn.Module):
         self.register_buffer("f_vol_5d", planar.to(dtype=dtype))
         # storage copies come from the float32 spectrum (f16 takes its brick scales from it)
         self._stencil = RT.Stencil(planar[0], True, self.pad_shape, self._stencil_dtype(dtype))
-        self._pair = (RT.PairStencil(planar[0], True, self.pad_shape, dtype)
-                      if dtype in (torch.float16, torch.bfloat16) else None)
-        self.use_pair_storage = True  # 16-bit: the spectral-NCC moments read the x-pair copy
+        self._pair = RT.PairStencil(planar[0], True, self.pad_shape, self._stencil_dtype(dtype))
+        self.use_pair_storage = True  # the spectral-NCC moments read the x-pair copy
         del planar
         self._fused_ws = {}  # (C, R, views, device) -> workspace of the fused value_and_grad
         self._fused_calls = {}  # prepared launches of the fused value_and_grad
 
     def _sncc_storage(self):
         """The spectrum copy the spectral-NCC moments kernels read: the x-pair
-        copy of 16-bit storage (unless ``use_pair_storage`` is off), else the stencil."""
+        copy (unless ``use_pair_storage`` is off), else the stencil."""
         return self._pair if (self._pair is not None and self.use_pair_storage) else self._stencil
 
     @staticmethod
@@ -453,10 +452,9 @@ class TorchDiffFVREngine(nn.Module):
         """
         src = self.f_vol_5d[0]
         self._stencil = RT.Stencil(src, True, self.pad_shape, self._stencil_dtype(dtype))
-        # 16-bit storage: the spectral-NCC moments kernels read an x-pair copy
-        # (half the stencil's bytes; the image path keeps the stencil)
-        self._pair = (RT.PairStencil(src, True, self.pad_shape, dtype)
-                      if dtype in (torch.float16, torch.bfloat16) else None)
+        # the spectral-NCC moments kernels read an x-pair copy (half the
+        # stencil's bytes; the image path keeps the stencil)
+        self._pair = RT.PairStencil(src, True, self.pad_shape, self._stencil_dtype(dtype))
         self.f_vol_5d = self.f_vol_5d.to(dtype=dtype)
         self._compiled_forward_core = None
         self._compiled_spectral_ncc = None

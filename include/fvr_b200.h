@@ -34,9 +34,18 @@ typedef enum {
   FVR_ERR_CUDA = 5         /* launch or driver error (cudaGetLastError)     */
 } fvr_status;
 
-/* FVR_BF16_PAIR / FVR_F16_PAIR name the x-pair spectrum storage (below),
- * accepted by the spectral-NCC moments entry points only. */
-typedef enum { FVR_F32 = 0, FVR_BF16 = 1, FVR_F16 = 2, FVR_F64 = 3, FVR_BF16_PAIR = 4, FVR_F16_PAIR = 5 } fvr_dtype;
+/* FVR_BF16_PAIR / FVR_F16_PAIR / FVR_F32_PAIR name the x-pair spectrum
+ * storage (below), accepted by the spectral-NCC moments entry points and the
+ * fused PoU block-image entry points only. */
+typedef enum {
+  FVR_F32 = 0,
+  FVR_BF16 = 1,
+  FVR_F16 = 2,
+  FVR_F64 = 3,
+  FVR_BF16_PAIR = 4,
+  FVR_F16_PAIR = 5,
+  FVR_F32_PAIR = 6
+} fvr_dtype;
 
 const char* fvr_status_string(int status);
 int fvr_version(void);
@@ -93,20 +102,23 @@ int64_t fvr_stencil_scale_count(int64_t D, int64_t H, int64_t W);
  * scratch_max: items * fvr_stencil_scale_count() uint32 (f16 only, else NULL). */
 int fvr_stencil_build(const void* master, int master_dtype, int master_planar, int64_t items, int64_t D, int64_t H,
                       int64_t W, int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream);
-/* x-pair layout of the same spectrum, 16-bit only (out_dtype FVR_BF16_PAIR or
- * FVR_F16_PAIR): (D+1)(H+1)(W+2) entries of 16 B; entry (ez, ey, ex) holds the
- * 4 complex values of voxel column x = ex-1 at (y, z) = (ey-1+dy, ez-1+dz),
- * ordered dz*2 + dy (zero outside the volume).  A trilinear sample in the
- * stencil cell (ez, ey, ex) reads entries ex and ex+1: 32 contiguous bytes,
- * half the storage of the stencil, so the samples of many slices meet in
- * fewer sectors.  f16: a power-of-two scale per slab of 16 x 16 (z, y)
- * entry rows over the whole x extent, so a sample's two entries share it
- * (fvr_stencil_pair_scale_count floats).  Same master formats as
- * fvr_stencil_build, one spectrum; scratch_max as there (f16 only). */
+/* x-pair layout of the same spectrum (out_dtype FVR_BF16_PAIR, FVR_F16_PAIR
+ * or FVR_F32_PAIR): (D+1)(H+1)(W+2) entries of 16 B (16-bit) or 32 B (f32);
+ * entry (ez, ey, ex) holds the 4 complex values of voxel column x = ex-1 at
+ * (y, z) = (ey-1+dy, ez-1+dz), ordered dz*2 + dy (zero outside the volume).
+ * A trilinear sample in the stencil cell (ez, ey, ex) reads entries ex and
+ * ex+1: 32 (64) contiguous bytes, half the storage of the stencil, so the
+ * samples of many slices meet in fewer sectors.  f16: a power-of-two scale
+ * per slab of 16 x 16 (z, y) entry rows over the whole x extent, so a
+ * sample's two entries share it (fvr_stencil_pair_scale_count floats).
+ * Same master formats and `items` batching as fvr_stencil_build (out item
+ * stride fvr_stencil_pair_bytes(); scales item stride
+ * fvr_stencil_pair_scale_count()); scratch_max as there (f16 only). */
 int64_t fvr_stencil_pair_bytes(int64_t D, int64_t H, int64_t W, int dtype);
 int64_t fvr_stencil_pair_scale_count(int64_t D, int64_t H, int64_t W);
-int fvr_stencil_pair_build(const void* master, int master_dtype, int master_planar, int64_t D, int64_t H, int64_t W,
-                           int out_dtype, void* out, float* scales, unsigned int* scratch_max, void* stream);
+int fvr_stencil_pair_build(const void* master, int master_dtype, int master_planar, int64_t items, int64_t D,
+                           int64_t H, int64_t W, int out_dtype, void* out, float* scales, unsigned int* scratch_max,
+                           void* stream);
 
 /* --------------------------------------- drop-in trilinear slice gather -- */
 /* fourier_slice_3d on the reference layout vol[B][2][D][H][W] (dtype f32 /
@@ -147,8 +159,8 @@ int64_t fvr_tc_sncc_mom_stride(void);
  * selects the launch shape (rows in flight per thread, resident CTAs per SM);
  * results do not depend on it beyond float summation order.  dtype: the
  * stencil storage (FVR_F32 / FVR_BF16 / FVR_F16) or the x-pair storage
- * (FVR_BF16_PAIR / FVR_F16_PAIR; stencil = its data, scales = its slab
- * scales), in this and the two value-and-gradient entry points below.
+ * (FVR_*_PAIR; stencil = its data, scales = its slab scales), in this and
+ * the two value-and-gradient entry points below.
  * Replaces TorchDiffFVREngine._spectral_ncc_core / forward_spectral_ncc,
  * src/fvr/torch_engine.py:269-307 (the gather of :176-234 included). */
 int fvr_tc_sncc_variants(void);

@@ -542,20 +542,24 @@ def _bf16_round(x):
     return (b.astype(np.uint32) << 16).view(np.float32)
 
 
-@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16, torch.float32])
 def test_pair_storage_build_matches_restatement(dtype):
-    """fvr_stencil_pair_build on a small planar spectrum: every 16-byte entry
+    """fvr_stencil_pair_build on two small planar spectra: every entry
     (ez, ey, ex) holds voxel column x = ex - 1 at (y, z) = (ey - 1 + dy,
-    ez - 1 + dz), zero outside; bf16 rounded to nearest, f16 divided by its
-    (z, y) slab's power-of-two scale (2^(e - 15) for the slab maximum
-    m = f 2^e; a slab is 16 x 16 entry rows over every x)."""
+    ez - 1 + dz), zero outside; f32 exact, bf16 rounded to nearest, f16
+    divided by its (z, y) slab's power-of-two scale (2^(e - 15) for the slab
+    maximum m = f 2^e; a slab is 16 x 16 entry rows over every x)."""
     import fvr._runtime as RT
 
     D, H, W = 5, 19, 18  # a slab boundary along y (H + 1 = 20 > 16)
     rng = np.random.default_rng(3)
     master = (rng.standard_normal((2, D, H, W)) * np.exp(rng.uniform(-3, 6, (2, D, H, W)))).astype(np.float32)
-    ps = RT.PairStencil(torch.from_numpy(master).cuda(), True, (D, H, W), dtype)
-    raw = ps.data.cpu().numpy().view(np.uint16).reshape(D + 1, H + 1, W + 2, 4, 2)
+    two = np.ascontiguousarray(np.stack([master, 2 * master]))  # two items; item 1 = 2 x item 0 (exact)
+    ps = RT.PairStencil(torch.from_numpy(two).cuda(), True, (D, H, W), dtype, items=2)
+    if dtype == torch.float32:  # 32-byte entries holding the master's values
+        got = ps.data.cpu().numpy().view(np.float32).reshape(2, D + 1, H + 1, W + 2, 4, 2)
+    else:
+        raw = ps.data.cpu().numpy().view(np.uint16).reshape(2, D + 1, H + 1, W + 2, 4, 2)[0]
     want = np.zeros((D + 1, H + 1, W + 2, 4, 2), np.float32)
     for ez in range(D + 1):
         for ey in range(H + 1):
@@ -565,13 +569,16 @@ def test_pair_storage_build_matches_restatement(dtype):
                     z, y = ez - 1 + (k >> 1), ey - 1 + (k & 1)
                     if 0 <= z < D and 0 <= y < H and 0 <= x < W:
                         want[ez, ey, ex, k] = master[:, z, y, x]
-    if dtype == torch.bfloat16:
+    if dtype == torch.float32:
+        assert np.array_equal(got[0], want) and np.array_equal(got[1], 2 * want)
+    elif dtype == torch.bfloat16:
         got = (raw.astype(np.uint32) << 16).view(np.float32)
         assert np.array_equal(got, _bf16_round(want))
     else:
-        sc = ps.scales.cpu().numpy()
         bz, by = (D + 16) // 16, (H + 16) // 16
-        assert sc.size == bz * by
+        sc = ps.scales.cpu().numpy()[:bz * by]
+        assert ps.scales.numel() == 2 * bz * by
+        assert np.array_equal(ps.scales.cpu().numpy()[bz * by:], 2 * sc)  # item 1's slabs: twice the maximum
         m = np.abs(want).max(axis=(2, 3, 4))
         for iz in range(bz):
             for iy in range(by):
@@ -582,11 +589,11 @@ def test_pair_storage_build_matches_restatement(dtype):
         assert np.array_equal(raw.view(np.float16), exp)
 
 
-@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16, torch.float32])
 @pytest.mark.parametrize("C,R", [(64, 128), (7, 37), (300, 16)])
 def test_pair_storage_moments_match_stencil(big, dtype, C, R):
-    """The spectral-NCC moments read the x-pair copy of 16-bit storage: loss
-    and pose gradient agree with the stencil copy of the same storage to the
+    """The spectral-NCC moments read the x-pair copy of the storage: loss and
+    pose gradient agree with the stencil copy of the same storage to the
     storage's rounding (both are rounded once from the float32 spectrum; f16
     scaled over different entry groups), for every launch variant."""
     import os
@@ -605,7 +612,7 @@ def test_pair_storage_moments_match_stencil(big, dtype, C, R):
     l0, g0 = eng.spectral_ncc_value_and_grad(poses, (fa, fl), ("ap", "lateral"))
     eng.use_pair_storage = True
     scale = float(g0.abs().max())
-    tol = 2e-3 if dtype == torch.float16 else 2e-2
+    tol = {torch.float16: 2e-3, torch.bfloat16: 2e-2, torch.float32: 1e-5}[dtype]
     try:
         for variant in range(L.load().fvr_tc_sncc_variants()):
             os.environ["FVR_SNCC_FUSED_VARIANT"] = str(variant)
