@@ -351,7 +351,6 @@ struct TabCell {
   int ex, ey, ez;
 };
 
-template <int DT = FVR_F32>
 __device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa, int4 ib, float4 fb) {
   TabCell c;
   c.tx = fa.x + fb.x;
@@ -367,8 +366,7 @@ __device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa
   const bool ok = static_cast<unsigned>(c.ex) <= static_cast<unsigned>(s.W) &&
                   static_cast<unsigned>(c.ey) <= static_cast<unsigned>(s.H) &&
                   static_cast<unsigned>(c.ez) <= static_cast<unsigned>(s.D);
-  // x-pair storage: W + 2 entries per x row, the cell's two at e and e + 1
-  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + (is_pair(DT) ? 2 : 1)) + c.ex : -1;
+  c.e = ok ? (c.ez * (s.H + 1) + c.ey) * (s.W + 1) + c.ex : -1;
   return c;
 }
 
@@ -376,9 +374,7 @@ __device__ __forceinline__ TabCell tab_cell(const Stencil& s, int4 ia, float4 fa
 // interpolated value and derivatives instead: 8 products, not 16).
 template <int DT>
 __device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw<DT>& r) {
-  if constexpr (is_pair(DT)) {
-    pair_load<DT>(s, c.e, c.ez, c.ey, r);
-  } else if constexpr (DT == FVR_F32) {
+  if constexpr (DT == FVR_F32) {
     if (c.e < 0 || !fvr_checked(c.e, stencil_entries(s), kSiteStencilEntry)) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) r.q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -403,19 +399,8 @@ __device__ __forceinline__ void tab_load(const Stencil& s, const TabCell& c, Raw
 }
 
 template <int DT>
-__device__ __forceinline__ void tab_decode2(const Raw<DT>& r, Sample8c& v);
-
-template <int DT>
 __device__ __forceinline__ void tab_decode(const Raw<DT>& r, Sample8& v) {
-  if constexpr (is_pair(DT)) {
-    Sample8c c;
-    tab_decode2<DT>(r, c);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      v.re[i] = c.c[i].x;
-      v.im[i] = c.c[i].y;
-    }
-  } else if constexpr (DT == FVR_F16) {
+  if constexpr (DT == FVR_F16) {
     const uint32_t w[8] = {r.q[0].x, r.q[0].y, r.q[0].z, r.q[0].w, r.q[1].x, r.q[1].y, r.q[1].z, r.q[1].w};
 #pragma unroll
     for (int i = 0; i < 8; ++i) {

@@ -35,8 +35,7 @@ typedef enum {
 } fvr_status;
 
 /* FVR_BF16_PAIR / FVR_F16_PAIR / FVR_F32_PAIR name the x-pair spectrum
- * storage (below), accepted by the spectral-NCC moments entry points and the
- * fused PoU block-image entry points only. */
+ * storage (below), accepted by the spectral-NCC moments entry points only. */
 typedef enum {
   FVR_F32 = 0,
   FVR_BF16 = 1,
