@@ -697,17 +697,19 @@ def _large_volume_fp64(vol, poses4, fts, R, sp0):
 
 
 def _sncc_step_roofline(storage, C, R, ms):
-    """Whole-step logical bytes of the batched spectral-NCC step: per view and sample the 8-corner gather of
-    the forward pass and again of the adjoint (8 B a corner in f32, 4 B in
-    16-bit storage), the 8 B target and, for f16, a 4 B brick scale; over the
-    step's CUDA-event time."""
+    """Bytes the batched spectral-NCC step must read, over the step's CUDA-event
+    time: per view and sample the 8 corners once (8 B a corner in f32, 4 B in
+    16-bit storage; the adjoint is fused into the same pass) and the 8 B
+    target.  The scope table's logical count (the 8-corner gather again for
+    the adjoint, and a 4 B brick scale for f16) is reported beside it."""
     peak, peak_kind = _peak_hbm()
     corner = 8 if storage == "f32" else 4
-    per_sample = 2 * 8 * corner + 8 + (4 if storage == "f16" else 0)
-    alg = 2 * C * R * R * per_sample
+    alg = 2 * C * R * R * (8 * corner + 8)
+    logical = 2 * C * R * R * (2 * 8 * corner + 8 + (4 if storage == "f16" else 0))
     achieved = alg / (ms * 1e-3) / 1e9
     return {"bound": "hbm", "alg_bytes_per_step": alg, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak,
+            "frac": achieved / peak, "scope_table_bytes_per_step": logical,
+            "scope_table_frac": logical / (ms * 1e-3) / 1e9 / peak,
             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
             "fallback 6.65 TB/s", "timing": "whole step (graph replay)"}
 

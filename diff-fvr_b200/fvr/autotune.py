@@ -34,9 +34,9 @@ def _l2_flush(device):
     return t
 
 
-def choose(kind, key, run, n_variants, reps=5, candidates=None):
-    """Return the fastest variant of ``run(variant)`` (launches one kernel) for
-    ``key``: the median of ``reps`` launches per variant, each after an L2
+def choose(kind, key, run, n_variants, reps=7, candidates=None):
+    """Return the fastest variant of ``run(variant)`` (launches the kernels of
+    one call) for ``key``: the median of ``reps`` calls per variant, each after an L2
     rewrite (the flush also keeps the device busy while the launch is
     enqueued, so the events time the launch alone).  ``candidates``
     restricts the variants tried (default: all)."""

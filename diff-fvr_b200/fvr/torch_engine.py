@@ -71,12 +71,19 @@ def _sncc_forward(eng, p, views, ftargs, hp, R, with_grad):
         L.call("fvr_tc_sncc_moments", *st.args(), L.ptr(p), C, nv, vcodes, fptrs, L.ptr(hp), L.ptr(lin), R, kap,
                int(with_grad), int(variant), L.ptr(ws), ws_bytes, s)
 
-    variant = autotune.choose("sncc", (st.code, C, R, nv, int(with_grad), st.dims), run,
+    def finalize(variant):  # the record count (and so this kernel's work) depends on the variant's grid
+        L.call("fvr_tc_sncc_finalize", L.ptr(ws), C, R, nv, int(with_grad), int(variant), L.ptr(mom), L.ptr(loss),
+               None, s)
+
+    def both(variant):
+        run(variant)
+        finalize(variant)
+
+    variant = autotune.choose("sncc", (st.code, C, R, nv, int(with_grad), st.dims), both,
                               L.load().fvr_tc_sncc_variants())
     with profiling.section("tc_sncc_moments"):
         run(variant)
-    L.call("fvr_tc_sncc_finalize", L.ptr(ws), C, R, nv, int(with_grad), int(variant), L.ptr(mom), L.ptr(loss), None,
-           s)
+    finalize(variant)
     return mom, loss
 
 
