@@ -50,14 +50,18 @@ def test_reference_arm_other_ranks_exit_without_work():
 
 
 def test_scope_table_byte_counts():
-    """The bench's algorithmic-byte counts reproduce the hot-path scope
-    table's per-pose-eval figures: 4.46 MB (f32) and 2.36 MB (bf16) for the
-    batched spectral-NCC step at out_res 128 with 2 views, and about 294 MB
-    for the PoU step at 52 blocks (P = 128, 256^2 detector, f32)."""
+    """The bench's logical byte counts reproduce the hot-path scope table's
+    per-pose-eval figures: 4.46 MB (f32) and 2.36 MB (bf16) for the batched
+    spectral-NCC step at out_res 128 with 2 views, and about 294 MB for the
+    PoU step at 52 blocks (P = 128, 256^2 detector, f32); the bytes that
+    step must read (8 corners once + the 8 B target per sample) beside them."""
     sys.path.insert(0, str(REPO))
     import bench
 
-    per_eval = {s: bench._sncc_step_roofline(s, 1, 128, 1.0)["alg_bytes_per_step"] for s in ("f32", "bf16", "f16")}
+    rl = {s: bench._sncc_step_roofline(s, 1, 128, 1.0) for s in ("f32", "bf16", "f16")}
+    per_eval = {s: r["scope_table_bytes_per_step"] for s, r in rl.items()}
+    assert rl["f32"]["alg_bytes_per_step"] == 2 * 128 * 128 * 72
+    assert rl["bf16"]["alg_bytes_per_step"] == rl["f16"]["alg_bytes_per_step"] == 2 * 128 * 128 * 40
     assert abs(per_eval["f32"] / 1e6 - 4.46) < 0.01
     assert abs(per_eval["bf16"] / 1e6 - 2.36) < 0.01
     assert abs(per_eval["f16"] / 1e6 - 2.49) < 0.01  # + 4 B brick scale per sample
