@@ -32,6 +32,16 @@ __device__ __forceinline__ void entry_values(const MT* m, int64_t plane, int D, 
   }
 }
 
+// atomicMax of non-negative float bits into table[idx], one atomic per group
+// of lanes that share idx (consecutive entries mostly share their brick, so
+// the lanes of a warp merge their maxima first instead of all contending for
+// one address).
+__device__ __forceinline__ void group_atomic_max(unsigned int* table, long long idx, unsigned int bits) {
+  const unsigned grp = __match_any_sync(__activemask(), idx);
+  const unsigned m = __reduce_max_sync(grp, bits);
+  if ((threadIdx.x & 31) == static_cast<unsigned>(__ffs(grp) - 1)) atomicMax(table + idx, m);
+}
+
 template <typename MT>
 __global__ void stencil_brick_max_kernel(const MT* __restrict__ m0, int64_t plane, int64_t items, int D, int H,
                                          int W, unsigned int* bmax0) {
@@ -43,7 +53,6 @@ __global__ void stencil_brick_max_kernel(const MT* __restrict__ m0, int64_t plan
        ee += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t item = ee / n1, e = ee - item * n1;
     const MT* m = m0 + item * 2 * static_cast<int64_t>(D) * H * W;
-    unsigned int* bmax = bmax0 + item * nb1;
     const int ex = static_cast<int>(e % (W + 1));
     const int ey = static_cast<int>((e / (W + 1)) % (H + 1));
     const int ez = static_cast<int>(e / (static_cast<int64_t>(W + 1) * (H + 1)));
@@ -53,7 +62,7 @@ __global__ void stencil_brick_max_kernel(const MT* __restrict__ m0, int64_t plan
 #pragma unroll
     for (int c = 0; c < 8; ++c) mx = fmaxf(mx, fmaxf(fabsf(re[c]), fabsf(im[c])));
     const int64_t b = (static_cast<int64_t>(ez / kBrick) * by + ey / kBrick) * bx + ex / kBrick;
-    atomicMax(bmax + b, __float_as_uint(mx));  // non-negative floats order like their bits
+    group_atomic_max(bmax0, item * nb1 + b, __float_as_uint(mx));  // non-negative floats order like their bits
   }
 }
 
@@ -174,7 +183,7 @@ __global__ void pair_slab_max_kernel(const MT* __restrict__ m0, int64_t plane, i
     float mx = 0.f;
 #pragma unroll
     for (int k = 0; k < 4; ++k) mx = fmaxf(mx, fmaxf(fabsf(re[k]), fabsf(im[k])));
-    atomicMax(smax0 + item * nb1 + g.slab(ez, ey), __float_as_uint(mx));  // non-negative floats order like their bits
+    group_atomic_max(smax0, item * nb1 + g.slab(ez, ey), __float_as_uint(mx));  // non-negative floats order like their bits
   }
 }
 
