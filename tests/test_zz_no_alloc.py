@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 FVR_ERR_WORKSPACE = 4
 
 
-def _problem(C, R=48, dtype=torch.float32):
+def _problem(C, R=48, dtype=torch.float32, storage="stencil"):
     from fvr import _lib as L
     from fvr import _runtime as RT
     from fvr.torch_engine import TorchDiffFVREngine
@@ -32,7 +32,8 @@ def _problem(C, R=48, dtype=torch.float32):
     fptrs = (ctypes.c_void_p * 2)(*[f.data_ptr() for f in fts])
     hp = RT.hp_filter(R, R, 4.0, dev)
     lin = RT.linspace(R, dev)
-    head = (*eng._stencil.args(), L.ptr(poses), C, 2, views, fptrs, L.ptr(hp), L.ptr(lin), R,
+    st = eng._pair if storage == "pair" else eng._stencil
+    head = (*st.args(), L.ptr(poses), C, 2, views, fptrs, L.ptr(hp), L.ptr(lin), R,
             RT.kappa(R, eng.spacing[0]), 0, None, 0)
     return eng, fts, poses, head, dev
 
@@ -45,12 +46,15 @@ def _outputs(C, dev):
 
 @pytest.mark.parametrize("C", [24, 256])
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.bfloat16])
-def test_static_scratch_matches_workspace_entry(dtype, C):
+@pytest.mark.parametrize("storage", ["stencil", "pair"])
+def test_static_scratch_matches_workspace_entry(storage, dtype, C):
     """C = 256 with two views is the scratch's limit (512 items: every item
-    record row and four 128-item chunks of the epilogue are used)."""
+    record row and four 128-item chunks of the epilogue are used); both
+    spectrum copies the engine keeps (the stencil, and the x-pair copy its
+    own spectral-NCC calls read)."""
     from fvr import _lib as L
 
-    eng, fts, poses, head, dev = _problem(C, dtype=dtype)
+    eng, fts, poses, head, dev = _problem(C, dtype=dtype, storage=storage)
     lib = L.load()
     s = L.stream_ptr(dev)
     ws_bytes = int(L.query("fvr_tc_sncc_fused_workspace", C, 48, 2))
