@@ -29,32 +29,37 @@ struct PouAxisTables {
   int k, n;
 };
 
-// sum over the support of vol * w0 * w1 * w2 for candidate block kb (fp64)
-__global__ void __launch_bounds__(256) pou_block_sums_kernel(const float* __restrict__ vol, PouAxisTables a0,
-                                                             PouAxisTables a1, PouAxisTables a2,
-                                                             double* __restrict__ sums) {
-  __shared__ double red[8];
+// Sum over the support of vol * w0 * w1 * w2 (fp64) for candidate block
+// kb = blockIdx.x: one warp per (z, y) row of the support, lanes along x (no
+// division per voxel), then warps in order.
+constexpr int kBlockSumThreads = 1024;
+
+__global__ void __launch_bounds__(kBlockSumThreads) pou_block_sums_kernel(const float* __restrict__ vol,
+                                                                          PouAxisTables a0, PouAxisTables a1,
+                                                                          PouAxisTables a2, double* __restrict__ sums) {
+  __shared__ double red[kBlockSumThreads / 32];
   const int kb = blockIdx.x;
   const int i0 = kb / (a1.k * a2.k), i1 = (kb / a2.k) % a1.k, i2 = kb % a2.k;
   const int s0 = a0.sup[2 * i0], l0 = a0.sup[2 * i0 + 1];
   const int s1 = a1.sup[2 * i1], l1 = a1.sup[2 * i1 + 1];
   const int s2 = a2.sup[2 * i2], l2 = a2.sup[2 * i2 + 1];
-  const int64_t tot = static_cast<int64_t>(l0) * l1 * l2;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const float* w2 = a2.w + i2 * a2.n + s2;
   double acc = 0.0;
-  for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
-    const int z = static_cast<int>(e / (static_cast<int64_t>(l1) * l2));
-    const int y = static_cast<int>((e / l2) % l1), x = static_cast<int>(e % l2);
-    const int gz = s0 + z, gy = s1 + y, gx = s2 + x;
-    const float wv = a0.w[i0 * a0.n + gz] * a1.w[i1 * a1.n + gy] * a2.w[i2 * a2.n + gx];
-    acc += static_cast<double>(vol[(static_cast<int64_t>(gz) * a1.n + gy) * a2.n + gx] * wv);
+  for (int zy = wid; zy < l0 * l1; zy += nw) {
+    const int z = zy / l1, y = zy - z * l1;
+    const int gz = s0 + z, gy = s1 + y;
+    const float wzy = a0.w[i0 * a0.n + gz] * a1.w[i1 * a1.n + gy];
+    const float* row = vol + (static_cast<int64_t>(gz) * a1.n + gy) * a2.n + s2;
+    for (int x = lane; x < l2; x += 32) acc += static_cast<double>(row[x] * (wzy * w2[x]));
   }
   acc = warp_sum(acc);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  if (lane == 0) red[wid] = acc;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < (blockDim.x >> 5); ++w) s += red[w];
-    sums[kb] = s;
+    double sum = 0.0;
+    for (int w = 0; w < nw; ++w) sum += red[w];
+    sums[kb] = sum;
   }
 }
 
@@ -1212,8 +1217,8 @@ int fvr_pou_block_sums(const float* vol, int64_t n0, int64_t n1, int64_t n2, con
   if (!vol || !w0 || !w1 || !w2 || !sup0 || !sup1 || !sup2 || !sums) return FVR_ERR_ARG;
   if (k0 < 1 || k1 < 1 || k2 < 1 || n0 < 1 || n1 < 1 || n2 < 1 || k0 * k1 * k2 > 65535) return FVR_ERR_ARG;
   PouAxisTables a0{w0, sup0, (int)k0, (int)n0}, a1{w1, sup1, (int)k1, (int)n1}, a2{w2, sup2, (int)k2, (int)n2};
-  pou_block_sums_kernel<<<static_cast<unsigned>(k0 * k1 * k2), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      vol, a0, a1, a2, sums);
+  pou_block_sums_kernel<<<static_cast<unsigned>(k0 * k1 * k2), kBlockSumThreads, 0,
+                          static_cast<cudaStream_t>(stream)>>>(vol, a0, a1, a2, sums);
   FVR_LAUNCH_CHECK();
   return FVR_OK;
 }
