@@ -423,21 +423,6 @@ def _f16_from_f32(eng, vol, dev, torch):
     eng._stencil, eng._pair, eng.f_vol_5d = fresh._stencil, fresh._pair, fresh.f_vol_5d
 
 
-def _pou_roofline(B, P, K, entry, pose_evals_per_s):
-    """Whole-step logical bytes per pose-eval of the PoU step: forward = slice gather B P^2 x entry + block-image
-    IFFT B P^2 x 12 B + warp K (B x 16 B of taps + 16 B rays / out);
-    adjoint = warp 2 x B K x 16 B + IFFT B P^2 x 12 B + slice B P^2 x entry
-    (entry: 64 B f32 / 32 B bf16 or f16 stencil entry), over the whole step time."""
-    peak, peak_kind = _peak_hbm()
-    fwd = B * P * P * entry + B * P * P * 12 + K * (B * 16 + 16)
-    adj = 2 * B * K * 16 + B * P * P * 12 + B * P * P * entry
-    achieved = (fwd + adj) * pose_evals_per_s / 1e9
-    return {"bound": "hbm", "alg_bytes_per_pose_eval": fwd + adj, "achieved": achieved, "peak": peak,
-            "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
-            "fallback 6.65 TB/s", "timing": "whole step (all kernels, eager autograd)"}
-
-
 _POU_SECTIONS = ("pou_slice", "pou_warp", "pou_warp_bwd", "pou_slice_adjoint")
 
 
@@ -460,17 +445,19 @@ def _pou_kernel_times(torch, step, steps, flush):
 
 def _pou_kernel_rooflines(kern_ms, B, N, P, entry):
     """Per-kernel HBM rooflines of the PoU step: algorithmic bytes per launch
-    over the kernel's event time.  Block-image kernels: every (block, pose)
-    slice sample reads one stencil entry (``entry`` bytes) and writes (forward)
-    or reads (adjoint) one float of the block image.  The warp kernels are
-    bound by issued instructions, not bytes: their times are listed only."""
+    over the kernel's event time.  Block-image kernels: the slice of a real
+    block is Hermitian, so one stencil entry (``entry`` bytes) per pair of
+    mirrored (block, pose) slice samples must be read, and each sample writes
+    (forward) or reads (adjoint) one float of the block image.  The warp
+    kernels are bound by issued instructions, not bytes: their times are
+    listed only."""
     peak, peak_kind = _peak_hbm()
     samples = B * N * P * P
     out = {"peak": peak, "unit": "GB/s", "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"
            if peak_kind == "measured" else "fallback 6.65 TB/s"}
     for name in ("pou_slice", "pou_slice_adjoint"):
         if name in kern_ms:
-            alg = samples * (entry + 4)
+            alg = samples * (entry // 2 + 4)
             ach = alg / (kern_ms[name] * 1e-3) / 1e9
             out[name] = {"ms": kern_ms[name], "alg_bytes_per_launch": alg, "achieved": ach, "frac": ach / peak}
     for name in ("pou_warp", "pou_warp_bwd"):
@@ -510,7 +497,6 @@ def _pou_leg(torch, dev, flush, warmup, steps):
         kern = _pou_kernel_times(torch, step, steps, flush)
         entry = 64 if name == "f32" else 32
         out[name] = {"value": value, "ms_per_step": ms, "blocks": int(m.B), "P": int(m.P),
-                     "roofline": _pou_roofline(int(m.B), int(m.P), 256 * 256, entry, value),
                      "kernels": _pou_kernel_rooflines(kern, int(m.B), CANDIDATES, int(m.P), entry)}
         del m, lattice
         torch.cuda.empty_cache()

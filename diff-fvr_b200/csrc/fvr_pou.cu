@@ -332,14 +332,148 @@ __device__ __forceinline__ void pou_table_sample(const Stencil& st, const Raw<DT
   }
 }
 
-// Smem layout of the fused image kernels: the P x (P + 1) complex image, then
-// the 2P-entry tables.
+// Smem layout of the fused forward image kernel: the P x (P + 1) complex
+// image, then the 2P-entry tables.
 __host__ __device__ constexpr int64_t pou_image_smem(int P) {
   return static_cast<int64_t>(P) * (P + 1) * 8 + 40 * 2 * static_cast<int64_t>(P) + 16;
 }
 
+// Hermitian pairing of slice samples.  A block is real, so its centred
+// spectrum obeys F[c + m] = conj F[c - m] for |m| < P/2 in every axis (grid
+// indices 1 .. P-1; index 0, the Nyquist plane, has no partner).  A slice
+// sample at c + k whose trilinear cell [i, i + 1] lies inside 1 .. P-1 in all
+// three axes therefore has the mirror sample S(c - k) = conj S(c + k), and the
+// spectrum's gradient there is -conj of the gradient at c + k.  The gradient
+// relation also needs the sample off the cell faces: on a face the trilinear
+// derivative is one-sided, and the side flips under the mirror, so the
+// adjoint pairs only samples whose fractions keep kPouMirrorMargin from 0 and 1.
+constexpr float kPouMirrorMargin = 1.f / 65536.f;
+
+__device__ __forceinline__ bool pou_mirror_cell(const TabCell& c, int P) {
+  const unsigned lim = static_cast<unsigned>(P - 3);  // cell i = e - 1 in 1 .. P-2
+  return static_cast<unsigned>(c.ex - 2) <= lim && static_cast<unsigned>(c.ey - 2) <= lim &&
+         static_cast<unsigned>(c.ez - 2) <= lim;
+}
+
+__device__ __forceinline__ bool pou_mirror_cell_deriv(const TabCell& c, int P) {
+  constexpr float lo = kPouMirrorMargin, hi = 1.f - kPouMirrorMargin;
+  return pou_mirror_cell(c, P) && c.tx >= lo && c.tx <= hi && c.ty >= lo && c.ty <= hi && c.tz >= lo && c.tz <= hi;
+}
+
+// Gathers slice row `i` (table order) at the natural-order columns lane + 32 m
+// into x.
+template <int DT, int M>
+__device__ __forceinline__ void pou_gather_row(const Stencil& st, const AxisTables& tab, int i, int lane,
+                                               Cx<float> (&x)[M]) {
+  constexpr int P = 32 * M, H = P / 2;
+  const int4 ia = tab.idx[P + i];
+  const float4 fa = tab.frac[P + i];
+  Raw<DT> raw[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int c = lane + 32 * m;
+    const int jj = c + H < P ? c + H : c - H;
+    tab_load<DT>(st, tab_cell(st, ia, fa, tab.idx[jj], tab.frac[jj]), raw[m]);
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int c = lane + 32 * m;
+    const int jj = c + H < P ? c + H : c - H;
+    Interp o;
+    pou_table_sample<DT, false>(st, raw[m], fa, tab.frac[jj], o);
+    x[m] = Cx<float>{o.sr, o.si};
+  }
+}
+
+// Value at natural column (P - c) mod P of a row held as lane + 32 m: lane
+// 32 - lane, register M - 1 - m; lane 0 keeps its own register (M - m) mod M.
+template <int M>
+__device__ __forceinline__ Cx<float> pou_row_mirror(const Cx<float> (&x)[M], int m, int lane) {
+  const int from = (32 - lane) & 31;
+  const float vx = __shfl_sync(0xffffffffu, x[M - 1 - m].x, from);
+  const float vy = __shfl_sync(0xffffffffu, x[M - 1 - m].y, from);
+  return lane == 0 ? x[(M - m) % M] : Cx<float>{vx, vy};
+}
+
+// Hermitian part (x[c] + conj x[-c]) / 2 of a row that is its own mirror (the
+// DC row and the Nyquist row, whose negated frequency is the row itself).
+template <int M>
+__device__ __forceinline__ void pou_row_hermitian(Cx<float> (&x)[M], int lane) {
+  Cx<float> v[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) v[m] = pou_row_mirror<M>(x, m, lane);
+#pragma unroll
+  for (int m = 0; m < M; ++m) x[m] = Cx<float>{0.5f * (x[m].x + v[m].x), 0.5f * (x[m].y - v[m].y)};
+}
+
+// Hermitian part of natural row u (1 <= u < P/2): h[c] = (S(u, c) +
+// conj S(P - u, P - c)) / 2.  Where the sample's cell has a Hermitian mirror
+// this is S(u, c) itself; the partner sample is gathered only elsewhere (the
+// Nyquist column, cells on the spectrum's border).  The first partner a lane
+// needs is loaded together with the row; further ones (rare) in more rounds.
+template <int DT, int M>
+__device__ __forceinline__ void pou_gather_row_hermitian(const Stencil& st, const AxisTables& tab, int u, int lane,
+                                                         Cx<float> (&h)[M]) {
+  constexpr int P = 32 * M, H = P / 2;
+  const int ti = u + H, tp = H - u;  // table rows of natural rows u and P - u
+  const int4 ia = tab.idx[P + ti], iap = tab.idx[P + tp];
+  const float4 fa = tab.frac[P + ti], fap = tab.frac[P + tp];
+  Raw<DT> raw[M];
+  unsigned pend = 0;
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int c = lane + 32 * m;
+    const int jj = c + H < P ? c + H : c - H;
+    const TabCell cell = tab_cell(st, ia, fa, tab.idx[jj], tab.frac[jj]);
+    if (c == H || !pou_mirror_cell(cell, P)) pend |= 1u << m;
+    tab_load<DT>(st, cell, raw[m]);
+  }
+  // partner of the first pending column, in the same round
+  int mp = pend ? __ffs(pend) - 1 : 0;
+  int jp = (P - ((lane + 32 * mp + H) % P)) % P;  // table column of natural column P - c
+  Raw<DT> rawp;
+  {
+    TabCell pc = tab_cell(st, iap, fap, tab.idx[jp], tab.frac[jp]);
+    if (!pend) pc.e = -1;
+    tab_load<DT>(st, pc, rawp);
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const int c = lane + 32 * m;
+    const int jj = c + H < P ? c + H : c - H;
+    Interp o;
+    pou_table_sample<DT, false>(st, raw[m], fa, tab.frac[jj], o);
+    h[m] = Cx<float>{o.sr, o.si};
+  }
+  for (;;) {
+    if (pend) {
+      Interp o;
+      pou_table_sample<DT, false>(st, rawp, fap, tab.frac[jp], o);
+#pragma unroll
+      for (int m = 0; m < M; ++m)
+        if (m == mp) h[m] = Cx<float>{0.5f * (h[m].x + o.sr), 0.5f * (h[m].y - o.si)};
+      pend &= pend - 1;
+    }
+    if (!__any_sync(0xffffffffu, pend != 0)) break;
+    mp = pend ? __ffs(pend) - 1 : 0;
+    jp = (P - ((lane + 32 * mp + H) % P)) % P;
+    TabCell pc = tab_cell(st, iap, fap, tab.idx[jp], tab.frac[jp]);
+    if (!pend) pc.e = -1;
+    tab_load<DT>(st, pc, rawp);
+  }
+}
+
 // imgs[b][n] = Re fftshift(ifft2(ifftshift(S))) for the slice S of block b at
 // pose n (the reference's _slice_and_ifft, cone_beam_fvr.py:480-505).
+//
+// Re ifft2(S) = ifft2(Herm S) with Herm S(k) = (S(k) + conj S(-k)) / 2 (index
+// -k mod P), and the slice of a real block is Hermitian wherever the mirror
+// relation above holds, so Herm S needs about half of the slice's stencil
+// entries.  Herm S is Hermitian by construction, so the row pass transforms
+// natural rows 0 .. P/2 only (rows P - u are the conjugates of rows u; rows 0
+// and P/2 are real after the transform and share one FFT as real and
+// imaginary part), and the column pass transforms two real-output columns per
+// complex FFT.  That is P/2 + P/2 FFTs instead of 2P.
 template <int DT, int M>
 __global__ void __launch_bounds__(kPouImgThreads, 1) pou_slice_ifft_kernel(PouSliceArgs a, float* __restrict__ imgs) {
   constexpr int P = 32 * M, PITCH = P + 1, H = P / 2, NW = kPouImgThreads / 32;
@@ -353,128 +487,259 @@ __global__ void __launch_bounds__(kPouImgThreads, 1) pou_slice_ifft_kernel(PouSl
   WarpFft<M, true> fft;
   fft.init(lane);
   __syncthreads();
-  // rows: gather the ifftshift-ordered slice row straight into registers
-  for (int r = wid; r < P; r += NW) {
-    const int i = r + H < P ? r + H : r - H;
-    const int4 ia = tab.idx[P + i];
-    const float4 fa = tab.frac[P + i];
-    Raw<DT> raw[M];
-    int jj[M];
+  // rows: unit 0 = natural rows 0 and H (table rows H and 0), unit u = row u
+  for (int u = wid; u < H; u += NW) {
+    Cx<float> h[M];
+    if (u == 0) {
+      Cx<float> x[M];
+      pou_gather_row<DT, M>(st, tab, H, lane, x);
+      pou_row_hermitian<M>(x, lane);
+      pou_gather_row<DT, M>(st, tab, 0, lane, h);
+      pou_row_hermitian<M>(h, lane);
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      const int c = lane + 32 * m;
-      jj[m] = c + H < P ? c + H : c - H;
-      const TabCell cell = tab_cell(st, ia, fa, tab.idx[jj[m]], tab.frac[jj[m]]);
-      tab_load<DT>(st, cell, raw[m]);
+      for (int m = 0; m < M; ++m) h[m] = Cx<float>{x[m].x - h[m].y, x[m].y + h[m].x};
+    } else {
+      pou_gather_row_hermitian<DT, M>(st, tab, u, lane, h);
     }
-    Cx<float> x[M];
+    fft.run(h, lane);
+    if (u == 0) {
 #pragma unroll
-    for (int m = 0; m < M; ++m) {
-      Interp o;
-      pou_table_sample<DT, false>(st, raw[m], fa, tab.frac[jj[m]], o);
-      x[m] = Cx<float>{o.sr, o.si};
+      for (int k = 0; k < M; ++k) {
+        buf[lane + 32 * k] = Cx<float>{h[k].x, 0.f};
+        buf[H * PITCH + lane + 32 * k] = Cx<float>{h[k].y, 0.f};
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < M; ++k) buf[u * PITCH + lane + 32 * k] = h[k];
     }
-    fft.run(x, lane);
-#pragma unroll
-    for (int k = 0; k < M; ++k) buf[r * PITCH + lane + 32 * k] = x[k];
   }
   __syncthreads();
-  // columns, in place (each warp owns whole columns)
-  for (int cc = wid; cc < P; cc += NW) {
-    Cx<float> x[M];
+  // columns: buffer columns 2t and 2t + 1 as real and imaginary part of one
+  // transform (rows r > H read as the conjugate of row P - r); the real
+  // results of both land in column 2t
+  for (int t = wid; t < H; t += NW) {
+    const int c1 = 2 * t;
+    Cx<float> z[M];
 #pragma unroll
-    for (int m = 0; m < M; ++m) x[m] = buf[(lane + 32 * m) * PITCH + cc];
-    fft.run(x, lane);
+    for (int m = 0; m < M; ++m) {
+      const int r = lane + 32 * m;
+      const int rr = r <= H ? r : P - r;
+      const float sg = r <= H ? 1.f : -1.f;
+      const Cx<float> p = buf[rr * PITCH + c1], q = buf[rr * PITCH + c1 + 1];
+      z[m] = Cx<float>{p.x - sg * q.y, sg * p.y + q.x};
+    }
+    fft.run(z, lane);
 #pragma unroll
-    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + cc] = x[k];
+    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + c1] = z[k];
   }
   __syncthreads();
-  // fftshift-ordered real part, coalesced rows
+  // fftshift-ordered image, coalesced rows
   const float scale = 1.f / static_cast<float>(P * P);
   float* out = imgs + (static_cast<int64_t>(b) * a.N + n) * P * P;
   for (int q = threadIdx.x; q < P * P; q += kPouImgThreads) {
     const int y = q / P, xq = q - y * P;
     const int ky = y + H < P ? y + H : y - H, kx = xq + H < P ? xq + H : xq - H;
-    out[q] = buf[wfft_pos<M>(ky) * PITCH + wfft_pos<M>(kx)].x * scale;
+    const int px = wfft_pos<M>(kx);
+    const Cx<float> v = buf[wfft_pos<M>(ky) * PITCH + (px & ~1)];
+    out[q] = ((px & 1) ? v.y : v.x) * scale;
   }
 }
 
+// Shared memory of the adjoint: the row-pair spectra [P/2][P + 1], the half
+// spectrum G [P][P/2 + 1], the axis tables, one partner queue per warp.
+constexpr int kPouQueue = 256;
+
+__host__ __device__ constexpr int64_t pou_adjoint_tables_at(int P) {
+  return ((static_cast<int64_t>(P / 2) * (P + 1) + static_cast<int64_t>(P) * (P / 2 + 1)) * 8 + 15) / 16 * 16;
+}
+
+__host__ __device__ constexpr int64_t pou_adjoint_smem(int P) {
+  return pou_adjoint_tables_at(P) + 40 * 2 * static_cast<int64_t>(P) + (kPouImgThreads / 32) * kPouQueue * 2;
+}
+
+// G at natural frequency indices (ki, kj) from the stored half kj <= P/2
+// (rows in transform order): G(-k) = conj G(k) for the transform of a real image.
+template <int M>
+__device__ __forceinline__ Cx<float> pou_half_spectrum(const Cx<float>* gb, int ki, int kj) {
+  constexpr int P = 32 * M, H = P / 2, GP = H + 1;
+  if (kj <= H) return gb[wfft_pos<M>(ki) * GP + kj];
+  const Cx<float> v = gb[wfft_pos<M>(ki == 0 ? 0 : P - ki) * GP + (P - kj)];
+  return Cx<float>{v.x, -v.y};
+}
+
+// acc += w (fx, fy) x <G, dS/dp> for the sample at table position (i, j).
+template <int DT, int M>
+__device__ __forceinline__ void pou_adjoint_sample(const Stencil& st, const AxisTables& tab, const Cx<float>* gb,
+                                                   const Raw<DT>& raw, int i, int j, float w, float (&acc)[6]) {
+  constexpr int P = 32 * M, H = P / 2;
+  const float4 fa = tab.frac[P + i], fb = tab.frac[j];
+  Interp o;
+  pou_table_sample<DT, true>(st, raw, fa, fb, o);
+  const Cx<float> G = pou_half_spectrum<M>(gb, i + H < P ? i + H : i - H, j + H < P ? j + H : j - H);
+  const float gx = G.x * w, gy = G.y * w;
+  const float e0 = gx * o.dxr + gy * o.dxi, e1 = gx * o.dyr + gy * o.dyi, e2 = gx * o.dzr + gy * o.dzi;
+  const float fx = fb.w, fy = fa.w;
+  acc[0] = fmaf(fx, e0, acc[0]);
+  acc[1] = fmaf(fx, e1, acc[1]);
+  acc[2] = fmaf(fx, e2, acc[2]);
+  acc[3] = fmaf(fy, e0, acc[3]);
+  acc[4] = fmaf(fy, e1, acc[4]);
+  acc[5] = fmaf(fy, e2, acc[5]);
+}
+
+// One warp's pass over `cnt` (<= 32 GROUP) queued samples from `head`.
+template <int DT, int M, int GROUP>
+__device__ __forceinline__ void pou_adjoint_queue(const Stencil& st, const AxisTables& tab, const Cx<float>* gb,
+                                                  const unsigned short* queue, int head, int cnt, int lane,
+                                                  float wscale, float (&acc)[6]) {
+  constexpr int P = 32 * M;
+  Raw<DT> raw[GROUP];
+  int qq[GROUP];
+#pragma unroll
+  for (int u = 0; u < GROUP; ++u) {
+    const bool ok = lane + 32 * u < cnt;
+    const int q = ok ? queue[(head + lane + 32 * u) & (kPouQueue - 1)] : 0;
+    qq[u] = ok ? q : -1;
+    const int i = q / P, j = q - (q / P) * P;
+    TabCell cell = tab_cell(st, tab.idx[P + i], tab.frac[P + i], tab.idx[j], tab.frac[j]);
+    if (!ok) cell.e = -1;
+    tab_load<DT>(st, cell, raw[u]);
+  }
+#pragma unroll
+  for (int u = 0; u < GROUP; ++u)
+    if (qq[u] >= 0) pou_adjoint_sample<DT, M>(st, tab, gb, raw[u], qq[u] / P, qq[u] % P, wscale, acc);
+  __syncwarp();
+}
+
 // Adjoint of pou_slice_ifft_kernel for one (pose, block): G = fftshift(fft2(
-// ifftshift(g))) / P^2 in shared memory, then per slice sample the products
-// of G with the spectrum's spatial derivatives, weighted by fx and fy:
+// ifftshift(g))) / P^2, then per slice sample the products of G with the
+// spectrum's spatial derivatives, weighted by fx and fy:
 // partial[n][b][6] = sum (fx <G, dS/dp_k>, fy <G, dS/dp_k>), k = x, y, z.
+//
+// G of a real image is Hermitian, so it is formed for kx <= P/2 only: the row
+// pass transforms image rows two at a time (real and imaginary part of one
+// FFT), the column pass separates them and transforms the P/2 + 1 columns
+// needed.  A slice sample and its mirror (fx, fy, dS/dp change sign, G and
+// dS/dp are conjugated) contribute the same products, so one stencil gather
+// serves both wherever the mirror relation holds: the loop runs over the
+// samples of positive row frequency (plus the Nyquist column), counts those
+// with a mirror twice, and queues the partners of the others; the Nyquist row
+// has no partner and goes through the queue once.
 template <int DT, int M>
 __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kernel(PouSliceArgs a,
                                                                                   const float* __restrict__ gimg,
                                                                                   double* __restrict__ partial) {
-  constexpr int P = 32 * M, PITCH = P + 1, H = P / 2, NW = kPouImgThreads / 32, GROUP = 4;
+  constexpr int P = 32 * M, PITCH = P + 1, H = P / 2, GP = H + 1, NW = kPouImgThreads / 32, GROUP = 4;
+  constexpr int BATCH = 32 * GROUP, NQ = P / NW;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[6 * NW];
-  Cx<float>* buf = reinterpret_cast<Cx<float>*>(smem);
-  const AxisTables tab = axis_tables(smem + ((static_cast<int64_t>(P) * PITCH * 8 + 15) / 16) * 16, 2 * P);
+  Cx<float>* zr = reinterpret_cast<Cx<float>*>(smem);
+  Cx<float>* gb = zr + H * PITCH;
+  const AxisTables tab = axis_tables(smem + pou_adjoint_tables_at(P), 2 * P);
   const int n = blockIdx.x, b = blockIdx.y;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned short* queue =
+      reinterpret_cast<unsigned short*>(smem + pou_adjoint_tables_at(P) + 80 * P) + wid * kPouQueue;
   const Stencil st = pou_block_stencil(a, b);
   pou_image_tables(tab, a, a.geo + n * kGeo);
   WarpFft<M, false> fft;
   fft.init(lane);
   const float* g = gimg + (static_cast<int64_t>(b) * a.N + n) * P * P;
-  for (int r = wid; r < P; r += NW) {
-    const int y = r + H < P ? r + H : r - H;
-    Cx<float> x[M];
+  // rows: transform input rows 2s, 2s + 1 (image rows y0, y0 + 1 after ifftshift) together
+  for (int s = wid; s < H; s += NW) {
+    const int y0 = 2 * s + H < P ? 2 * s + H : 2 * s - H;
+    Cx<float> z[M];
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       const int c = lane + 32 * m;
-      x[m] = Cx<float>{__ldg(g + y * P + (c + H < P ? c + H : c - H)), 0.f};
+      const int xc = c + H < P ? c + H : c - H;
+      z[m] = Cx<float>{__ldg(g + y0 * P + xc), __ldg(g + (y0 + 1) * P + xc)};
+    }
+    fft.run(z, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) zr[s * PITCH + lane + 32 * k] = z[k];
+  }
+  __syncthreads();
+  // columns kx = 0 .. P/2: split the pair spectra (Z(k) + conj Z(-k)) / 2 and
+  // (Z(k) - conj Z(-k)) / 2i, then transform over the rows
+  for (int kx = wid; kx <= H; kx += NW) {
+    const int p0 = wfft_pos<M>(kx), p1 = wfft_pos<M>(kx == 0 ? 0 : P - kx);
+    Cx<float> x[M];
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      const int y = lane + 32 * m, sr = (y >> 1) * PITCH;
+      const Cx<float> A = zr[sr + p0], B = zr[sr + p1];
+      x[m] = (y & 1) ? Cx<float>{0.5f * (A.y + B.y), 0.5f * (B.x - A.x)}
+                     : Cx<float>{0.5f * (A.x + B.x), 0.5f * (A.y - B.y)};
     }
     fft.run(x, lane);
 #pragma unroll
-    for (int k = 0; k < M; ++k) buf[r * PITCH + lane + 32 * k] = x[k];
+    for (int k = 0; k < M; ++k) gb[(lane + 32 * k) * GP + kx] = x[k];
   }
-  __syncthreads();
-  for (int cc = wid; cc < P; cc += NW) {
-    Cx<float> x[M];
-#pragma unroll
-    for (int m = 0; m < M; ++m) x[m] = buf[(lane + 32 * m) * PITCH + cc];
-    fft.run(x, lane);
-#pragma unroll
-    for (int k = 0; k < M; ++k) buf[(lane + 32 * k) * PITCH + cc] = x[k];
-  }
+  // the Nyquist row (table row 0) starts the queue
+  if (lane < NQ) queue[lane] = static_cast<unsigned short>(wid * NQ + lane);
+  int head = 0, tail = NQ;
   __syncthreads();
   const float scale = 1.f / static_cast<float>(P * P);
   float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  for (int q0 = threadIdx.x; q0 < P * P; q0 += kPouImgThreads * GROUP) {
+  const unsigned below = (1u << lane) - 1u;
+  // own samples t < H P: table rows H+1 .. P-1 (all columns), row H (columns
+  // 0 and H .. P-1), rows 1 .. H-1 (column 0); H P is a multiple of the
+  // thread count, so every warp runs the same iterations
+  for (int t0 = threadIdx.x; t0 < H * P; t0 += kPouImgThreads * GROUP) {
     Raw<DT> raw[GROUP];
-    int qq[GROUP];
+    int qi[GROUP], qj[GROUP];
+    float wt[GROUP];
 #pragma unroll
     for (int u = 0; u < GROUP; ++u) {
-      const int q = q0 + u * kPouImgThreads;
-      qq[u] = q;
-      const int i = q < P * P ? q / P : 0, j = q < P * P ? q - (q / P) * P : 0;
+      const int t = t0 + u * kPouImgThreads;
+      int i, j;
+      if (t < (H - 1) * P) {
+        i = H + 1 + t / P;
+        j = t - (t / P) * P;
+      } else if (t < (H - 1) * P + H + 1) {
+        i = H;
+        j = t == (H - 1) * P ? 0 : H + t - (H - 1) * P - 1;
+      } else if (t < H * P) {
+        i = t - (H - 1) * P - H;
+        j = 0;
+      } else {
+        i = 0;
+        j = 0;
+      }
       TabCell cell = tab_cell(st, tab.idx[P + i], tab.frac[P + i], tab.idx[j], tab.frac[j]);
-      if (q >= P * P) cell.e = -1;
+      float w = t < H * P ? scale : 0.f;
+      bool need = false;
+      if (j >= 1 && (i > H || (i == H && j > H)) && w != 0.f) {
+        if (pou_mirror_cell_deriv(cell, P)) {
+          w *= 2.f;
+        } else {
+          const TabCell pc = tab_cell(st, tab.idx[2 * P - i], tab.frac[2 * P - i], tab.idx[P - j], tab.frac[P - j]);
+          need = pc.e >= 0;
+        }
+      }
+      const unsigned mask = __ballot_sync(0xffffffffu, need);
+      if (need) queue[(tail + __popc(mask & below)) & (kPouQueue - 1)] = static_cast<unsigned short>((P - i) * P + P - j);
+      tail += __popc(mask);
+      if (w == 0.f) cell.e = -1;
+      qi[u] = i;
+      qj[u] = j;
+      wt[u] = w;
       tab_load<DT>(st, cell, raw[u]);
     }
 #pragma unroll
-    for (int u = 0; u < GROUP; ++u) {
-      const int q = qq[u];
-      if (q >= P * P) continue;
-      const int i = q / P, j = q - i * P;
-      const float4 fa = tab.frac[P + i], fb = tab.frac[j];
-      Interp o;
-      pou_table_sample<DT, true>(st, raw[u], fa, fb, o);
-      const int ki = i + H < P ? i + H : i - H, kj = j + H < P ? j + H : j - H;
-      const Cx<float> G = buf[wfft_pos<M>(ki) * PITCH + wfft_pos<M>(kj)];
-      const float gx = G.x * scale, gy = G.y * scale;
-      const float e0 = gx * o.dxr + gy * o.dxi, e1 = gx * o.dyr + gy * o.dyi, e2 = gx * o.dzr + gy * o.dzi;
-      const float fx = fb.w, fy = fa.w;
-      acc[0] = fmaf(fx, e0, acc[0]);
-      acc[1] = fmaf(fx, e1, acc[1]);
-      acc[2] = fmaf(fx, e2, acc[2]);
-      acc[3] = fmaf(fy, e0, acc[3]);
-      acc[4] = fmaf(fy, e1, acc[4]);
-      acc[5] = fmaf(fy, e2, acc[5]);
+    for (int u = 0; u < GROUP; ++u)
+      if (wt[u] != 0.f) pou_adjoint_sample<DT, M>(st, tab, gb, raw[u], qi[u], qj[u], wt[u], acc);
+    __syncwarp();
+    if (tail - head >= BATCH) {
+      pou_adjoint_queue<DT, M, GROUP>(st, tab, gb, queue, head, BATCH, lane, scale, acc);
+      head += BATCH;
     }
+  }
+  while (tail > head) {
+    const int cnt = tail - head < BATCH ? tail - head : BATCH;
+    pou_adjoint_queue<DT, M, GROUP>(st, tab, gb, queue, head, cnt, lane, scale, acc);
+    head += cnt;
   }
 #pragma unroll
   for (int m = 0; m < 6; ++m) {
@@ -1137,7 +1402,7 @@ using namespace fvr;
 template <int DT, int M>
 static int pou_image_launch(bool adjoint, const PouSliceArgs& a, int B, const float* gimg, float* imgs,
                             double* part, cudaStream_t s) {
-  const int64_t smem = pou_image_smem(32 * M);
+  const int64_t smem = adjoint ? pou_adjoint_smem(32 * M) : pou_image_smem(32 * M);
   dim3 grid(static_cast<unsigned>(a.N), static_cast<unsigned>(B));
   if (adjoint) {
     static bool attr = false;

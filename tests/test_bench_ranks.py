@@ -50,11 +50,12 @@ def test_reference_arm_other_ranks_exit_without_work():
 
 
 def test_scope_table_byte_counts():
-    """The bench's logical byte counts reproduce the hot-path scope table's
-    per-pose-eval figures: 4.46 MB (f32) and 2.36 MB (bf16) for the batched
-    spectral-NCC step at out_res 128 with 2 views, and about 294 MB for the
-    PoU step at 52 blocks (P = 128, 256^2 detector, f32); the bytes that
-    step must read (8 corners once + the 8 B target per sample) beside them."""
+    """The bench's logical byte counts reproduce the per-pose-eval figures of
+    the spectral-NCC step: 4.46 MB (f32) and 2.36 MB (bf16) at out_res 128
+    with 2 views, with the bytes that step must read (8 corners once + the
+    8 B target per sample) beside them.  The PoU block-image kernels count
+    one stencil entry per mirrored pair of slice samples plus one image float
+    per sample."""
     sys.path.insert(0, str(REPO))
     import bench
 
@@ -65,5 +66,6 @@ def test_scope_table_byte_counts():
     assert abs(per_eval["f32"] / 1e6 - 4.46) < 0.01
     assert abs(per_eval["bf16"] / 1e6 - 2.36) < 0.01
     assert abs(per_eval["f16"] / 1e6 - 2.49) < 0.01  # + 4 B brick scale per sample
-    pou = bench._pou_roofline(52, 128, 256 * 256, 64, 1.0)["alg_bytes_per_pose_eval"]
-    assert abs(pou / 1e6 - 294.1) < 0.2
+    pou = bench._pou_kernel_rooflines({"pou_slice": 1.0, "pou_slice_adjoint": 1.0}, 52, 64, 128, 64)
+    for k in ("pou_slice", "pou_slice_adjoint"):  # one 64 B entry per mirrored sample pair + one image float
+        assert pou[k]["alg_bytes_per_launch"] == 52 * 64 * 128 * 128 * (32 + 4)

@@ -396,12 +396,20 @@ def test_edge_dominant_ncc_vs_torch64(B, Bt, C, H, W, crop, w, mean):
 # ------------------------------------------------ fused block-image kernels
 
 
-@pytest.mark.parametrize("block_res,dtype", [(32, torch.float32), (48, torch.bfloat16), (64, torch.float32),
-                                             (64, torch.bfloat16), (80, torch.float32)])
+@pytest.mark.parametrize("block_res,dtype", [(32, torch.float32), (48, torch.bfloat16), (48, torch.float16),
+                                             (64, torch.float32), (64, torch.bfloat16), (80, torch.float32),
+                                             (80, torch.float16)])
 def test_fused_block_images_match_slice_plus_fft(block_res, dtype):
     """fvr_pou_slice_image (slice + inverse FFT in one CTA) and its adjoint
     equal the unfused slice kernel + batched FFT path, P = 2 x block_res in
-    {64, 96, 128, 160}."""
+    {64, 96, 128, 160}.
+
+    The fused kernels read one sample of each Hermitian pair (S(-k) =
+    conj S(k)) where the unfused path reads both.  The two are separate
+    roundings of conjugate spectrum values: identical in f32 up to the FFT's
+    own rounding, and one 16-bit step apart wherever that rounding moves a
+    value across a 16-bit boundary (block spectra of lengths with a factor 3
+    or 5), hence the looser 16-bit bounds."""
     import ctypes
 
     import fvr._lib as L
@@ -430,7 +438,8 @@ def test_fused_block_images_match_slice_plus_fft(block_res, dtype):
     L.call("fvr_pou_slice", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N, L.ptr(m._freqs),
            L.ptr(slices), s)
     ref = RT.fft2d(slices, inverse=True, out_shift=RT.SHIFT_FFT, scale=1.0 / (P * P), out_mode=RT.OUT_REAL)
-    assert rel_l2(fused.cpu().numpy(), ref.cpu().numpy()) < 2e-6
+    tol_fwd, tol_adj = (2e-6, 2e-5) if dtype == torch.float32 else (1e-5, 2e-4)
+    assert rel_l2(fused.cpu().numpy(), ref.cpu().numpy()) < tol_fwd
     # adjoint against the unfused FFT + slice adjoint (tile sums)
     g = torch.from_numpy(np.random.default_rng(1).standard_normal((B, N, P, P)).astype(np.float32)).to(dev)
     wsb = L.query("fvr_pou_slice_image_adjoint_workspace", B, N)
@@ -445,4 +454,4 @@ def test_fused_block_images_match_slice_plus_fft(block_res, dtype):
            L.ptr(m._freqs), L.ptr(G), L.ptr(ws2), wsb2, s)
     tiles = (P * P + 255) // 256
     want = ws2[: N * B * tiles * 6 * 8].view(torch.float64).view(N, B, tiles, 6).sum(2).cpu().numpy()
-    assert rel_l2(got, want) < 2e-5
+    assert rel_l2(got, want) < tol_adj
