@@ -448,9 +448,12 @@ def _pou_kernel_rooflines(kern_ms, B, N, P, entry):
     over the kernel's event time.  Block-image kernels: the slice of a real
     block is Hermitian, so one stencil entry (``entry`` bytes) per pair of
     mirrored (block, pose) slice samples must be read, and each sample writes
-    (forward) or reads (adjoint) one float of the block image.  The warp
-    kernels are bound by issued instructions, not bytes: their times are
-    listed only."""
+    (forward) or reads (adjoint) one float of the block image.  On the
+    separable pinhole lattice the adjoint section is one fused launch that
+    also does the warp adjoint (it reads the forward image instead of an
+    image gradient), so no pou_warp_bwd section appears.  The warp kernels
+    are bound by issued instructions, not bytes: their times are listed
+    only."""
     peak, peak_kind = _peak_hbm()
     samples = B * N * P * P
     out = {"peak": peak, "unit": "GB/s", "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"

@@ -77,6 +77,7 @@ enum : unsigned {
   kSiteWarpGrad,          // PoU warp adjoint image-gradient atomic
   kSiteWarpStrip,         // PoU warp row-strip shared-memory access
   kSiteWarpStripRow,      // PoU warp row-strip image row read
+  kSiteWarpFused,         // fused PoU warp adjoint: detector-row buffer and column-map reads
 };
 
 template <typename T>

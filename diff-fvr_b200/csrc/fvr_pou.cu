@@ -611,6 +611,252 @@ __device__ __forceinline__ void pou_adjoint_queue(const Stencil& st, const AxisT
   __syncwarp();
 }
 
+// Detector side of the fused warp + block-image adjoint, for a separable
+// pinhole lattice: every detector column shares one ray coordinate rx and
+// every detector row one ry (the invariant lattice's rays agree per column and
+// per row up to float rounding; rxc / ryr hold the midpoints).  Block b of pose
+// n then samples image column ix + tx = (d_b rx - cu) / ds + c of every pixel
+// in a column and image row iy + ty = (d_b ry - cv) / ds + c of every pixel in
+// a row, so the warp's adjoint separates: per detector row r, a gather along x
+// (no atomics) gives T_r[x] = sum_c g[r][c] wx(c, x) and its x-slope versions;
+// image row iy(r) receives (1 - ty) T_r and row iy(r) + 1 receives ty T_r.
+struct PouWarpSep {
+  const float* imgs;   // [B][N][P][P] forward block images
+  const double* offs;  // [B][N][3]: d_b, cu, cv
+  const float* rxc;    // [W] column ray coordinate
+  const float* ryr;    // [Hd] row ray coordinate
+  const float* ic;     // [Hd W]
+  const float* gout;   // [N][Hd W]
+  double* goffs;       // [3][B][N]: dL/d(d_b, cu, cv)
+  int Hd, W;
+  double inv_ds, c_idx;
+};
+
+// Shared memory of the fused adjoint beyond the block-image adjoint's: one
+// detector-row buffer per warp [16][W + 4], column map (ix, tx) [W], row map
+// (iy, ty) [Hd], per image index -1 .. P-1 the first and last detector column
+// and row with that index [4][P + 1].
+constexpr int kPouFusedMaxW = 256;
+
+__host__ __device__ constexpr int64_t pou_fused_extra(int P, int Hd, int W) {
+  return 4LL * (kPouImgThreads / 32) * (W + 4) + 8LL * W + 8LL * Hd + 16LL * (P + 1);
+}
+
+__host__ __device__ constexpr int64_t pou_fused_smem(int P, int Hd, int W) {
+  return (pou_adjoint_smem(P) + 15) / 16 * 16 + pou_fused_extra(P, Hd, W);
+}
+
+// dL/dimgs of block b at pose n into `gimg` [P][P] (shared memory, zeroed
+// here) and the pose-offset sums (sum g dv/dpx, sum g rx dv/dpx, sum g dv/dpy,
+// sum g ry dv/dpy) of this (pose, block), with the forward image staged in
+// `img` [P][P].  The x gather of a detector row is T[x] = sum of the row's
+// values over image column x's taps (every row has the same taps).  Warp w
+// owns image rows [(w/2) P/8, (w/2 + 1) P/8) at the columns of half w % 2 of
+// the image, whose taps its lanes hold in registers: it runs over the
+// detector rows whose iy lies in [(w/2) P/8 - 1, (w/2 + 1) P/8 - 1] and adds
+// only into its own rows and columns, so no two warps write one element; a
+// detector row's sums are counted by the warps owning image row max(iy, 0),
+// each over its own columns.
+template <int M>
+__device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N, unsigned char* sep, float* img,
+                                        float* gimg, double (&sums)[4]) {
+  constexpr int P = 32 * M, NW = kPouImgThreads / 32;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int W = w.W, Hd = w.Hd;
+  float* wbuf = reinterpret_cast<float*>(sep);
+  int2* cmap = reinterpret_cast<int2*>(wbuf + NW * (W + 4));
+  int2* rmap = cmap + W;
+  int* clo = reinterpret_cast<int*>(rmap + Hd);
+  int* chi = clo + (P + 1);
+  int* rlo = chi + (P + 1);
+  int* rhi = rlo + (P + 1);
+  const double* o = w.offs + 3 * (static_cast<int64_t>(b) * N + n);
+  const double db = o[0], cu = o[1], cv = o[2];
+  for (int k = threadIdx.x; k < 4 * (P + 1); k += kPouImgThreads) clo[k] = ((k / (P + 1)) & 1) ? -1 : 0x7fffffff;
+  for (int c = threadIdx.x; c < W; c += kPouImgThreads) {
+    const double px = (db * static_cast<double>(__ldg(w.rxc + c)) - cu) * w.inv_ds + w.c_idx;
+    const bool ok = px > -1.0 && px < static_cast<double>(P);
+    const double f = floor(px);
+    cmap[c] = make_int2(ok ? static_cast<int>(f) : -2, __float_as_int(static_cast<float>(px - f)));
+  }
+  for (int r = threadIdx.x; r < Hd; r += kPouImgThreads) {
+    const double py = (db * static_cast<double>(__ldg(w.ryr + r)) - cv) * w.inv_ds + w.c_idx;
+    const bool ok = py > -1.0 && py < static_cast<double>(P);
+    const double f = floor(py);
+    rmap[r] = make_int2(ok ? static_cast<int>(f) : -2, __float_as_int(static_cast<float>(py - f)));
+  }
+  const float4* src = reinterpret_cast<const float4*>(w.imgs + (static_cast<int64_t>(b) * N + n) * P * P);
+  for (int q = threadIdx.x; q < P * P / 4; q += kPouImgThreads) {
+    reinterpret_cast<float4*>(img)[q] = __ldg(src + q);
+    reinterpret_cast<float4*>(gimg)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < W; c += kPouImgThreads) {
+    const int ix = cmap[c].x;
+    if (ix >= -1) {
+      atomicMin(clo + ix + 1, c);
+      atomicMax(chi + ix + 1, c);
+    }
+  }
+  for (int r = threadIdx.x; r < Hd; r += kPouImgThreads) {
+    const int iy = rmap[r].x;
+    if (iy >= -1) {
+      atomicMin(rlo + iy + 1, r);
+      atomicMax(rhi + iy + 1, r);
+    }
+  }
+  __syncthreads();
+  // warp = (row group, column half): the image rows that receive
+  // contributions, [Y0, Y1], split in 8 equal bands, and the image columns
+  // [h P/2, (h + 1) P/2); each lane keeps its columns' taps in registers
+  constexpr int HALF = P / 2, MW = (HALF + 31) / 32, TCR = 6;
+  const int rg = wid >> 1, h = wid & 1, xa = h * HALF;
+  int ylo = 0x7fffffff, yhi = -1;  // valid iy + 1 range
+  for (int k = lane; k <= P; k += 32)
+    if (rlo[k] <= rhi[k]) {
+      ylo = min(ylo, k);
+      yhi = max(yhi, k);
+    }
+  ylo = __reduce_min_sync(0xffffffffu, ylo);
+  yhi = __reduce_max_sync(0xffffffffu, yhi);
+  if (ylo > yhi) return;
+  const int Y0 = max(ylo - 1, 0), Y1 = min(yhi, P - 1);  // rows iy and iy + 1 of the valid detector rows
+  const int y_lo = Y0 + (rg * (Y1 - Y0 + 1)) / 8, y_hi = Y0 + ((rg + 1) * (Y1 - Y0 + 1)) / 8;
+  if (y_lo >= y_hi) return;
+  int ra = 0x7fffffff, rb = -1;  // detector rows with iy + 1 in [y_lo, y_hi]
+  for (int k = y_lo + lane; k <= y_hi; k += 32) {
+    ra = min(ra, rlo[k]);
+    rb = max(rb, rhi[k]);
+  }
+  int ca = 0x7fffffff, cb = -1;  // detector columns with ix + 1 in [xa, xa + HALF]
+  for (int k = xa + lane; k <= xa + HALF; k += 32) {
+    ca = min(ca, clo[k]);
+    cb = max(cb, chi[k]);
+  }
+  ra = __reduce_min_sync(0xffffffffu, ra);
+  rb = __reduce_max_sync(0xffffffffu, rb);
+  ca = __reduce_min_sync(0xffffffffu, ca);
+  cb = __reduce_max_sync(0xffffffffu, cb);
+  if (ra > rb || ca > cb) return;
+  ca &= ~3;  // float4 staging from a 16-byte boundary (W is a multiple of 4)
+  const int nq = (cb - ca + 4) / 4, ncw = 4 * nq;  // staged float4 chunks, columns
+  float* mybuf = wbuf + static_cast<int64_t>(wid) * (W + 4);  // the row's columns [ca, ca + ncw), then a zero
+  // taps of image column x: detector columns with ix == x (weight 1 - tx,
+  // slope -1) and ix == x - 1 (weight tx, slope +1); unused slots read the zero
+  int toff[MW][TCR];  // mybuf index, sign bit set for slope -1
+  float tw[MW][TCR], trx[MW][TCR];
+  bool over = false;
+#pragma unroll
+  for (int m = 0; m < MW; ++m) {
+#pragma unroll
+    for (int k = 0; k < TCR; ++k) {
+      toff[m][k] = ncw;
+      tw[m][k] = 0.f;
+      trx[m][k] = 0.f;
+    }
+    const int x = xa + lane + 32 * m;
+    if (lane + 32 * m >= HALF) continue;
+    // the columns of one index form the range [clo, chi] when px is monotone
+    // in the column (checked per tap; otherwise the column loops below)
+    const int a0 = clo[x + 1], a1 = clo[x];
+    const int n0 = max(chi[x + 1] - a0 + 1, 0), n1 = max(chi[x] - a1 + 1, 0);
+    over |= n0 + n1 > TCR;
+#pragma unroll
+    for (int q = 0; q < TCR; ++q) {
+      if (q >= n0 + n1) continue;
+      const bool cls = q >= n0;  // false: ix == x, true: ix == x - 1
+      const int c = cls ? a1 + q - n0 : a0 + q;
+      const int2 e = cmap[c];
+      over |= e.x != (cls ? x - 1 : x);
+      const float t = __int_as_float(e.y), rx = __ldg(w.rxc + c);
+      toff[m][q] = (c - ca) | (cls ? 0 : static_cast<int>(0x80000000u));
+      tw[m][q] = cls ? t : 1.f - t;
+      trx[m][q] = cls ? rx : -rx;
+    }
+  }
+  const bool regs = !__any_sync(0xffffffffu, over);  // else the column loops below
+  const float4* gp = reinterpret_cast<const float4*>(w.gout + static_cast<int64_t>(n) * Hd * W);
+  const float4* ip = reinterpret_cast<const float4*>(w.ic);
+  constexpr int NJ = kPouFusedMaxW / 128;  // float4 chunks per lane
+  float4 gv[NJ], iv[NJ];
+  auto load = [&](int r) {
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const int q = lane + 32 * j;
+      const int64_t e = (static_cast<int64_t>(r) * W + ca) / 4 + q;
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      gv[j] = q < nq ? __ldg(gp + e) : z;
+      iv[j] = q < nq ? __ldg(ip + e) : z;
+    }
+  };
+  if (lane == 0) mybuf[ncw] = 0.f;
+  load(ra);
+  for (int r = ra; r <= rb; ++r) {
+#pragma unroll
+    for (int j = 0; j < NJ; ++j)
+      if (lane + 32 * j < nq)
+        reinterpret_cast<float4*>(mybuf)[lane + 32 * j] =
+            make_float4(gv[j].x * iv[j].x, gv[j].y * iv[j].y, gv[j].z * iv[j].z, gv[j].w * iv[j].w);
+    if (r < rb) load(r + 1);
+    __syncwarp();
+    const int iy = rmap[r].x;
+    if (iy >= y_lo - 1 && iy < y_hi && iy >= -1) {
+      const float ty = __int_as_float(rmap[r].y), uy = 1.f - ty;
+      float fs[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int m = 0; m < MW; ++m) {
+        const int xl = lane + 32 * m;
+        if (xl >= HALF) continue;
+        const int x = xa + xl;
+        float T = 0.f, Td = 0.f, Tr = 0.f;
+        if (regs) {
+#pragma unroll
+          for (int k = 0; k < TCR; ++k) {
+            const int o = toff[m][k];
+            const int i = o & 0x7fffffff;
+            const float g = fvr_checked(i, ncw + 1, kSiteWarpFused) ? mybuf[i] : 0.f;
+            T = fmaf(tw[m][k], g, T);
+            Td += __int_as_float(__float_as_int(g) ^ (o & static_cast<int>(0x80000000u)));
+            Tr = fmaf(trx[m][k], g, Tr);
+          }
+        } else {
+          for (int c = clo[x + 1]; c <= chi[x + 1]; ++c) {  // ix == x: weight 1 - tx, slope -1
+            const int2 e = cmap[c];
+            if (e.x != x || !fvr_checked(c - ca, ncw, kSiteWarpFused)) continue;
+            const float g = mybuf[c - ca];
+            T = fmaf(g, 1.f - __int_as_float(e.y), T);
+            Td -= g;
+            Tr = fmaf(-g, __ldg(w.rxc + c), Tr);
+          }
+          for (int c = clo[x]; c <= chi[x]; ++c) {  // ix == x - 1: weight tx, slope +1
+            const int2 e = cmap[c];
+            if (e.x != x - 1 || !fvr_checked(c - ca, ncw, kSiteWarpFused)) continue;
+            const float g = mybuf[c - ca];
+            T = fmaf(g, __int_as_float(e.y), T);
+            Td += g;
+            Tr = fmaf(g, __ldg(w.rxc + c), Tr);
+          }
+        }
+        const float iu = iy >= 0 ? img[iy * P + x] : 0.f, il = iy + 1 < P ? img[(iy + 1) * P + x] : 0.f;
+        const float it = uy * iu + ty * il, di = il - iu;
+        fs[0] = fmaf(Td, it, fs[0]);
+        fs[1] = fmaf(Tr, it, fs[1]);
+        fs[2] = fmaf(T, di, fs[2]);
+        if (iy >= y_lo) gimg[iy * P + x] += uy * T;
+        if (iy + 1 < y_hi) gimg[(iy + 1) * P + x] += ty * T;
+      }
+      if (max(iy, 0) >= y_lo) {
+        const double ryv = static_cast<double>(__ldg(w.ryr + r));
+        sums[0] += static_cast<double>(fs[0]);
+        sums[1] += static_cast<double>(fs[1]);
+        sums[2] += static_cast<double>(fs[2]);
+        sums[3] += ryv * static_cast<double>(fs[2]);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // Adjoint of pou_slice_ifft_kernel for one (pose, block): G = fftshift(fft2(
 // ifftshift(g))) / P^2, then per slice sample the products of G with the
 // spectrum's spatial derivatives, weighted by fx and fy:
@@ -625,9 +871,15 @@ __device__ __forceinline__ void pou_adjoint_queue(const Stencil& st, const AxisT
 // samples of positive row frequency (plus the Nyquist column), counts those
 // with a mirror twice, and queues the partners of the others; the Nyquist row
 // has no partner and goes through the queue once.
-template <int DT, int M>
+//
+// FUSED: dL/dimgs is not read from memory but formed in shared memory from
+// the detector gradient (pou_warp_gather_adjoint), which also gives this
+// (pose, block)'s pose-offset gradients; the warp adjoint kernel and the
+// block-image gradient buffer drop out.
+template <int DT, int M, bool FUSED>
 __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kernel(PouSliceArgs a,
                                                                                   const float* __restrict__ gimg,
+                                                                                  PouWarpSep wsep,
                                                                                   double* __restrict__ partial) {
   constexpr int P = 32 * M, PITCH = P + 1, H = P / 2, GP = H + 1, NW = kPouImgThreads / 32, GROUP = 4;
   constexpr int BATCH = 32 * GROUP, NQ = P / NW;
@@ -637,6 +889,7 @@ __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kerne
   Cx<float>* gb = zr + H * PITCH;
   const AxisTables tab = axis_tables(smem + pou_adjoint_tables_at(P), 2 * P);
   const int n = blockIdx.x, b = blockIdx.y;
+  const int64_t nblk = gridDim.y;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned short* queue =
       reinterpret_cast<unsigned short*>(smem + pou_adjoint_tables_at(P) + 80 * P) + wid * kPouQueue;
@@ -644,7 +897,28 @@ __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kerne
   pou_image_tables(tab, a, a.geo + n * kGeo);
   WarpFft<M, false> fft;
   fft.init(lane);
-  const float* g = gimg + (static_cast<int64_t>(b) * a.N + n) * P * P;
+  const float* g = FUSED ? reinterpret_cast<const float*>(gb)
+                         : gimg + (static_cast<int64_t>(b) * a.N + n) * P * P;
+  if constexpr (FUSED) {
+    double sums[4] = {0.0, 0.0, 0.0, 0.0};
+    pou_warp_gather_adjoint<M>(wsep, n, b, a.N, smem + (pou_adjoint_smem(P) + 15) / 16 * 16,
+                               reinterpret_cast<float*>(zr), reinterpret_cast<float*>(gb), sums);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double v = warp_sum(sums[k]);
+      if (lane == 0) red[k * NW + wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int k = 0; k < 4; ++k)
+        for (int v = 0; v < NW; ++v) t[k] += red[k * NW + v];
+      const int64_t B = nblk, e = static_cast<int64_t>(b) * a.N + n;
+      wsep.goffs[e] = wsep.inv_ds * (t[1] + t[3]);
+      wsep.goffs[B * a.N + e] = -wsep.inv_ds * t[0];
+      wsep.goffs[2 * B * a.N + e] = -wsep.inv_ds * t[2];
+    }
+  }
   // rows: transform input rows 2s, 2s + 1 (image rows y0, y0 + 1 after ifftshift) together
   for (int s = wid; s < H; s += NW) {
     const int y0 = 2 * s + H < P ? 2 * s + H : 2 * s - H;
@@ -653,7 +927,10 @@ __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kerne
     for (int m = 0; m < M; ++m) {
       const int c = lane + 32 * m;
       const int xc = c + H < P ? c + H : c - H;
-      z[m] = Cx<float>{__ldg(g + y0 * P + xc), __ldg(g + (y0 + 1) * P + xc)};
+      if constexpr (FUSED)
+        z[m] = Cx<float>{g[y0 * P + xc], g[(y0 + 1) * P + xc]};
+      else
+        z[m] = Cx<float>{__ldg(g + y0 * P + xc), __ldg(g + (y0 + 1) * P + xc)};
     }
     fft.run(z, lane);
 #pragma unroll
@@ -750,7 +1027,7 @@ __global__ void __launch_bounds__(kPouImgThreads, 1) pou_fft_slice_adjoint_kerne
   if (threadIdx.x < 6) {
     double sum = 0.0;
     for (int w = 0; w < NW; ++w) sum += red[threadIdx.x * NW + w];
-    partial[(static_cast<int64_t>(n) * gridDim.y + b) * 6 + threadIdx.x] = sum;
+    partial[(static_cast<int64_t>(n) * nblk + b) * 6 + threadIdx.x] = sum;
   }
 }
 
@@ -1407,12 +1684,12 @@ static int pou_image_launch(bool adjoint, const PouSliceArgs& a, int B, const fl
   if (adjoint) {
     static bool attr = false;
     if (!attr) {
-      if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem)) != cudaSuccess)
+      if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
         return FVR_ERR_CUDA;
       attr = true;
     }
-    pou_fft_slice_adjoint_kernel<DT, M><<<grid, kPouImgThreads, smem, s>>>(a, gimg, part);
+    pou_fft_slice_adjoint_kernel<DT, M, false><<<grid, kPouImgThreads, smem, s>>>(a, gimg, PouWarpSep{}, part);
   } else {
     static bool attr = false;
     if (!attr) {
@@ -1435,6 +1712,33 @@ static int pou_image_dispatch(bool adjoint, const PouSliceArgs& a, int B, const 
     case 96: return pou_image_launch<DT, 3>(adjoint, a, B, gimg, imgs, part, s);
     case 128: return pou_image_launch<DT, 4>(adjoint, a, B, gimg, imgs, part, s);
     case 160: return pou_image_launch<DT, 5>(adjoint, a, B, gimg, imgs, part, s);
+  }
+  return FVR_ERR_UNSUPPORTED;
+}
+
+template <int DT, int M>
+static int pou_fused_launch(const PouSliceArgs& a, int B, const PouWarpSep& w, double* part, cudaStream_t s) {
+  const int64_t smem = pou_fused_smem(32 * M, w.Hd, w.W);
+  static int64_t attr = 0;  // largest dynamic shared memory opted in so far
+  if (smem > attr) {
+    if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+      return FVR_ERR_CUDA;
+    attr = smem;
+  }
+  pou_fft_slice_adjoint_kernel<DT, M, true>
+      <<<dim3(static_cast<unsigned>(a.N), static_cast<unsigned>(B)), kPouImgThreads, smem, s>>>(a, nullptr, w, part);
+  FVR_LAUNCH_CHECK();
+  return FVR_OK;
+}
+
+template <int DT>
+static int pou_fused_dispatch(const PouSliceArgs& a, int B, const PouWarpSep& w, double* part, cudaStream_t s) {
+  switch (a.P) {
+    case 64: return pou_fused_launch<DT, 2>(a, B, w, part, s);
+    case 96: return pou_fused_launch<DT, 3>(a, B, w, part, s);
+    case 128: return pou_fused_launch<DT, 4>(a, B, w, part, s);
+    case 160: return pou_fused_launch<DT, 5>(a, B, w, part, s);
   }
   return FVR_ERR_UNSUPPORTED;
 }
@@ -1590,6 +1894,44 @@ int fvr_pou_slice_image_adjoint(int dtype, const void* stencil, const float* sca
   if (ws_bytes < fvr_pou_slice_image_adjoint_workspace(B, N)) return FVR_ERR_WORKSPACE;
   return pou_image_common(true, dtype, stencil, scales, B, P, geo, N, freqs, grad_imgs, nullptr,
                           static_cast<double*>(workspace), stream);
+}
+
+int fvr_pou_warp_image_adjoint_supported(int64_t P, int64_t H, int64_t W) {
+  if (!(P == 64 || P == 96 || P == 128 || P == 160) || H < 1 || W < 4 || W % 4 || W > kPouFusedMaxW || H > 65535)
+    return 0;
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 0;
+  const int64_t static_bytes = 6 * (kPouImgThreads / 32) * static_cast<int64_t>(sizeof(double));
+  return pou_fused_smem(static_cast<int>(P), static_cast<int>(H), static_cast<int>(W)) + static_bytes <= optin ? 1 : 0;
+}
+
+int fvr_pou_warp_image_adjoint(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
+                               const double* geo, int64_t N, const float* freqs, const float* imgs,
+                               const double* offs, const float* rxc, const float* ryr, const float* ic,
+                               const float* gout, int64_t H, int64_t W, double inv_ds, double c_idx, double* goffs,
+                               void* workspace, int64_t ws_bytes, void* stream) {
+  if (!imgs || !offs || !rxc || !ryr || !ic || !gout || !goffs || !workspace || !geo || !freqs) return FVR_ERR_ARG;
+  if ((reinterpret_cast<uintptr_t>(gout) | reinterpret_cast<uintptr_t>(ic) | reinterpret_cast<uintptr_t>(imgs)) & 15)
+    return FVR_ERR_ARG;
+  if (B < 1 || N < 1 || B > 65535 || N > 2147483647) return FVR_ERR_ARG;
+  if (ws_bytes < fvr_pou_slice_image_adjoint_workspace(B, N)) return FVR_ERR_WORKSPACE;
+  if (!fvr_pou_warp_image_adjoint_supported(P, H, W)) return FVR_ERR_UNSUPPORTED;
+  Stencil st;
+  const int rc = pou_stencil(dtype, stencil, scales, P, &st);
+  if (rc) return rc;
+  PouSliceArgs a{st, fvr_stencil_bytes(P, P, P, dtype), fvr_stencil_scale_count(P, P, P), geo, freqs, (int)P, (int)N,
+                 static_cast<double>(P / 2)};
+  const PouWarpSep w{imgs, offs, rxc, ryr, ic, gout, goffs, (int)H, (int)W, inv_ds, c_idx};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* part = static_cast<double*>(workspace);
+  switch (dtype) {
+    case FVR_F32: return pou_fused_dispatch<FVR_F32>(a, (int)B, w, part, s);
+    case FVR_BF16: return pou_fused_dispatch<FVR_BF16>(a, (int)B, w, part, s);
+    case FVR_F16: return pou_fused_dispatch<FVR_F16>(a, (int)B, w, part, s);
+  }
+  return FVR_ERR_DTYPE;
 }
 
 int fvr_pou_warp(const float* imgs, int64_t B, int64_t N, int64_t P, const void* db, const void* cu, const void* cv,

@@ -93,6 +93,9 @@ SIGNATURES = {
     "fvr_pou_slice_image": (I32, [I32, P, P, I64, I64, P, I64, P, P, P]),
     "fvr_pou_slice_image_adjoint_workspace": (I64, [I64, I64]),
     "fvr_pou_slice_image_adjoint": (I32, [I32, P, P, I64, I64, P, I64, P, P, P, I64, P]),
+    "fvr_pou_warp_image_adjoint_supported": (I32, [I64, I64, I64]),
+    "fvr_pou_warp_image_adjoint": (I32, [I32, P, P, I64, I64, P, I64, P, P, P, P, P, P, P, I64, I64, F64, F64, P, P,
+                                         I64, P]),
     "fvr_pou_warp": (I32, [P, I64, I64, I64, P, P, P, I32, I64, P, P, P, I64, I64, F64, F64, P, P]),
     "fvr_pou_warp_bwd_workspace": (I64, [I64, I64, I64]),
     "fvr_pou_warp_bwd": (I32, [P, I64, I64, I64, P, P, P, I32, I64, P, P, P, I64, I64, F64, F64, P, P, P, P, P, I64,

@@ -151,12 +151,37 @@ def edge_dominant_ncc(pred, target, border_crop=None, multiscale_weight=0.25, re
 _LATTICE_CACHE: Dict[Tuple, Tuple] = {}
 
 
+# A lattice is taken as separable (one ray coordinate per detector column and
+# one per row) when its per-column rx and per-row ry spreads are within this
+# fraction of the largest |rx| / |ry|: float rounding of rays that agree
+# exactly, so a pixel's sampling position moves by about the rounding of the
+# position arithmetic itself.
+_SEPARABLE_REL = 2.0 ** -20
+
+
+def _separable_rays(rx, ry):
+    """(rxc [W], ryr [H]) midpoints of the per-column rx and per-row ry ranges
+    of a lattice, or None when the rays do not separate (see _SEPARABLE_REL)."""
+    if rx.ndim != 2 or rx.shape != ry.shape:
+        return None
+    cmax, cmin = rx.amax(0), rx.amin(0)
+    rmax, rmin = ry.amax(1), ry.amin(1)
+    sx = float((cmax - cmin).max()) / max(float(rx.abs().max()), 1e-30)
+    sy = float((rmax - rmin).max()) / max(float(ry.abs().max()), 1e-30)
+    if not (sx <= _SEPARABLE_REL and sy <= _SEPARABLE_REL):
+        return None
+    rxc = (0.5 * (cmax.double() + cmin.double())).float().contiguous()
+    ryr = (0.5 * (rmax.double() + rmin.double())).float().contiguous()
+    return rxc, ryr
+
+
 def _prepared_lattice(lattice, device):
     """Device copies of an 11-tuple lattice's ray tables and its basis
-    (src0, u0, v0, n0) as 12 host doubles, cached per (storage, device): the
-    lattice is a per-geometry constant, moved once.  The entry holds the
-    lattice's own tensors, so their storage cannot be freed and reused by
-    another lattice while the entry exists."""
+    (src0, u0, v0, n0) as 12 host doubles, and its separable ray tables when
+    it has them, cached per (storage, device): the lattice is a per-geometry
+    constant, moved once.  The entry holds the lattice's own tensors, so their
+    storage cannot be freed and reused by another lattice while the entry
+    exists."""
     key = tuple(int(t.data_ptr()) for t in lattice[:8]) + (str(device),)
     hit = _LATTICE_CACHE.get(key)
     if hit is None:
@@ -165,7 +190,7 @@ def _prepared_lattice(lattice, device):
         basis = torch.cat([lattice[i].reshape(3) for i in (0, 2, 3, 4)]).detach().double().cpu()
         base = (_ct.c_double * 12)(*[float(x) for x in basis])
         rays = tuple(t.detach().to(device=device, dtype=torch.float32).contiguous() for t in lattice[5:8])
-        hit = (key, base, rays, tuple(lattice[:8]))
+        hit = (key, base, rays, tuple(lattice[:8]), _separable_rays(rays[0], rays[1]))
         _LATTICE_CACHE[key] = hit
     return hit
 
@@ -237,29 +262,41 @@ class _PinholeFn(torch.autograd.Function):
                    _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), H * W, 0,
                    1.0 / model.ds_block, float(P // 2), L.ptr(out), s)
         ctx.save_for_backward(geo, offs, imgs, rx, ry, ic)
-        ctx.meta = (model, base, mats.dtype)
+        ctx.meta = (model, base, mats.dtype, _LATTICE_CACHE[base_key][4])
         return out
 
     @staticmethod
     def backward(ctx, g_out):
         geo, offs, imgs, rx, ry, ic = ctx.saved_tensors
-        model, base, mdt = ctx.meta
+        model, base, mdt, sep = ctx.meta
         dev = geo.device
         B, N, P = model.B, int(geo.shape[0]), model.P
         H, W = int(rx.shape[0]), int(rx.shape[1])
         s = L.stream_ptr(dev)
         g = g_out.detach().to(device=dev, dtype=torch.float32).contiguous()
-        grad_imgs = torch.zeros((B, N, P, P), dtype=torch.float32, device=dev)
         goffs = torch.empty((3, B, N), dtype=torch.float64, device=dev)
-        wsb = L.query("fvr_pou_warp_bwd_workspace", B, N, H * W)
-        ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
-        with profiling.section("pou_warp_bwd"):
-            L.call("fvr_pou_warp_bwd", L.ptr(imgs), B, N, P, L.ptr(offs), _ct.c_void_p(offs.data_ptr() + 8),
-                   _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), H * W, 0,
-                   1.0 / model.ds_block, float(P // 2), L.ptr(g), L.ptr(grad_imgs), L.ptr(goffs), None, L.ptr(ws),
-                   wsb, s)
-        ws2, tiles = _block_images_adjoint(model, geo, N, grad_imgs, s)
-        del grad_imgs
+        if (sep is not None and model.fused_warp_adjoint and g.data_ptr() % 16 == 0 and ic.data_ptr() % 16 == 0
+                and L.query("fvr_pou_warp_image_adjoint_supported", P, H, W)):
+            # warp adjoint + block-image adjoint in one launch: dL/dimgs stays in shared memory
+            st = model._stencil
+            wsb = L.query("fvr_pou_slice_image_adjoint_workspace", B, N)
+            ws2 = torch.empty(wsb, dtype=torch.uint8, device=dev)
+            with profiling.section("pou_slice_adjoint"):
+                L.call("fvr_pou_warp_image_adjoint", st.code, L.ptr(st.data), L.ptr(st.scales), B, P, L.ptr(geo), N,
+                       L.ptr(model._freqs), L.ptr(imgs), L.ptr(offs), L.ptr(sep[0]), L.ptr(sep[1]), L.ptr(ic), L.ptr(g),
+                       H, W, 1.0 / model.ds_block, float(P // 2), L.ptr(goffs), L.ptr(ws2), wsb, s)
+            tiles = 1
+        else:
+            grad_imgs = torch.zeros((B, N, P, P), dtype=torch.float32, device=dev)
+            wsb = L.query("fvr_pou_warp_bwd_workspace", B, N, H * W)
+            ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+            with profiling.section("pou_warp_bwd"):
+                L.call("fvr_pou_warp_bwd", L.ptr(imgs), B, N, P, L.ptr(offs), _ct.c_void_p(offs.data_ptr() + 8),
+                       _ct.c_void_p(offs.data_ptr() + 16), 1, 3, L.ptr(rx), L.ptr(ry), L.ptr(ic), H * W, 0,
+                       1.0 / model.ds_block, float(P // 2), L.ptr(g), L.ptr(grad_imgs), L.ptr(goffs), None,
+                       L.ptr(ws), wsb, s)
+            ws2, tiles = _block_images_adjoint(model, geo, N, grad_imgs, s)
+            del grad_imgs
         gm = torch.empty((N, 4, 4), dtype=torch.float32, device=dev)
         L.call("fvr_pou_pose_backward", L.ptr(ws2), tiles, L.ptr(goffs), None, 0, L.ptr(geo), L.ptr(model.centers), B,
                N, base, float(P) * model.ds_block, L.ptr(gm), None, s)
@@ -291,6 +328,8 @@ class PerspectiveSlabFVR(nn.Module):
                  dtype=torch.float32, use_triton=True, device=None):
         super().__init__()
         self.use_triton = bool(use_triton)
+        # pinhole adjoint: warp + block-image adjoint in one launch on separable lattices
+        self.fused_warp_adjoint = True
         self._compiled_project_core = None
         self._compiled_project_invariant = None
         vol = torch.as_tensor(vol_3d).detach().float()
@@ -481,7 +520,7 @@ class PerspectiveSlabFVR(nn.Module):
             H, W = int(lattice[1].shape[0]), int(lattice[1].shape[1])
             return torch.zeros((0, 1, H, W), dtype=torch.float32, device=home) + 0.0 * pose_mats.sum()
         if len(lattice) >= 11:
-            key, _, (rx, ry, ic), _ = _prepared_lattice(lattice, self._dev)
+            key, _, (rx, ry, ic), _, _ = _prepared_lattice(lattice, self._dev)
             mats = pose_mats if home == self._dev else pose_mats.to(self._dev)
             out = _PinholeFn.apply(mats, self, rx, ry, ic, key)
         else:

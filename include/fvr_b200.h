@@ -320,6 +320,24 @@ int64_t fvr_pou_slice_image_adjoint_workspace(int64_t B, int64_t N);
 int fvr_pou_slice_image_adjoint(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
                                 const double* geo, int64_t N, const float* freqs, const float* grad_imgs,
                                 void* workspace, int64_t ws_bytes, void* stream);
+/* Fused warp + block-image adjoint for a separable pinhole lattice (every
+ * detector column shares one ray coordinate rxc[c], every row one ryr[r]):
+ * from the detector gradient gout[N][H][W] (times ic[H][W]) and the forward
+ * block images imgs[B][N][P][P], one CTA per (pose, block) forms dL/dimgs in
+ * shared memory by a gather along detector rows (no atomics, no image-gradient
+ * buffer), writes goffs[3][B][N] = dL/d(d_b, cu, cv) (offs[B][N][3] fp64) and
+ * the slice partials workspace[N][B][6] that fvr_pou_pose_backward takes with
+ * tiles = 1, i.e. fvr_pou_warp_bwd + fvr_pou_slice_image_adjoint in one
+ * launch.  Supported (fvr_pou_warp_image_adjoint_supported) for P in
+ * {64, 96, 128, 160}, W a multiple of 4 up to 256 and the shared memory that
+ * takes; gout, ic and imgs start on 16-byte boundaries.  Autograd of
+ * src/fvr/triton_slice.py:409-496 with cone_beam_fvr.py:480-505. */
+int fvr_pou_warp_image_adjoint_supported(int64_t P, int64_t H, int64_t W);
+int fvr_pou_warp_image_adjoint(int dtype, const void* stencil, const float* scales, int64_t B, int64_t P,
+                               const double* geo, int64_t N, const float* freqs, const float* imgs,
+                               const double* offs, const float* rxc, const float* ryr, const float* ic,
+                               const float* gout, int64_t H, int64_t W, double inv_ds, double c_idx, double* goffs,
+                               void* workspace, int64_t ws_bytes, void* stream);
 /* out[N][K] = ic[q] * sum_b bilinear(imgs[b][n], (d_b rx - cu)/ds + c, (d_b ry - cv)/ds + c),
  * zero padding; offsets float (offs_f64 = 0) or double, element (b, n) at
  * index (b*N + n) * ostride; ray tables shared (ray_stride 0) or per pose

@@ -292,6 +292,43 @@ def test_presets_and_parity_offsets():
     assert torch.allclose(offs.abs().max(dim=0).values, torch.tensor([0.5, 1.0, 2.0]))
 
 
+@pytest.mark.parametrize("block_res,det,dtype", [(32, 64, torch.float32), (48, 96, torch.bfloat16),
+                                                 (64, 256, torch.float32), (64, 128, torch.float16),
+                                                 (32, 256, torch.float32)])
+def test_fused_warp_adjoint_matches_two_kernel_path(block_res, det, dtype):
+    """On a separable pinhole lattice the backward takes the fused warp +
+    block-image adjoint (fvr_pou_warp_image_adjoint: dL/dimgs formed in shared
+    memory by a gather along detector rows); its pose gradient equals the
+    two-kernel path's (fvr_pou_warp_bwd scatter + fvr_pou_slice_image_adjoint).
+    The last case puts about five detector columns on each image column, more
+    taps than the kernel keeps in registers, so its column-loop path runs."""
+    import fvr._lib as L
+    from fvr import synthetic
+    from fvr.cone_beam_fvr import PerspectiveSlabFVR, _prepared_lattice
+
+    vol = synthetic.make_ellipsoid_volume(96, 0)
+    m = PerspectiveSlabFVR.from_volume(vol, vox_mm=2.0, grid_blocks=(3, 3, 3), block_res=block_res, overlap=0.5,
+                                       dtype=dtype)
+    f = 1020.0 / (3.2 * 64 / det)
+    k_inv = np.array([[1 / f, 0, -0.5 * det / f], [0, 1 / f, -0.5 * det / f], [0, 0, 1.0]])
+    lat = m.make_pinhole_lattice(_t(k_inv), 1020.0, det, det)
+    assert _prepared_lattice(lat, m._dev)[4] is not None
+    assert L.query("fvr_pou_warp_image_adjoint_supported", m.P, det, det) == 1
+    mats = synthetic.make_pinhole_mats(4, 3, sad_mm=765.0)
+    grads, outs = [], []
+    for fused in (True, False):
+        m.fused_warp_adjoint = fused
+        mm = mats.to(DEV).requires_grad_(True)
+        out = m.forward_pinhole(mm, lat)
+        w = torch.from_numpy(np.random.default_rng(5).standard_normal(out.shape).astype(np.float32)).to(DEV)
+        (out * w).sum().backward()
+        grads.append(mm.grad.cpu().numpy())
+        outs.append(out.detach().cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    assert np.abs(grads[1]).max() > 0
+    assert rel_l2(grads[0], grads[1]) < 1e-5
+
+
 def test_full_geometry_subset_vs_oracle():
     """4x4x4 blocks, 50 % overlap, block_res 32 on a seeded 96^3 volume, 256x... pinhole
     at SDD 1020 / SAD 765: forward and mats gradient against the float64 oracle."""
