@@ -635,82 +635,30 @@ struct PouWarpSep {
 // Shared memory of the fused adjoint beyond the block-image adjoint's: one
 // detector-row buffer per warp [16][W + 4], column map (ix, tx) [W], row map
 // (iy, ty) [Hd], per image index -1 .. P-1 the first and last detector column
-// and row with that index [4][P + 1].
+// and row with that index [4][P + 1], the largest tap count [4].
 constexpr int kPouFusedMaxW = 256;
 
 __host__ __device__ constexpr int64_t pou_fused_extra(int P, int Hd, int W) {
-  return 4LL * (kPouImgThreads / 32) * (W + 4) + 8LL * W + 8LL * Hd + 16LL * (P + 1);
+  return 4LL * (kPouImgThreads / 32) * (W + 4) + 8LL * W + 8LL * Hd + 16LL * (P + 1) + 16;
 }
 
 __host__ __device__ constexpr int64_t pou_fused_smem(int P, int Hd, int W) {
   return (pou_adjoint_smem(P) + 15) / 16 * 16 + pou_fused_extra(P, Hd, W);
 }
 
-// dL/dimgs of block b at pose n into `gimg` [P][P] (shared memory, zeroed
-// here) and the pose-offset sums (sum g dv/dpx, sum g rx dv/dpx, sum g dv/dpy,
-// sum g ry dv/dpy) of this (pose, block), with the forward image staged in
-// `img` [P][P].  The x gather of a detector row is T[x] = sum of the row's
-// values over image column x's taps (every row has the same taps).  Warp w
-// owns image rows [(w/2) P/8, (w/2 + 1) P/8) at the columns of half w % 2 of
-// the image, whose taps its lanes hold in registers: it runs over the
-// detector rows whose iy lies in [(w/2) P/8 - 1, (w/2 + 1) P/8 - 1] and adds
-// only into its own rows and columns, so no two warps write one element; a
-// detector row's sums are counted by the warps owning image row max(iy, 0),
-// each over its own columns.
-template <int M>
-__device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N, unsigned char* sep, float* img,
-                                        float* gimg, double (&sums)[4]) {
-  constexpr int P = 32 * M, NW = kPouImgThreads / 32;
+// Detector-row pass of the fused adjoint for one layout: warp = (row band,
+// column part); the image rows that receive contributions, [Y0, Y1], split in
+// 16 / NCP equal bands, and the image columns [h P/NCP, (h + 1) P/NCP); each
+// lane keeps up to TCR taps of each of its columns in registers (columns with
+// more taps, or detector columns out of order, take column loops instead).
+template <int M, int NCP, int TCR>
+__device__ void pou_gather_rows(const PouWarpSep& w, int n, float* wbuf, const int2* cmap, const int2* rmap,
+                                const int* clo, const int* chi, const int* rlo, const int* rhi, const float* img,
+                                float* gimg, double (&sums)[4]) {
+  constexpr int P = 32 * M, PART = P / NCP, MW = (PART + 31) / 32, RG = kPouImgThreads / 32 / NCP;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int W = w.W, Hd = w.Hd;
-  float* wbuf = reinterpret_cast<float*>(sep);
-  int2* cmap = reinterpret_cast<int2*>(wbuf + NW * (W + 4));
-  int2* rmap = cmap + W;
-  int* clo = reinterpret_cast<int*>(rmap + Hd);
-  int* chi = clo + (P + 1);
-  int* rlo = chi + (P + 1);
-  int* rhi = rlo + (P + 1);
-  const double* o = w.offs + 3 * (static_cast<int64_t>(b) * N + n);
-  const double db = o[0], cu = o[1], cv = o[2];
-  for (int k = threadIdx.x; k < 4 * (P + 1); k += kPouImgThreads) clo[k] = ((k / (P + 1)) & 1) ? -1 : 0x7fffffff;
-  for (int c = threadIdx.x; c < W; c += kPouImgThreads) {
-    const double px = (db * static_cast<double>(__ldg(w.rxc + c)) - cu) * w.inv_ds + w.c_idx;
-    const bool ok = px > -1.0 && px < static_cast<double>(P);
-    const double f = floor(px);
-    cmap[c] = make_int2(ok ? static_cast<int>(f) : -2, __float_as_int(static_cast<float>(px - f)));
-  }
-  for (int r = threadIdx.x; r < Hd; r += kPouImgThreads) {
-    const double py = (db * static_cast<double>(__ldg(w.ryr + r)) - cv) * w.inv_ds + w.c_idx;
-    const bool ok = py > -1.0 && py < static_cast<double>(P);
-    const double f = floor(py);
-    rmap[r] = make_int2(ok ? static_cast<int>(f) : -2, __float_as_int(static_cast<float>(py - f)));
-  }
-  const float4* src = reinterpret_cast<const float4*>(w.imgs + (static_cast<int64_t>(b) * N + n) * P * P);
-  for (int q = threadIdx.x; q < P * P / 4; q += kPouImgThreads) {
-    reinterpret_cast<float4*>(img)[q] = __ldg(src + q);
-    reinterpret_cast<float4*>(gimg)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  __syncthreads();
-  for (int c = threadIdx.x; c < W; c += kPouImgThreads) {
-    const int ix = cmap[c].x;
-    if (ix >= -1) {
-      atomicMin(clo + ix + 1, c);
-      atomicMax(chi + ix + 1, c);
-    }
-  }
-  for (int r = threadIdx.x; r < Hd; r += kPouImgThreads) {
-    const int iy = rmap[r].x;
-    if (iy >= -1) {
-      atomicMin(rlo + iy + 1, r);
-      atomicMax(rhi + iy + 1, r);
-    }
-  }
-  __syncthreads();
-  // warp = (row group, column half): the image rows that receive
-  // contributions, [Y0, Y1], split in 8 equal bands, and the image columns
-  // [h P/2, (h + 1) P/2); each lane keeps its columns' taps in registers
-  constexpr int HALF = P / 2, MW = (HALF + 31) / 32, TCR = 6;
-  const int rg = wid >> 1, h = wid & 1, xa = h * HALF;
+  const int rg = wid / NCP, h = wid % NCP, xa = h * PART;
   int ylo = 0x7fffffff, yhi = -1;  // valid iy + 1 range
   for (int k = lane; k <= P; k += 32)
     if (rlo[k] <= rhi[k]) {
@@ -721,15 +669,15 @@ __device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N
   yhi = __reduce_max_sync(0xffffffffu, yhi);
   if (ylo > yhi) return;
   const int Y0 = max(ylo - 1, 0), Y1 = min(yhi, P - 1);  // rows iy and iy + 1 of the valid detector rows
-  const int y_lo = Y0 + (rg * (Y1 - Y0 + 1)) / 8, y_hi = Y0 + ((rg + 1) * (Y1 - Y0 + 1)) / 8;
+  const int y_lo = Y0 + (rg * (Y1 - Y0 + 1)) / RG, y_hi = Y0 + ((rg + 1) * (Y1 - Y0 + 1)) / RG;
   if (y_lo >= y_hi) return;
   int ra = 0x7fffffff, rb = -1;  // detector rows with iy + 1 in [y_lo, y_hi]
   for (int k = y_lo + lane; k <= y_hi; k += 32) {
     ra = min(ra, rlo[k]);
     rb = max(rb, rhi[k]);
   }
-  int ca = 0x7fffffff, cb = -1;  // detector columns with ix + 1 in [xa, xa + HALF]
-  for (int k = xa + lane; k <= xa + HALF; k += 32) {
+  int ca = 0x7fffffff, cb = -1;  // detector columns with ix + 1 in [xa, xa + PART]
+  for (int k = xa + lane; k <= xa + PART; k += 32) {
     ca = min(ca, clo[k]);
     cb = max(cb, chi[k]);
   }
@@ -755,7 +703,7 @@ __device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N
       trx[m][k] = 0.f;
     }
     const int x = xa + lane + 32 * m;
-    if (lane + 32 * m >= HALF) continue;
+    if (lane + 32 * m >= PART) continue;
     // the columns of one index form the range [clo, chi] when px is monotone
     // in the column (checked per tap; otherwise the column loops below)
     const int a0 = clo[x + 1], a1 = clo[x];
@@ -806,7 +754,7 @@ __device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N
 #pragma unroll
       for (int m = 0; m < MW; ++m) {
         const int xl = lane + 32 * m;
-        if (xl >= HALF) continue;
+        if (xl >= PART) continue;
         const int x = xa + xl;
         float T = 0.f, Td = 0.f, Tr = 0.f;
         if (regs) {
@@ -855,6 +803,78 @@ __device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N
     }
     __syncwarp();
   }
+}
+
+// dL/dimgs of block b at pose n into `gimg` [P][P] (shared memory, zeroed
+// here) and the pose-offset sums (sum g dv/dpx, sum g rx dv/dpx, sum g dv/dpy,
+// sum g ry dv/dpy) of this (pose, block), with the forward image staged in
+// `img` [P][P].  The x gather of a detector row is T[x] = sum of the row's
+// values over image column x's taps (every row has the same taps).  Each warp
+// owns a band of image rows at a part of the image columns, whose taps its
+// lanes hold in registers: it runs over the detector rows whose iy lies in
+// [band start - 1, band end - 1] and adds only into its own rows and columns,
+// so no two warps write one element; a detector row's sums are counted by the
+// warps owning image row max(iy, 0), each over its own columns.  Two column
+// parts of up to 6 taps per column, or (larger detector-to-image
+// magnification) four parts of up to 12.
+template <int M>
+__device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N, unsigned char* sep, float* img,
+                                        float* gimg, double (&sums)[4]) {
+  constexpr int P = 32 * M, NW = kPouImgThreads / 32;
+  const int W = w.W, Hd = w.Hd;
+  float* wbuf = reinterpret_cast<float*>(sep);
+  int2* cmap = reinterpret_cast<int2*>(wbuf + NW * (W + 4));
+  int2* rmap = cmap + W;
+  int* clo = reinterpret_cast<int*>(rmap + Hd);
+  int* chi = clo + (P + 1);
+  int* rlo = chi + (P + 1);
+  int* rhi = rlo + (P + 1);
+  int* tmax = rhi + (P + 1);
+  const double* o = w.offs + 3 * (static_cast<int64_t>(b) * N + n);
+  const double db = o[0], cu = o[1], cv = o[2];
+  for (int k = threadIdx.x; k < 4 * (P + 1); k += kPouImgThreads) clo[k] = ((k / (P + 1)) & 1) ? -1 : 0x7fffffff;
+  if (threadIdx.x == 0) *tmax = 0;
+  for (int c = threadIdx.x; c < W; c += kPouImgThreads) {
+    const double px = (db * static_cast<double>(__ldg(w.rxc + c)) - cu) * w.inv_ds + w.c_idx;
+    const bool ok = px > -1.0 && px < static_cast<double>(P);
+    const double f = floor(px);
+    cmap[c] = make_int2(ok ? static_cast<int>(f) : -2, __float_as_int(static_cast<float>(px - f)));
+  }
+  for (int r = threadIdx.x; r < Hd; r += kPouImgThreads) {
+    const double py = (db * static_cast<double>(__ldg(w.ryr + r)) - cv) * w.inv_ds + w.c_idx;
+    const bool ok = py > -1.0 && py < static_cast<double>(P);
+    const double f = floor(py);
+    rmap[r] = make_int2(ok ? static_cast<int>(f) : -2, __float_as_int(static_cast<float>(py - f)));
+  }
+  const float4* src = reinterpret_cast<const float4*>(w.imgs + (static_cast<int64_t>(b) * N + n) * P * P);
+  for (int q = threadIdx.x; q < P * P / 4; q += kPouImgThreads) {
+    reinterpret_cast<float4*>(img)[q] = __ldg(src + q);
+    reinterpret_cast<float4*>(gimg)[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < W; c += kPouImgThreads) {
+    const int ix = cmap[c].x;
+    if (ix >= -1) {
+      atomicMin(clo + ix + 1, c);
+      atomicMax(chi + ix + 1, c);
+    }
+  }
+  for (int r = threadIdx.x; r < Hd; r += kPouImgThreads) {
+    const int iy = rmap[r].x;
+    if (iy >= -1) {
+      atomicMin(rlo + iy + 1, r);
+      atomicMax(rhi + iy + 1, r);
+    }
+  }
+  __syncthreads();
+  // largest tap count of an image column picks the register layout
+  for (int x = threadIdx.x; x < P; x += kPouImgThreads)
+    atomicMax(tmax, max(chi[x + 1] - clo[x + 1] + 1, 0) + max(chi[x] - clo[x] + 1, 0));
+  __syncthreads();
+  if (*tmax <= 6)
+    pou_gather_rows<M, 2, 6>(w, n, wbuf, cmap, rmap, clo, chi, rlo, rhi, img, gimg, sums);
+  else
+    pou_gather_rows<M, 4, 12>(w, n, wbuf, cmap, rmap, clo, chi, rlo, rhi, img, gimg, sums);
 }
 
 // Adjoint of pou_slice_ifft_kernel for one (pose, block): G = fftshift(fft2(
@@ -1738,7 +1758,6 @@ static int pou_fused_dispatch(const PouSliceArgs& a, int B, const PouWarpSep& w,
     case 64: return pou_fused_launch<DT, 2>(a, B, w, part, s);
     case 96: return pou_fused_launch<DT, 3>(a, B, w, part, s);
     case 128: return pou_fused_launch<DT, 4>(a, B, w, part, s);
-    case 160: return pou_fused_launch<DT, 5>(a, B, w, part, s);
   }
   return FVR_ERR_UNSUPPORTED;
 }
@@ -1897,8 +1916,7 @@ int fvr_pou_slice_image_adjoint(int dtype, const void* stencil, const float* sca
 }
 
 int fvr_pou_warp_image_adjoint_supported(int64_t P, int64_t H, int64_t W) {
-  if (!(P == 64 || P == 96 || P == 128 || P == 160) || H < 1 || W < 4 || W % 4 || W > kPouFusedMaxW || H > 65535)
-    return 0;
+  if (!(P == 64 || P == 96 || P == 128) || H < 1 || W < 4 || W % 4 || W > kPouFusedMaxW || H > 65535) return 0;
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)

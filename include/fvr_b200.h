@@ -329,7 +329,7 @@ int fvr_pou_slice_image_adjoint(int dtype, const void* stencil, const float* sca
  * the slice partials workspace[N][B][6] that fvr_pou_pose_backward takes with
  * tiles = 1, i.e. fvr_pou_warp_bwd + fvr_pou_slice_image_adjoint in one
  * launch.  Supported (fvr_pou_warp_image_adjoint_supported) for P in
- * {64, 96, 128, 160}, W a multiple of 4 up to 256 and the shared memory that
+ * {64, 96, 128}, W a multiple of 4 up to 256 and the shared memory that
  * takes; gout, ic and imgs start on 16-byte boundaries.  Autograd of
  * src/fvr/triton_slice.py:409-496 with cone_beam_fvr.py:480-505. */
 int fvr_pou_warp_image_adjoint_supported(int64_t P, int64_t H, int64_t W);

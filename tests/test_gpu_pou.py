@@ -292,22 +292,23 @@ def test_presets_and_parity_offsets():
     assert torch.allclose(offs.abs().max(dim=0).values, torch.tensor([0.5, 1.0, 2.0]))
 
 
-@pytest.mark.parametrize("block_res,det,dtype", [(32, 64, torch.float32), (48, 96, torch.bfloat16),
-                                                 (64, 256, torch.float32), (64, 128, torch.float16),
-                                                 (32, 256, torch.float32)])
-def test_fused_warp_adjoint_matches_two_kernel_path(block_res, det, dtype):
+@pytest.mark.parametrize("block_res,det,dtype,grid", [(32, 64, torch.float32, 3), (48, 96, torch.bfloat16, 3),
+                                                      (64, 256, torch.float32, 3), (64, 128, torch.float16, 3),
+                                                      (32, 256, torch.float32, 3), (32, 256, torch.float32, 2)])
+def test_fused_warp_adjoint_matches_two_kernel_path(block_res, det, dtype, grid):
     """On a separable pinhole lattice the backward takes the fused warp +
     block-image adjoint (fvr_pou_warp_image_adjoint: dL/dimgs formed in shared
     memory by a gather along detector rows); its pose gradient equals the
     two-kernel path's (fvr_pou_warp_bwd scatter + fvr_pou_slice_image_adjoint).
-    The last case puts about five detector columns on each image column, more
-    taps than the kernel keeps in registers, so its column-loop path runs."""
+    The last two cases put about five and seven detector columns on each image
+    column: the kernel's 12-tap register layout, then (more taps than that)
+    its column loops."""
     import fvr._lib as L
     from fvr import synthetic
     from fvr.cone_beam_fvr import PerspectiveSlabFVR, _prepared_lattice
 
     vol = synthetic.make_ellipsoid_volume(96, 0)
-    m = PerspectiveSlabFVR.from_volume(vol, vox_mm=2.0, grid_blocks=(3, 3, 3), block_res=block_res, overlap=0.5,
+    m = PerspectiveSlabFVR.from_volume(vol, vox_mm=2.0, grid_blocks=(grid,) * 3, block_res=block_res, overlap=0.5,
                                        dtype=dtype)
     f = 1020.0 / (3.2 * 64 / det)
     k_inv = np.array([[1 / f, 0, -0.5 * det / f], [0, 1 / f, -0.5 * det / f], [0, 0, 1.0]])
