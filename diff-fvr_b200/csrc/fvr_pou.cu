@@ -649,8 +649,8 @@ __host__ __device__ constexpr int64_t pou_fused_smem(int P, int Hd, int W) {
 // Detector-row pass of the fused adjoint for one layout: warp = (row band,
 // column part); the image rows that receive contributions, [Y0, Y1], split in
 // 16 / NCP equal bands, and the image columns [h P/NCP, (h + 1) P/NCP); each
-// lane keeps up to TCR taps of each of its columns in registers (columns with
-// more taps, or detector columns out of order, take column loops instead).
+// lane keeps up to TCR/2 taps of each class of each of its columns in
+// registers (more, or detector columns out of order, take column loops).
 template <int M, int NCP, int TCR>
 __device__ void pou_gather_rows(const PouWarpSep& w, int n, float* wbuf, const int2* cmap, const int2* rmap,
                                 const int* clo, const int* chi, const int* rlo, const int* rhi, const float* img,
@@ -689,17 +689,19 @@ __device__ void pou_gather_rows(const PouWarpSep& w, int n, float* wbuf, const i
   ca &= ~3;  // float4 staging from a 16-byte boundary (W is a multiple of 4)
   const int nq = (cb - ca + 4) / 4, ncw = 4 * nq;  // staged float4 chunks, columns
   float* mybuf = wbuf + static_cast<int64_t>(wid) * (W + 4);  // the row's columns [ca, ca + ncw), then a zero
-  // taps of image column x: detector columns with ix == x (weight 1 - tx,
-  // slope -1) and ix == x - 1 (weight tx, slope +1); unused slots read the zero
-  int toff[MW][TCR];  // mybuf index, sign bit set for slope -1
-  float tw[MW][TCR], trx[MW][TCR];
+  // taps of image column x: slots [0, TCR/2) hold the detector columns with
+  // ix == x (weight 1 - tx, slope -1), slots [TCR/2, TCR) those with
+  // ix == x - 1 (weight tx, slope +1); unused slots read the zero
+  constexpr int HT = TCR / 2;
+  int toff[MW][TCR];  // mybuf index
+  float tt[MW][TCR], trx[MW][TCR];
   bool over = false;
 #pragma unroll
   for (int m = 0; m < MW; ++m) {
 #pragma unroll
     for (int k = 0; k < TCR; ++k) {
       toff[m][k] = ncw;
-      tw[m][k] = 0.f;
+      tt[m][k] = 0.f;
       trx[m][k] = 0.f;
     }
     const int x = xa + lane + 32 * m;
@@ -708,18 +710,18 @@ __device__ void pou_gather_rows(const PouWarpSep& w, int n, float* wbuf, const i
     // in the column (checked per tap; otherwise the column loops below)
     const int a0 = clo[x + 1], a1 = clo[x];
     const int n0 = max(chi[x + 1] - a0 + 1, 0), n1 = max(chi[x] - a1 + 1, 0);
-    over |= n0 + n1 > TCR;
+    over |= n0 > HT || n1 > HT;
 #pragma unroll
     for (int q = 0; q < TCR; ++q) {
-      if (q >= n0 + n1) continue;
-      const bool cls = q >= n0;  // false: ix == x, true: ix == x - 1
-      const int c = cls ? a1 + q - n0 : a0 + q;
+      const bool cls = q >= HT;  // false: ix == x, true: ix == x - 1
+      const int qq = cls ? q - HT : q;
+      if (qq >= (cls ? n1 : n0)) continue;
+      const int c = (cls ? a1 : a0) + qq;
       const int2 e = cmap[c];
       over |= e.x != (cls ? x - 1 : x);
-      const float t = __int_as_float(e.y), rx = __ldg(w.rxc + c);
-      toff[m][q] = (c - ca) | (cls ? 0 : static_cast<int>(0x80000000u));
-      tw[m][q] = cls ? t : 1.f - t;
-      trx[m][q] = cls ? rx : -rx;
+      toff[m][q] = c - ca;
+      tt[m][q] = __int_as_float(e.y);
+      trx[m][q] = __ldg(w.rxc + c);
     }
   }
   const bool regs = !__any_sync(0xffffffffu, over);  // else the column loops below
@@ -757,16 +759,23 @@ __device__ void pou_gather_rows(const PouWarpSep& w, int n, float* wbuf, const i
         if (xl >= PART) continue;
         const int x = xa + xl;
         float T = 0.f, Td = 0.f, Tr = 0.f;
-        if (regs) {
+        if (regs) {  // per class: sum g, sum tx g, sum rx g
+          float s0 = 0.f, u0 = 0.f, r0 = 0.f, s1 = 0.f, u1 = 0.f, r1 = 0.f;
 #pragma unroll
-          for (int k = 0; k < TCR; ++k) {
-            const int o = toff[m][k];
-            const int i = o & 0x7fffffff;
-            const float g = fvr_checked(i, ncw + 1, kSiteWarpFused) ? mybuf[i] : 0.f;
-            T = fmaf(tw[m][k], g, T);
-            Td += __int_as_float(__float_as_int(g) ^ (o & static_cast<int>(0x80000000u)));
-            Tr = fmaf(trx[m][k], g, Tr);
+          for (int k = 0; k < HT; ++k) {
+            const int i0 = toff[m][k], i1 = toff[m][HT + k];
+            const float g0 = fvr_checked(i0, ncw + 1, kSiteWarpFused) ? mybuf[i0] : 0.f;
+            const float g1 = fvr_checked(i1, ncw + 1, kSiteWarpFused) ? mybuf[i1] : 0.f;
+            s0 += g0;
+            u0 = fmaf(tt[m][k], g0, u0);
+            r0 = fmaf(trx[m][k], g0, r0);
+            s1 += g1;
+            u1 = fmaf(tt[m][HT + k], g1, u1);
+            r1 = fmaf(trx[m][HT + k], g1, r1);
           }
+          T = (s0 - u0) + u1;
+          Td = s1 - s0;
+          Tr = r1 - r0;
         } else {
           for (int c = clo[x + 1]; c <= chi[x + 1]; ++c) {  // ix == x: weight 1 - tx, slope -1
             const int2 e = cmap[c];
@@ -815,8 +824,8 @@ __device__ void pou_gather_rows(const PouWarpSep& w, int n, float* wbuf, const i
 // [band start - 1, band end - 1] and adds only into its own rows and columns,
 // so no two warps write one element; a detector row's sums are counted by the
 // warps owning image row max(iy, 0), each over its own columns.  Two column
-// parts of up to 6 taps per column, or (larger detector-to-image
-// magnification) four parts of up to 12.
+// parts with up to 3 detector columns per image index (6 taps per column),
+// or (larger detector-to-image magnification) four parts with up to 6 (12).
 template <int M>
 __device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N, unsigned char* sep, float* img,
                                         float* gimg, double (&sums)[4]) {
@@ -867,11 +876,10 @@ __device__ void pou_warp_gather_adjoint(const PouWarpSep& w, int n, int b, int N
     }
   }
   __syncthreads();
-  // largest tap count of an image column picks the register layout
-  for (int x = threadIdx.x; x < P; x += kPouImgThreads)
-    atomicMax(tmax, max(chi[x + 1] - clo[x + 1] + 1, 0) + max(chi[x] - clo[x] + 1, 0));
+  // the most detector columns on one image index picks the register layout
+  for (int k = threadIdx.x; k <= P; k += kPouImgThreads) atomicMax(tmax, max(chi[k] - clo[k] + 1, 0));
   __syncthreads();
-  if (*tmax <= 6)
+  if (*tmax <= 3)
     pou_gather_rows<M, 2, 6>(w, n, wbuf, cmap, rmap, clo, chi, rlo, rhi, img, gimg, sums);
   else
     pou_gather_rows<M, 4, 12>(w, n, wbuf, cmap, rmap, clo, chi, rlo, rhi, img, gimg, sums);
