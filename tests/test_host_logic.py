@@ -98,3 +98,28 @@ def test_capture_guard_restores_the_collector():
         assert not gc.isenabled()
     finally:
         (gc.enable if was else gc.disable)()
+
+
+def test_separable_ray_tables():
+    """Host logic of the fused PoU warp adjoint: a pinhole lattice whose rays
+    agree per detector column (rx) and per row (ry) up to float rounding gives
+    the per-column and per-row midpoints; a skewed lattice gives None (the
+    two-kernel backward then runs)."""
+    from fvr.cone_beam_fvr import _SEPARABLE_REL, _separable_rays
+
+    H, W = 6, 8
+    cols = torch.linspace(-0.1, 0.1, W)
+    rows = torch.linspace(-0.08, 0.08, H)
+    rx = cols.repeat(H, 1).clone()
+    ry = rows[:, None].repeat(1, W).clone()
+    rx[2, 3] = torch.nextafter(rx[2, 3], torch.tensor(1.0))  # one float step, as the lattice's rounding
+    out = _separable_rays(rx, ry)
+    assert out is not None
+    rxc, ryr = out
+    assert rxc.shape == (W,) and ryr.shape == (H,)
+    assert torch.allclose(rxc, cols, rtol=0, atol=1e-8) and torch.equal(ryr, rows)
+    skew = rx + 1e-3 * torch.arange(H, dtype=torch.float32)[:, None]  # rx moves along a column
+    assert _separable_rays(skew, ry) is None
+    assert _separable_rays(rx, ry + 1e-3 * torch.arange(W, dtype=torch.float32)[None, :]) is None
+    assert _separable_rays(rx.reshape(-1), ry.reshape(-1)) is None
+    assert 0 < _SEPARABLE_REL < 1e-5
