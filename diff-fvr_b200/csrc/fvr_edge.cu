@@ -349,13 +349,10 @@ int fvr_edge_ncc_backward(const float* a, const float* b, int64_t B, int64_t Bt,
   int rc = edge_args(a, b, B, Bt, C, H, W, crop, ms_weight, &e);
   if (rc) return rc;
   if (!stats || !g || !grad) return FVR_ERR_ARG;
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(edge_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEdgeGradSmem) !=
-        cudaSuccess)
-      return FVR_ERR_CUDA;
-    attr_set = true;
-  }
+  // the shared-memory opt-in is a per-device setting: made before every launch
+  if (cudaFuncSetAttribute(edge_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEdgeGradSmem) !=
+      cudaSuccess)
+    return FVR_ERR_CUDA;
   dim3 grid(static_cast<unsigned>(cdiv64(W, kEdgeTile)), static_cast<unsigned>(cdiv64(H, kEdgeTile)),
             static_cast<unsigned>(B * C));
   edge_grad_kernel<<<grid, kEdgeThreads, kEdgeGradSmem, static_cast<cudaStream_t>(stream)>>>(

@@ -1709,23 +1709,16 @@ static int pou_image_launch(bool adjoint, const PouSliceArgs& a, int B, const fl
                             double* part, cudaStream_t s) {
   const int64_t smem = adjoint ? pou_adjoint_smem(32 * M) : pou_image_smem(32 * M);
   dim3 grid(static_cast<unsigned>(a.N), static_cast<unsigned>(B));
+  // the shared-memory opt-in is a per-device setting: made before every launch
   if (adjoint) {
-    static bool attr = false;
-    if (!attr) {
-      if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M, false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
-        return FVR_ERR_CUDA;
-      attr = true;
-    }
+    if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+      return FVR_ERR_CUDA;
     pou_fft_slice_adjoint_kernel<DT, M, false><<<grid, kPouImgThreads, smem, s>>>(a, gimg, PouWarpSep{}, part);
   } else {
-    static bool attr = false;
-    if (!attr) {
-      if (cudaFuncSetAttribute(pou_slice_ifft_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem)) != cudaSuccess)
-        return FVR_ERR_CUDA;
-      attr = true;
-    }
+    if (cudaFuncSetAttribute(pou_slice_ifft_kernel<DT, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+      return FVR_ERR_CUDA;
     pou_slice_ifft_kernel<DT, M><<<grid, kPouImgThreads, smem, s>>>(a, imgs);
   }
   FVR_LAUNCH_CHECK();
@@ -1747,13 +1740,9 @@ static int pou_image_dispatch(bool adjoint, const PouSliceArgs& a, int B, const 
 template <int DT, int M>
 static int pou_fused_launch(const PouSliceArgs& a, int B, const PouWarpSep& w, double* part, cudaStream_t s) {
   const int64_t smem = pou_fused_smem(32 * M, w.Hd, w.W);
-  static int64_t attr = 0;  // largest dynamic shared memory opted in so far
-  if (smem > attr) {
-    if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem)) != cudaSuccess)
-      return FVR_ERR_CUDA;
-    attr = smem;
-  }
+  if (cudaFuncSetAttribute(pou_fft_slice_adjoint_kernel<DT, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)  // per-device setting: before every launch
+    return FVR_ERR_CUDA;
   pou_fft_slice_adjoint_kernel<DT, M, true>
       <<<dim3(static_cast<unsigned>(a.N), static_cast<unsigned>(B)), kPouImgThreads, smem, s>>>(a, nullptr, w, part);
   FVR_LAUNCH_CHECK();
