@@ -59,6 +59,11 @@ def main():
         o = m.forward_pinhole(mats, lat)
         (o * o).sum().backward()
         out[f"pou_{name}"] = o.flatten().tolist()[::7] + mats.grad.flatten().tolist()
+        m.fused_warp_adjoint = False  # the two-kernel backward (warp adjoint + block-image adjoint)
+        mats3 = mats.detach().clone().requires_grad_(True)
+        (m.forward_pinhole(mats3, lat) ** 2).sum().backward()
+        out[f"pou_two_kernel_{name}"] = mats3.grad.flatten().tolist()
+        m.fused_warp_adjoint = True
         mats2 = mats.detach().clone().requires_grad_(True)
         o2 = m.forward_pinhole(mats2, lat[:5])
         o2.sum().backward()
